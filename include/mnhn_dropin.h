@@ -1,0 +1,89 @@
+/*
+ * Drop-in entry points: the functions of MNHN-Tree-Tools' Smith-Waterman path,
+ * with the reference's names and CPU-build signatures, exported by
+ * libswgpu.so.  A caller written against the reference (cluster_dbscan_SW.c,
+ * adaptive_clustering.c, find_closest_sequence_SW.c, filter.c, comparison.c)
+ * links against libswgpu.so instead of smith_waterman.o, dbscan_SW.o,
+ * dataset.o and cluster_io.o.  All distance work runs on the GPU; there is no
+ * CPU fallback.  When no usable GPU is present the functions print an error
+ * and return the empty result documented below.
+ *
+ * Each declaration names the reference interface it replaces.
+ */
+#ifndef MNHN_DROPIN_H
+#define MNHN_DROPIN_H
+
+#include <stdio.h>
+#include "mnhn_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* smith-waterman.h:1 / smith-waterman.c:16-80.  Distance 4*max(len_a,len_b)
+   minus the best linear-gap local alignment score of A[1..len_a] against
+   B[1..len_b] (+4 match, -4 mismatch, -3 gap).  A and B must be readable at
+   [0..len].  `work` is accepted and ignored.  Returns UINT_MAX on a GPU error. */
+unsigned int score(char* A, char* B, size_t len_a, size_t len_b, int* work);
+
+/* dataset.c:264-344.  FASTA records; first token of every sequence line,
+   upper-cased; a line without a token repeats the previous token. */
+dataset dataset_from_fasta(FILE* in);
+
+/* dataset.c (free_sequences_from_dataset): frees the sequences and lengths. */
+void free_sequences_from_dataset(dataset ds);
+
+/* dbscan.h:30 / dbscan.c:950-1047.  DBSCAN over the Smith-Waterman distance
+   ((float)d <= epsilon), seed test minpts < |N|, expansion test |N| >= minpts,
+   clusters and members in the reference's traversal order.  epsilon == -1
+   becomes 0.015 and minpts == -1 becomes 5 (dbscan.c:980-989).  All pair
+   distances of a dataset are scored once on the GPU and reused by later calls
+   on the same sequences.  Returns {0, NULL} on a GPU error. */
+split_set dbscan_SW(dataset ds, float epsilon, int minpts);
+
+/* dbscan.h:72-81 / dbscan.c:1117-1380.  Adaptive eps sweep: halving search for
+   a start with more than one cluster, eps += inc until one cluster remains,
+   layers kept when their cluster count strictly drops, log lines on stdout,
+   split sets written to <prefix>%04d.  When `dbscanner` is dbscan_SW the
+   distances are scored once for the whole sweep.  Layers are produced in eps
+   order whatever `n_threads` is.  Where the reference calls _exit(1) this
+   function prints the same message and returns; swgpu_last_dropin_status()
+   then returns non-zero. */
+void adaptive_dbscan(split_set (*dbscanner)(dataset, float, int), dataset ds, float epsilon_start,
+                     float epsilon_inc, int minpts, char* split_files_prefix, int n_threads);
+
+/* cluster_io.c:638-669: "SPLIT_SET", int32 n_clusters, then per cluster
+   int32 n_members, int32 id, int32 members[]; opened without O_TRUNC. */
+void store_split_set(char* filename, split_set s);
+
+/* cluster_io.c:595-636. */
+split_set read_split_set(char* filename);
+
+/* cluster_io.c:672-699: records ">sequence_<idx>", 50 characters per line. */
+void create_single_cluster_file(char* filename, cluster cl, dataset ds);
+
+/* cluster_io.c:701-720: one file <prefix>-%03d per cluster. */
+void create_cluster_files(char* prefix, split_set s, dataset ds);
+
+/* cluster_io.c:564-593: ascending indices that belong to no cluster. */
+cluster data_not_in_clusters(split_set s, dataset ds);
+
+/* cluster_io.c:446-501.  The larger cluster (a on ties) is sorted in place
+   when it has more than 20 members, as in the reference. */
+cluster intersection_of_clusters(cluster a, cluster b);
+
+/* cluster_io.c:407-444: new cluster i is connected to ancient cluster j when
+   |j ∩ i| > 0.8 |j|.  Returns new_set.n_clusters entries. */
+cluster_connections* generate_split_set_relation(split_set ancient, split_set new_set);
+
+/* cluster_io.c:722-729. */
+void free_split_set_and_associated_clusters(split_set s);
+
+/* Status of the last drop-in call that can fail without a return code
+   (adaptive_dbscan, dbscan_SW, score): 0 on success, else an swe_status. */
+int swgpu_last_dropin_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MNHN_DROPIN_H */

@@ -1,0 +1,58 @@
+/*
+ * Data structures of MNHN-Tree-Tools' Smith-Waterman path, with the field
+ * layout of the reference so that reference-style callers link unchanged.
+ *
+ *   dataset              dataset.h:27-35
+ *   cluster              cluster.h:10-15
+ *   split_set            cluster.h:20-23
+ *   cluster_connections  cluster.h:28-31
+ *   neighbors            dbscan.h:5-8
+ *
+ * Ownership follows the reference: arrays inside returned structs come from
+ * malloc and are released with free() (free_split_set_and_associated_clusters,
+ * cluster_io.c:722-729, and free_sequences_from_dataset).
+ */
+#ifndef MNHN_TYPES_H
+#define MNHN_TYPES_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  char** sequences;          /* NUL-terminated, upper-cased sequences */
+  size_t* sequence_lengths;  /* strlen of each sequence */
+  void** binary_sequences;   /* unused on this path */
+  int n_values;              /* number of sequences */
+  float** values;            /* unused on this path */
+  int n_dimensions;          /* unused on this path */
+  size_t max_sequence_length;
+} dataset;
+
+typedef struct {
+  int* members;   /* dataset indices, in the order DBSCAN reached them */
+  int n_members;
+  int id;         /* position of the cluster in its split set */
+} cluster;
+
+typedef struct {
+  int n_clusters;
+  cluster* clusters;
+} split_set;
+
+typedef struct {
+  int* connections;
+  int n_connections;
+} cluster_connections;
+
+typedef struct {
+  int* members;   /* ascending dataset indices, the query point included */
+  int n_members;
+} neighbors;
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MNHN_TYPES_H */

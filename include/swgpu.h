@@ -1,0 +1,142 @@
+/*
+ * swgpu — B200 engine for MNHN-Tree-Tools' all-pairs Smith-Waterman
+ * neighbourhood path.  Plain C ABI: plain pointers and sizes, no C++ or torch
+ * types.
+ *
+ * The reference has no engine API: its OpenCL queue, kernel launches and
+ * thresholding sit inline in dbscan.c (opencl_initialization :97-284,
+ * region_query :471-522, MPI split :309-468).  These calls replace that inline
+ * code; the reference-named functions in mnhn_dropin.h are built on them.
+ *
+ * Every call returns an swe_status (0 = SWE_OK).  Nothing here exits the
+ * process.  A context owns one CUDA stream on one device; use one context per
+ * host thread (calls on one context are not thread-safe).
+ */
+#ifndef SWGPU_H
+#define SWGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdio.h>
+#include "mnhn_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SWE_OK = 0,
+  SWE_ERR_INVALID = 1,    /* bad argument or input */
+  SWE_ERR_CUDA = 2,       /* CUDA runtime error */
+  SWE_ERR_OOM = 3,        /* device or host allocation failed */
+  SWE_ERR_NO_DEVICE = 4,  /* no usable CUDA device */
+  SWE_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+  SWE_ERR_RERUN = 6,      /* the 32-bit rerun queue overflowed */
+  SWE_ERR_STATE = 7,      /* call out of order (e.g. no dataset uploaded) */
+  SWE_ERR_IO = 8,         /* file could not be read or written */
+  SWE_ERR_SWEEP = 9       /* adaptive sweep cannot reach one cluster */
+} swe_status;
+
+typedef struct swe_ctx swe_ctx;
+
+typedef struct {
+  int device;          /* CUDA device ordinal */
+  int sat_limit;       /* 16-bit maxima >= sat_limit are rescored in 32-bit
+                          (0 = default 32000; only tests lower it) */
+  int packs_per_block; /* row-sequence pairs per tile (0 = default 32) */
+  int threads;         /* threads per CTA of the 16x2 kernel (0 = 256) */
+  int inject_timeout;  /* test hook: 1 = the score pass's first tile waits on a
+                          copy that is never issued, so its bounded wait runs
+                          out and the pass returns SWE_ERR_TIMEOUT */
+} swe_opts;
+
+typedef struct {
+  int64_t n_sequences;
+  int64_t n_fast;          /* sequences on the packed 16-bit path */
+  int64_t n_exceptional;   /* sequences on the 32-bit path (rare symbols, long, empty) */
+  int64_t unique_pairs;    /* n*(n-1)/2 */
+  double cells;            /* sum over unique pairs of len_a*len_b */
+  double tile_cells;       /* cells the 16x2 kernel actually processed, padding included */
+  int64_t reruns;          /* pairs rescored in 32-bit after the saturation guard */
+  int64_t n_tiles;
+  double ms_score_pass;    /* device time of the last score pass */
+  double ms_fast_kernel;   /* device time of the 16x2 kernel inside it */
+  double ms_last_neighbors;/* device time of the last eps threshold pass */
+  int dist_bytes;          /* 2 (uint16 matrix) or 4 */
+  int64_t h2d_bytes;       /* host->device bytes since the last upload began */
+  int64_t d2h_bytes;       /* device->host bytes since the last upload began */
+  int64_t kernel_launches; /* this library's kernel launches since the last upload began */
+} swe_stats;
+
+const char* swe_strerror(swe_status s);
+
+swe_status swe_create(swe_ctx** out, const swe_opts* opts /* may be NULL */);
+void swe_destroy(swe_ctx* ctx);
+/* Message of the last failure on this context (never NULL). */
+const char* swe_last_error(const swe_ctx* ctx);
+
+/* Copies n sequences to the device.  seqs[i] must be readable at
+   [0 .. lens[i]]; position 0 never takes part in a score and position lens[i]
+   does (it is the NUL terminator for C strings), as in smith-waterman.c:56-58. */
+swe_status swe_upload(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n);
+
+/* Scores every pair of the uploaded sequences into the device distance matrix
+   (one pass; later neighbour/DBSCAN calls reuse it). */
+swe_status swe_score_all_pairs(swe_ctx* ctx);
+
+/* Copies the n x n distance matrix to host memory (out holds n*n entries). */
+swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out);
+
+/* eps-neighbourhoods of every point, the reference's region_query
+   (dbscan.c:525-561) for all points at once: ascending indices k with
+   (float)d(k,i) <= eps, i itself included.  *row_ptr (n+1 entries) and *cols
+   are malloc'd; release them with swe_free. */
+swe_status swe_neighbors(swe_ctx* ctx, float eps, int64_t** row_ptr, int** cols);
+
+/* DBSCAN at one eps (dbscan.c:950-1047 semantics) on the scored matrix.
+   The split set is malloc'd reference-style. */
+swe_status swe_dbscan(swe_ctx* ctx, float eps, int minpts, split_set* out);
+
+/* Adaptive sweep (dbscan.c:1117-1380 semantics) on the scored matrix.  Log
+   lines go to `log` (stdout when NULL); split sets are written to
+   <prefix>%04d unless prefix is NULL.  If out_sets is not NULL it receives a
+   malloc'd array of the kept layers (free each with
+   free_split_set_and_associated_clusters, then the array with swe_free). */
+swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, const char* prefix,
+                        FILE* log, split_set** out_sets, int* out_n_sets);
+
+/* Distances of one query to every uploaded sequence (out holds n entries).
+   q must be readable at [0 .. qlen]. */
+swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsigned* out);
+
+/* Distances of explicit pairs of uploaded sequences. */
+swe_status swe_score_pairs(swe_ctx* ctx, const int* a, const int* b, int64_t npairs, unsigned* out);
+
+swe_status swe_get_stats(const swe_ctx* ctx, swe_stats* out);
+
+/* DBSCAN replay (dbscan.c:950-1047 order semantics) on caller-provided
+   neighbourhoods; host only, no GPU involved.  Row i of `bits` is
+   words_per_row 64-bit words with bit k set iff k is an eps-neighbour of i
+   (i itself included when eps >= 0); counts[i] is that row's popcount. */
+swe_status swe_dbscan_bitmap(int n, const uint64_t* bits, int words_per_row, const int* counts, int minpts,
+                             split_set* out);
+
+/* Measures, on `device`, the issue rate of the 16x2 kernel's per-cell
+   instruction mix (one PRMT, three packed add-max, one packed max) on
+   independent chains: *cells_per_s DP cells per second (two per packed
+   update) and *lane_instr_per_s the corresponding 32-bit-lane instructions
+   per second.  The integer roofline of the score pass is derived from it. */
+swe_status swe_measure_mix_peak(int device, double* cells_per_s, double* lane_instr_per_s);
+
+/* Step timer on the context's stream: start records a CUDA event, stop
+   records a second one, waits for it and returns the elapsed milliseconds.
+   Host work between the two calls (DBSCAN replay) is inside the interval. */
+swe_status swe_timer_start(swe_ctx* ctx);
+swe_status swe_timer_stop(swe_ctx* ctx, double* ms);
+
+void swe_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWGPU_H */

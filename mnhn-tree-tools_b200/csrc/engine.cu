@@ -1,0 +1,925 @@
+// swgpu engine: context, upload, score pass, eps neighbourhoods.
+//
+// Replaces the reference's inline OpenCL runtime (dbscan.c:97-298) and the
+// per-point region_query launches (dbscan.c:471-522): the sequences go to the
+// device once, one score pass fills the n x n distance matrix in HBM, and
+// every later eps threshold reads that matrix instead of re-scoring.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "host_internal.h"
+#include "sw_device.cuh"
+#include "sw_kernels.cuh"
+
+using namespace swgpu;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (p && count <= n) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+template <typename T>
+struct HostPinned {
+  T* p = nullptr;
+  size_t n = 0;
+  HostPinned() = default;
+  HostPinned(const HostPinned&) = delete;
+  HostPinned& operator=(const HostPinned&) = delete;
+  ~HostPinned() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (p && count <= n) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+}  // namespace
+
+struct swe_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int num_sms = 148;
+  int sat_limit = 32000;
+  int packs_per_block = 32;
+  int threads = 256;
+  int inject_timeout = 0;
+  int graph_kernels = 0;
+  std::string err;
+
+  // dataset (host)
+  int n = 0;
+  int max_len = 0;
+  int max_fast_len = 0;
+  int nfast = 0;
+  std::vector<int> len;
+  std::vector<int64_t> off;
+  std::vector<uint8_t> codes;
+  int code_of[256];
+  std::vector<int> order, exc;
+  std::vector<uint8_t> is_exc;
+  int npacks = 0;
+  int max_block_rows = 0;
+  int max_cols = 0;
+  size_t smem = 0;
+  int fast_grid = 0;
+  std::vector<FastTile> tiles;
+
+  // dataset (device)
+  DevBuf<uint8_t> d_codes;
+  DevBuf<int64_t> d_off;
+  DevBuf<int> d_len, d_order, d_exc, d_pack_off, d_pack_rows;
+  DevBuf<uint8_t> d_isexc;
+  DevBuf<uint16_t> d_sel;
+  DevBuf<FastTile> d_tiles;
+  DevBuf<unsigned> d_ctr;  // [0] tile counter, [1] status, [2] rerun count
+  DevBuf<int2> d_rerun;
+  unsigned rerun_cap = 0;
+  bool rerun_possible = false;
+  DevBuf<int> d_scratch;
+  long long scratch_stride = 0;
+  int gen_grid = 0;
+
+  // distances
+  DevBuf<uint16_t> d_D16;
+  DevBuf<uint32_t> d_D32;
+  int dist_bytes = 2;
+  bool scored = false;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t tev[2] = {nullptr, nullptr};
+
+  // neighbour bitmaps
+  int wpr = 0;
+  DevBuf<uint64_t> d_bits;
+  DevBuf<int> d_counts;
+  HostPinned<uint64_t> h_bits;
+  HostPinned<int> h_counts;
+  long long bits_T = LLONG_MIN;
+
+  // small transfers
+  DevBuf<uint8_t> d_q;
+  DevBuf<unsigned> d_out;
+  DevBuf<int2> d_pairs;
+  DevBuf<int64_t> d_small_off;
+  DevBuf<int> d_small_len;
+  DevBuf<int> d_small_scratch;
+  DevBuf<long long> d_row_ptr;
+  DevBuf<int> d_cols;
+
+  swe_stats stats{};
+
+  ~swe_ctx() {
+    cudaSetDevice(device);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : tev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace {
+
+swe_status fail(swe_ctx* ctx, swe_status s, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return s;
+}
+
+swe_status cuda_fail(swe_ctx* ctx, cudaError_t e, const char* what) {
+  const swe_status s = (e == cudaErrorMemoryAllocation) ? SWE_ERR_OOM : SWE_ERR_CUDA;
+  return fail(ctx, s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+swe_status check_kernel_status(swe_ctx* ctx, unsigned status) {
+  if (status & KST_TIMEOUT) return fail(ctx, SWE_ERR_TIMEOUT, "device-side wait timed out");
+  if (status & KST_RERUN_OVERFLOW) return fail(ctx, SWE_ERR_RERUN, "32-bit rerun queue overflowed");
+  if (status & KST_BAD_TILE) return fail(ctx, SWE_ERR_STATE, "invalid tile descriptor");
+  return SWE_OK;
+}
+
+void drop_graph(swe_ctx* ctx) {
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  ctx->graph = nullptr;
+}
+
+// Builds the code table: A C G T N NUL -> 0..5, the most frequent other
+// symbol -> 6, the remaining symbols by descending frequency -> 7, 8, ...
+void build_code_table(const uint64_t* freq, int* code_of) {
+  for (int c = 0; c < 256; ++c) code_of[c] = -1;
+  code_of[(unsigned char)'A'] = CODE_A;
+  code_of[(unsigned char)'C'] = CODE_C;
+  code_of[(unsigned char)'G'] = CODE_G;
+  code_of[(unsigned char)'T'] = CODE_T;
+  code_of[(unsigned char)'N'] = CODE_N;
+  code_of[0] = CODE_NUL;
+  std::vector<int> rest;
+  for (int c = 0; c < 256; ++c)
+    if (code_of[c] < 0 && freq[c] > 0) rest.push_back(c);
+  std::stable_sort(rest.begin(), rest.end(), [&](int a, int b) { return freq[a] > freq[b]; });
+  int next = CODE_EXTRA;
+  for (int c : rest) code_of[c] = next++;
+  // symbols that never occur get the remaining codes, so queries can be encoded
+  for (int c = 0; c < 256; ++c)
+    if (code_of[c] < 0) code_of[c] = next++;
+}
+
+// Stream-ordered copy that also counts the bytes crossing PCIe.
+cudaError_t cpy(swe_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  if (kind == cudaMemcpyHostToDevice) ctx->stats.h2d_bytes += (int64_t)bytes;
+  else if (kind == cudaMemcpyDeviceToHost) ctx->stats.d2h_bytes += (int64_t)bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, st);
+}
+
+swe_status select_device(swe_ctx* ctx) {
+  CK(cudaSetDevice(ctx->device));
+  return SWE_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* swe_strerror(swe_status s) {
+  switch (s) {
+    case SWE_OK: return "ok";
+    case SWE_ERR_INVALID: return "invalid argument";
+    case SWE_ERR_CUDA: return "CUDA error";
+    case SWE_ERR_OOM: return "out of memory";
+    case SWE_ERR_NO_DEVICE: return "no usable CUDA device";
+    case SWE_ERR_TIMEOUT: return "device-side wait timed out";
+    case SWE_ERR_RERUN: return "32-bit rerun queue overflowed";
+    case SWE_ERR_STATE: return "call out of order";
+    case SWE_ERR_IO: return "file could not be read or written";
+    case SWE_ERR_SWEEP: return "adaptive sweep cannot reach one cluster";
+  }
+  return "unknown status";
+}
+
+const char* swe_last_error(const swe_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+void swe_free(void* p) { free(p); }
+
+swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
+  if (!out) return SWE_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return SWE_ERR_NO_DEVICE;
+  }
+  const int dev = opts ? opts->device : 0;
+  if (dev < 0 || dev >= ndev) return SWE_ERR_INVALID;
+  swe_ctx* ctx = new (std::nothrow) swe_ctx();
+  if (!ctx) return SWE_ERR_OOM;
+  ctx->device = dev;
+  if (opts && opts->sat_limit > 0) ctx->sat_limit = opts->sat_limit;
+  if (opts && opts->packs_per_block > 0) ctx->packs_per_block = std::min(opts->packs_per_block, 256);
+  if (opts && opts->threads > 0) {
+    if (opts->threads % 32 != 0 || opts->threads > 256) {
+      delete ctx;
+      return SWE_ERR_INVALID;
+    }
+    ctx->threads = opts->threads;
+  }
+  if (opts && opts->inject_timeout) ctx->inject_timeout = 1;
+  cudaError_t e = cudaSetDevice(dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
+  for (auto& ev : ctx->ev)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  for (auto& ev : ctx->tev)
+    if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  cudaDeviceProp prop;
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, dev);
+  if (e == cudaSuccess) {
+    ctx->num_sms = prop.multiProcessorCount;
+    e = ctx->d_ctr.alloc(4);
+  }
+  if (e != cudaSuccess) {
+    delete ctx;
+    return e == cudaErrorMemoryAllocation ? SWE_ERR_OOM : SWE_ERR_CUDA;
+  }
+  *out = ctx;
+  return SWE_OK;
+}
+
+void swe_destroy(swe_ctx* ctx) { delete ctx; }
+
+swe_status swe_upload(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (n < 0 || (n > 0 && (!seqs || !lens))) return fail(ctx, SWE_ERR_INVALID, "bad sequence arrays");
+  if (swe_status s = select_device(ctx)) return s;
+  drop_graph(ctx);
+  ctx->scored = false;
+  ctx->bits_T = LLONG_MIN;
+  ctx->n = n;
+  ctx->len.assign(n, 0);
+  ctx->off.assign(n, 0);
+  ctx->is_exc.assign(n, 0);
+  ctx->stats = swe_stats{};
+
+  // alphabet over the effective symbols s[1..len]
+  uint64_t freq[256] = {0};
+  int64_t total = 0;
+  int max_len = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!seqs[i] && lens[i] > 0) return fail(ctx, SWE_ERR_INVALID, "null sequence pointer");
+    if (lens[i] > (size_t)(INT_MAX / 8)) return fail(ctx, SWE_ERR_INVALID, "sequence too long");
+    const int L = (int)lens[i];
+    ctx->len[i] = L;
+    max_len = std::max(max_len, L);
+    const unsigned char* s = reinterpret_cast<const unsigned char*>(seqs[i]);
+    for (int r = 0; r < L; ++r) freq[s[r + 1]]++;
+    ctx->off[i] = total;
+    total += (L + 15) & ~15;
+  }
+  ctx->max_len = max_len;
+  build_code_table(freq, ctx->code_of);
+  ctx->codes.assign((size_t)std::max<int64_t>(total, 16), 0);
+  ctx->order.clear();
+  ctx->exc.clear();
+  int max_fast = 0;
+  for (int i = 0; i < n; ++i) {
+    const int L = ctx->len[i];
+    const unsigned char* s = reinterpret_cast<const unsigned char*>(seqs[i]);
+    uint8_t* dst = ctx->codes.data() + ctx->off[i];
+    bool fast = (L >= 1 && L <= FAST_MAX_LEN);
+    for (int r = 0; r < L; ++r) {
+      const int c = ctx->code_of[s[r + 1]];
+      dst[r] = (uint8_t)c;
+      if (c >= FAST_CODES) fast = false;
+    }
+    if (fast) {
+      ctx->order.push_back(i);
+      max_fast = std::max(max_fast, L);
+    } else {
+      ctx->exc.push_back(i);
+      ctx->is_exc[i] = 1;
+    }
+  }
+  ctx->max_fast_len = max_fast;
+  std::stable_sort(ctx->order.begin(), ctx->order.end(),
+                   [&](int a, int b) { return ctx->len[a] > ctx->len[b]; });
+  const int nfast = (int)ctx->order.size();
+  ctx->nfast = nfast;
+
+  // packs of two consecutive sorted sequences; blocks of PB packs start on
+  // 8-row (16-byte) boundaries so a whole block is one bulk copy
+  const int PB = ctx->packs_per_block;
+  const int npacks = (nfast + 1) / 2;
+  ctx->npacks = npacks;
+  std::vector<int> pack_off(npacks + 1, 0), pack_rows(std::max(npacks, 1), 0);
+  const int nblocks = (npacks + PB - 1) / PB;
+  std::vector<int> block_rows(std::max(nblocks, 1), 0);
+  int64_t row = 0;
+  int max_block_rows = 8;
+  for (int q = 0; q < nblocks; ++q) {
+    row = (row + 7) & ~int64_t(7);
+    const int64_t start = row;
+    for (int pk = q * PB; pk < std::min(npacks, (q + 1) * PB); ++pk) {
+      const int a = ctx->order[2 * pk];
+      const int b = (2 * pk + 1 < nfast) ? ctx->order[2 * pk + 1] : -1;
+      const int R = std::max(ctx->len[a], b >= 0 ? ctx->len[b] : 0);
+      pack_off[pk] = (int)row;
+      pack_rows[pk] = R;
+      row += R;
+    }
+    block_rows[q] = (int)(row - start);
+    max_block_rows = std::max(max_block_rows, (int)((row - start + 7) & ~int64_t(7)));
+    if (row > INT_MAX / 2) return fail(ctx, SWE_ERR_INVALID, "dataset too large for one upload");
+  }
+  row = (row + 7) & ~int64_t(7);
+  pack_off[npacks] = (int)row;
+  ctx->max_block_rows = max_block_rows;
+
+  // tiles: blocks of column sequences (longest first) against row blocks
+  const int cta_warps = ctx->threads / 32;
+  ctx->tiles.clear();
+  std::vector<double> cost;
+  double tile_cells = 0;
+  for (int b0 = 0; b0 < nfast;) {
+    const int L = ctx->len[ctx->order[b0]];
+    const int lpb = L <= 8 * FAST_MAX_W ? 8 : (L <= 16 * FAST_MAX_W ? 16 : 32);
+    const int W = (L + lpb - 1) / lpb;
+    const int nb = std::min(nfast - b0, cta_warps * (32 / lpb));
+    for (int q = 0; q < nblocks; ++q) {
+      const int maxA = std::min(nfast - 1, (q + 1) * 2 * PB - 1);
+      if (maxA > b0) {
+        ctx->tiles.push_back(FastTile{b0, nb, q, W | (lpb << 8)});
+        const double c = (double)nb * lpb * W * block_rows[q];
+        cost.push_back(c);
+        tile_cells += 2.0 * c;
+      }
+    }
+    b0 += nb;
+  }
+  {
+    std::vector<int> idx(ctx->tiles.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<FastTile> sorted(ctx->tiles.size());
+    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]];
+    ctx->tiles.swap(sorted);
+  }
+  ctx->max_cols = cta_warps * 4;
+  ctx->smem = fast_smem_bytes(ctx->max_block_rows, ctx->max_cols, PB);
+
+  // statistics
+  {
+    double sum = 0, sq = 0;
+    for (int i = 0; i < n; ++i) {
+      sum += ctx->len[i];
+      sq += (double)ctx->len[i] * ctx->len[i];
+    }
+    ctx->stats.cells = (sum * sum - sq) / 2.0;
+    ctx->stats.tile_cells = tile_cells;
+    ctx->stats.n_sequences = n;
+    ctx->stats.n_fast = nfast;
+    ctx->stats.n_exceptional = (int64_t)ctx->exc.size();
+    ctx->stats.unique_pairs = (int64_t)n * (n - 1) / 2;
+    ctx->stats.n_tiles = (int64_t)ctx->tiles.size();
+  }
+
+  // device copies
+  CK(ctx->d_codes.alloc(ctx->codes.size()));
+  CK(ctx->d_off.alloc(std::max(n, 1)));
+  CK(ctx->d_len.alloc(std::max(n, 1)));
+  CK(ctx->d_isexc.alloc(std::max(n, 1)));
+  CK(ctx->d_order.alloc(std::max(nfast, 1)));
+  CK(ctx->d_exc.alloc(std::max<size_t>(ctx->exc.size(), 1)));
+  CK(ctx->d_pack_off.alloc(npacks + 1));
+  CK(ctx->d_pack_rows.alloc(std::max(npacks, 1)));
+  CK(ctx->d_sel.alloc(std::max<int64_t>(row, 8)));
+  CK(ctx->d_tiles.alloc(std::max<size_t>(ctx->tiles.size(), 1)));
+  cudaStream_t st = ctx->st;
+  CK(cpy(ctx, ctx->d_codes.p, ctx->codes.data(), ctx->codes.size(), cudaMemcpyHostToDevice, st));
+  if (n > 0) {
+    CK(cpy(ctx, ctx->d_off.p, ctx->off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st));
+    CK(cpy(ctx, ctx->d_len.p, ctx->len.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    CK(cpy(ctx, ctx->d_isexc.p, ctx->is_exc.data(), n, cudaMemcpyHostToDevice, st));
+  }
+  if (nfast > 0)
+    CK(cpy(ctx, ctx->d_order.p, ctx->order.data(), sizeof(int) * nfast, cudaMemcpyHostToDevice, st));
+  if (!ctx->exc.empty())
+    CK(cpy(ctx, ctx->d_exc.p, ctx->exc.data(), sizeof(int) * ctx->exc.size(), cudaMemcpyHostToDevice,
+                       st));
+  CK(cpy(ctx, ctx->d_pack_off.p, pack_off.data(), sizeof(int) * (npacks + 1), cudaMemcpyHostToDevice,
+                     st));
+  if (npacks > 0)
+    CK(cpy(ctx, ctx->d_pack_rows.p, pack_rows.data(), sizeof(int) * npacks, cudaMemcpyHostToDevice,
+                       st));
+  if (!ctx->tiles.empty())
+    CK(cpy(ctx, ctx->d_tiles.p, ctx->tiles.data(), sizeof(FastTile) * ctx->tiles.size(),
+                       cudaMemcpyHostToDevice, st));
+  ctx->stats.kernel_launches += 1;
+  CK(launch_build_sel(ctx->d_codes.p, ctx->d_off.p, ctx->d_len.p, ctx->d_order.p, nfast, ctx->d_pack_off.p,
+                      npacks, ctx->d_sel.p, st));
+
+  // distance matrix
+  ctx->dist_bytes = max_len <= 16383 ? 2 : 4;
+  ctx->stats.dist_bytes = ctx->dist_bytes;
+  const size_t nn = (size_t)n * (size_t)n;
+  ctx->d_D16.release();
+  ctx->d_D32.release();
+  if (ctx->dist_bytes == 2) CK(ctx->d_D16.alloc(std::max<size_t>(nn, 1)));
+  else CK(ctx->d_D32.alloc(std::max<size_t>(nn, 1)));
+
+  // 32-bit path resources: rerun queue (only when the guard can fire) and
+  // per-warp boundary columns for sequences longer than one 512-column chunk
+  ctx->rerun_possible = (long long)ctx->sat_limit <= 4LL * max_fast + 8;
+  double tile_pairs = 0;
+  for (const auto& t : ctx->tiles) tile_pairs += 2.0 * t.nb * PB;
+  ctx->rerun_cap = ctx->rerun_possible ? (unsigned)std::min(tile_pairs, (double)(1u << 26)) : 1024u;
+  CK(ctx->d_rerun.alloc(std::max(ctx->rerun_cap, 1u)));
+  ctx->gen_grid = ctx->num_sms * 4;
+  ctx->scratch_stride = 0;
+  if (max_len > GEN_CHUNK) {
+    ctx->scratch_stride = (long long)max_len + 1;
+    const long long warps = (long long)ctx->gen_grid * 8;
+    const long long budget = 1LL << 31;  // bytes
+    if (warps * ctx->scratch_stride * 4 > budget)
+      ctx->gen_grid = (int)std::max<long long>(ctx->num_sms, budget / (ctx->scratch_stride * 4 * 8));
+    CK(ctx->d_scratch.alloc((size_t)ctx->gen_grid * 8 * ctx->scratch_stride));
+  }
+
+  // 16x2 kernel launch shape
+  CK(fast_set_smem_limit(ctx->smem));
+  const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
+  ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
+  CK(cudaStreamSynchronize(st));
+  return SWE_OK;
+}
+
+static swe_status build_score_graph(swe_ctx* ctx) {
+  cudaStream_t st = ctx->st;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemsetAsync(ctx->d_ctr.p, 0, 4 * sizeof(unsigned), st);
+  ctx->graph_kernels = 1;
+  if (e == cudaSuccess) e = launch_diag(ctx->d_D16.p, ctx->d_D32.p, ctx->n, st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], st);
+  if (e == cudaSuccess && !ctx->tiles.empty()) {
+    FastParams p{};
+    p.codes = ctx->d_codes.p;
+    p.code_off = ctx->d_off.p;
+    p.len = ctx->d_len.p;
+    p.order = ctx->d_order.p;
+    p.nfast = ctx->nfast;
+    p.sel = ctx->d_sel.p;
+    p.pack_row_off = ctx->d_pack_off.p;
+    p.pack_rows = ctx->d_pack_rows.p;
+    p.npacks = ctx->npacks;
+    p.packs_per_block = ctx->packs_per_block;
+    p.tiles = ctx->d_tiles.p;
+    p.ntiles = (int)ctx->tiles.size();
+    p.tile_counter = ctx->d_ctr.p;
+    p.D16 = ctx->d_D16.p;
+    p.D32 = ctx->d_D32.p;
+    p.n = ctx->n;
+    p.rerun = ctx->d_rerun.p;
+    p.rerun_count = ctx->d_ctr.p + 2;
+    p.rerun_cap = ctx->rerun_cap;
+    p.sat_limit = ctx->sat_limit;
+    p.status = ctx->d_ctr.p + 1;
+    p.max_block_rows = ctx->max_block_rows;
+    p.max_cols_per_cta = ctx->max_cols;
+    p.wait_limit = ctx->inject_timeout ? (1u << 10) : (1u << 24);
+    p.inject_timeout = ctx->inject_timeout;
+    e = launch_fast(p, ctx->fast_grid, ctx->threads, ctx->smem, st);
+    ctx->graph_kernels++;
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], st);
+  GenParams g{};
+  g.codes = ctx->d_codes.p;
+  g.code_off = ctx->d_off.p;
+  g.len = ctx->d_len.p;
+  g.n = ctx->n;
+  g.D16 = ctx->d_D16.p;
+  g.D32 = ctx->d_D32.p;
+  g.scratch = ctx->d_scratch.p;
+  g.scratch_stride = ctx->scratch_stride;
+  g.nwarps_total = ctx->gen_grid * 8;
+  g.status = ctx->d_ctr.p + 1;
+  g.is_exc = ctx->d_isexc.p;
+  if (e == cudaSuccess && !ctx->exc.empty()) {
+    GenParams x = g;
+    x.mode = GEN_EXC_CROSS;
+    x.exc = ctx->d_exc.p;
+    x.nexc = (int)ctx->exc.size();
+    e = launch_generic(x, ctx->gen_grid, st);
+    ctx->graph_kernels++;
+  }
+  if (e == cudaSuccess && ctx->rerun_possible) {
+    GenParams r = g;
+    r.mode = GEN_PAIRS;
+    r.pairs = ctx->d_rerun.p;
+    r.npairs_dev = ctx->d_ctr.p + 2;
+    e = launch_generic(r, ctx->gen_grid, st);
+    ctx->graph_kernels++;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->graph, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    ctx->graph = nullptr;
+    return cuda_fail(ctx, e, "building the score-pass graph");
+  }
+  return SWE_OK;
+}
+
+swe_status swe_score_all_pairs(swe_ctx* ctx) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  ctx->bits_T = LLONG_MIN;
+  if (ctx->n == 0) {
+    ctx->scored = true;
+    return SWE_OK;
+  }
+  if (!ctx->graph)
+    if (swe_status s = build_score_graph(ctx)) return s;
+  CK(cudaEventRecord(ctx->ev[2], ctx->st));
+  CK(cudaGraphLaunch(ctx->graph, ctx->st));
+  ctx->stats.kernel_launches += ctx->graph_kernels;
+  CK(cudaEventRecord(ctx->ev[3], ctx->st));
+  unsigned ctr[4];
+  CK(cpy(ctx, ctr, ctx->d_ctr.p, sizeof(ctr), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  float ms = 0, msf = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+  cudaEventElapsedTime(&msf, ctx->ev[0], ctx->ev[1]);
+  ctx->stats.ms_score_pass = ms;
+  ctx->stats.ms_fast_kernel = msf;
+  ctx->stats.reruns = std::min(ctr[2], ctx->rerun_cap);
+  if (swe_status s = check_kernel_status(ctx, ctr[1])) return s;
+  ctx->scored = true;
+  return SWE_OK;
+}
+
+swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out) {
+  if (!ctx || (!out && ctx->n > 0)) return SWE_ERR_INVALID;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  const size_t nn = (size_t)ctx->n * ctx->n;
+  if (nn == 0) return SWE_OK;
+  if (ctx->dist_bytes == 4) {
+    CK(cudaMemcpy(out, ctx->d_D32.p, nn * 4, cudaMemcpyDeviceToHost));
+    return SWE_OK;
+  }
+  std::vector<uint16_t> tmp;
+  try {
+    tmp.resize(nn);
+  } catch (...) {
+    return fail(ctx, SWE_ERR_OOM, "host buffer");
+  }
+  CK(cudaMemcpy(tmp.data(), ctx->d_D16.p, nn * 2, cudaMemcpyDeviceToHost));
+  for (size_t k = 0; k < nn; ++k) out[k] = tmp[k];
+  return SWE_OK;
+}
+
+}  // extern "C"
+
+// Neighbour bitmap of threshold T on the host (pinned), cached per T.
+static swe_status ensure_bitmap(swe_ctx* ctx, long long T) {
+  if (ctx->bits_T == T) return SWE_OK;
+  const int n = ctx->n;
+  ctx->wpr = (n + 63) / 64;
+  const size_t words = (size_t)n * (size_t)ctx->wpr;
+  CK(ctx->h_bits.alloc(std::max<size_t>(words, 1)));
+  CK(ctx->h_counts.alloc(std::max(n, 1)));
+  if (T < 0 || n == 0) {
+    if (words) memset(ctx->h_bits.p, 0, words * 8);
+    if (n) memset(ctx->h_counts.p, 0, sizeof(int) * n);
+    ctx->bits_T = T;
+    return SWE_OK;
+  }
+  CK(ctx->d_bits.alloc(words));
+  CK(ctx->d_counts.alloc(n));
+  CK(cudaEventRecord(ctx->ev[2], ctx->st));
+  ctx->stats.kernel_launches += 1;
+  CK(launch_bitmap(ctx->d_D16.p, ctx->d_D32.p, n, T, ctx->d_bits.p, ctx->wpr, ctx->d_counts.p, ctx->st));
+  CK(cudaEventRecord(ctx->ev[3], ctx->st));
+  CK(cpy(ctx, ctx->h_bits.p, ctx->d_bits.p, words * 8, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cpy(ctx, ctx->h_counts.p, ctx->d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+  ctx->stats.ms_last_neighbors = ms;
+  ctx->bits_T = T;
+  return SWE_OK;
+}
+
+extern "C" {
+
+swe_status swe_neighbors(swe_ctx* ctx, float eps, int64_t** row_ptr, int** cols) {
+  if (!ctx || !row_ptr || !cols) return SWE_ERR_INVALID;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  const long long T = eps_threshold(eps);
+  if (swe_status s = ensure_bitmap(ctx, T)) return s;
+  const int n = ctx->n;
+  int64_t* rp = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
+  if (!rp) return fail(ctx, SWE_ERR_OOM, "row_ptr");
+  rp[0] = 0;
+  for (int i = 0; i < n; ++i) rp[i + 1] = rp[i] + ctx->h_counts.p[i];
+  const int64_t E = rp[n];
+  int* cl = (int*)malloc(sizeof(int) * std::max<int64_t>(E, 1));
+  if (!cl) {
+    free(rp);
+    return fail(ctx, SWE_ERR_OOM, "cols");
+  }
+  if (E > 0) {
+    swe_status s = SWE_OK;
+    cudaError_t e = ctx->d_row_ptr.alloc(n + 1);
+    if (e == cudaSuccess) e = ctx->d_cols.alloc(E);
+    if (e == cudaSuccess)
+      e = cpy(ctx, ctx->d_row_ptr.p, rp, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx->st);
+    ctx->stats.kernel_launches += 1;
+    if (e == cudaSuccess)
+      e = launch_csr_fill(ctx->d_bits.p, n, ctx->wpr, ctx->d_row_ptr.p, ctx->d_cols.p, ctx->st);
+    if (e == cudaSuccess) e = cpy(ctx, cl, ctx->d_cols.p, sizeof(int) * E, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) s = cuda_fail(ctx, e, "neighbour lists");
+    if (s) {
+      free(rp);
+      free(cl);
+      return s;
+    }
+  }
+  *row_ptr = rp;
+  *cols = cl;
+  return SWE_OK;
+}
+
+swe_status swe_dbscan(swe_ctx* ctx, float eps, int minpts, split_set* out) {
+  if (!ctx || !out) return SWE_ERR_INVALID;
+  out->n_clusters = 0;
+  out->clusters = nullptr;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  if (eps == -1) eps = 0.015f;  // dbscan.c:980-984
+  if (minpts == -1) minpts = 5; // dbscan.c:985-989
+  const long long T = eps_threshold(eps);
+  if (swe_status s = ensure_bitmap(ctx, T)) return s;
+  const int rc = dbscan_replay_bitmap(ctx->n, ctx->h_bits.p, ctx->wpr, ctx->h_counts.p, minpts, out);
+  if (rc) return fail(ctx, (swe_status)rc, "dbscan replay");
+  return SWE_OK;
+}
+
+swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, const char* prefix,
+                        FILE* log, split_set** out_sets, int* out_n_sets) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  DbscanFn fn = [ctx, minpts](float eps, split_set* o) { return (int)swe_dbscan(ctx, eps, minpts, o); };
+  std::vector<split_set> kept;
+  std::string err;
+  const long long fixed = 4LL * ctx->max_len;  // every distance is <= 4*max_len
+  const int rc = adaptive_sweep(ctx->n, eps_start, eps_inc, minpts, prefix, log ? log : stdout, fn, fixed,
+                                &kept, &err);
+  if (rc) {
+    for (auto& s : kept) free_split_set_and_associated_clusters(s);
+    return fail(ctx, (swe_status)rc, err);
+  }
+  if (out_sets) {
+    split_set* arr = (split_set*)malloc(sizeof(split_set) * std::max<size_t>(kept.size(), 1));
+    if (!arr) {
+      for (auto& s : kept) free_split_set_and_associated_clusters(s);
+      return fail(ctx, SWE_ERR_OOM, "split set array");
+    }
+    for (size_t k = 0; k < kept.size(); ++k) arr[k] = kept[k];
+    *out_sets = arr;
+    if (out_n_sets) *out_n_sets = (int)kept.size();
+  } else {
+    for (auto& s : kept) free_split_set_and_associated_clusters(s);
+  }
+  return SWE_OK;
+}
+
+swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsigned* out) {
+  if (!ctx || (!q && qlen > 0) || (!out && ctx->n > 0)) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  if (ctx->n == 0) return SWE_OK;
+  if (qlen > (size_t)(INT_MAX / 8)) return fail(ctx, SWE_ERR_INVALID, "query too long");
+  const int L = (int)qlen;
+  std::vector<uint8_t> qc((size_t)std::max(L, 1) + 15, 0);
+  for (int r = 0; r < L; ++r) qc[r] = (uint8_t)ctx->code_of[(unsigned char)q[r + 1]];
+  CK(ctx->d_q.alloc(qc.size()));
+  CK(ctx->d_out.alloc(ctx->n));
+  long long need_stride = std::min<long long>(L, ctx->max_len) > GEN_CHUNK ? std::max<long long>(L, ctx->max_len) + 1 : 0;
+  int grid = ctx->gen_grid;
+  int* scratch = ctx->d_scratch.p;
+  long long stride = ctx->scratch_stride;
+  if (need_stride > stride) {
+    grid = ctx->num_sms;
+    CK(ctx->d_small_scratch.alloc((size_t)grid * 8 * need_stride));
+    scratch = ctx->d_small_scratch.p;
+    stride = need_stride;
+  }
+  CK(cpy(ctx, ctx->d_q.p, qc.data(), qc.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(ctx->d_ctr.p + 1, 0, sizeof(unsigned), ctx->st));
+  GenParams g{};
+  g.mode = GEN_QUERY;
+  g.codes = ctx->d_codes.p;
+  g.code_off = ctx->d_off.p;
+  g.len = ctx->d_len.p;
+  g.n = ctx->n;
+  g.qcodes = ctx->d_q.p;
+  g.qlen = L;
+  g.out = ctx->d_out.p;
+  g.scratch = scratch;
+  g.scratch_stride = stride;
+  g.nwarps_total = grid * 8;
+  g.status = ctx->d_ctr.p + 1;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_generic(g, grid, ctx->st));
+  CK(cpy(ctx, out, ctx->d_out.p, sizeof(unsigned) * ctx->n, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return SWE_OK;
+}
+
+swe_status swe_score_pairs(swe_ctx* ctx, const int* a, const int* b, int64_t npairs, unsigned* out) {
+  if (!ctx || npairs < 0 || (npairs > 0 && (!a || !b || !out))) return SWE_ERR_INVALID;
+  if (npairs == 0) return SWE_OK;
+  if (swe_status s = select_device(ctx)) return s;
+  std::vector<int2> pr(npairs);
+  for (int64_t k = 0; k < npairs; ++k) {
+    if (a[k] < 0 || a[k] >= ctx->n || b[k] < 0 || b[k] >= ctx->n)
+      return fail(ctx, SWE_ERR_INVALID, "pair index out of range");
+    pr[k] = make_int2(a[k], b[k]);
+  }
+  CK(ctx->d_pairs.alloc(npairs));
+  CK(ctx->d_out.alloc(npairs));
+  CK(cpy(ctx, ctx->d_pairs.p, pr.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice, ctx->st));
+  GenParams g{};
+  g.mode = GEN_PAIRS_OUT;
+  g.codes = ctx->d_codes.p;
+  g.code_off = ctx->d_off.p;
+  g.len = ctx->d_len.p;
+  g.n = ctx->n;
+  g.pairs = ctx->d_pairs.p;
+  g.npairs = npairs;
+  g.out = ctx->d_out.p;
+  g.scratch = ctx->d_scratch.p;
+  g.scratch_stride = ctx->scratch_stride;
+  g.nwarps_total = ctx->gen_grid * 8;
+  g.status = ctx->d_ctr.p + 1;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_generic(g, ctx->gen_grid, ctx->st));
+  CK(cpy(ctx, out, ctx->d_out.p, sizeof(unsigned) * npairs, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return SWE_OK;
+}
+
+swe_status swe_measure_mix_peak(int device, double* cells_per_s, double* lane_instr_per_s) {
+  if (!cells_per_s || !lane_instr_per_s) return SWE_ERR_INVALID;
+  swe_ctx* ctx = nullptr;
+  swe_opts o{};
+  o.device = device;
+  if (swe_status s = swe_create(&ctx, &o)) return s;
+  struct Guard {
+    swe_ctx* c;
+    ~Guard() { swe_destroy(c); }
+  } guard{ctx};
+  const int block = 256, grid = ctx->num_sms * 8, iters = 4096;
+  DevBuf<uint32_t> sink;
+  CK(sink.alloc((size_t)grid * block));
+  CK(launch_mix_probe(sink.p, grid, block, 64, ctx->st));  // warm-up
+  CK(cudaEventRecord(ctx->ev[0], ctx->st));
+  CK(launch_mix_probe(sink.p, grid, block, iters, ctx->st));
+  CK(cudaEventRecord(ctx->ev[1], ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+  const double updates = (double)grid * block * iters * 8.0;  // packed cell updates (8 chains)
+  *cells_per_s = 2.0 * updates / (ms * 1e-3);
+  *lane_instr_per_s = 5.0 * updates / (ms * 1e-3);
+  return SWE_OK;
+}
+
+swe_status swe_timer_start(swe_ctx* ctx) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  CK(cudaEventRecord(ctx->tev[0], ctx->st));
+  return SWE_OK;
+}
+
+swe_status swe_timer_stop(swe_ctx* ctx, double* ms) {
+  if (!ctx || !ms) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  CK(cudaEventRecord(ctx->tev[1], ctx->st));
+  CK(cudaEventSynchronize(ctx->tev[1]));
+  float f = 0;
+  CK(cudaEventElapsedTime(&f, ctx->tev[0], ctx->tev[1]));
+  *ms = f;
+  return SWE_OK;
+}
+
+swe_status swe_get_stats(const swe_ctx* ctx, swe_stats* out) {
+  if (!ctx || !out) return SWE_ERR_INVALID;
+  *out = ctx->stats;
+  return SWE_OK;
+}
+
+}  // extern "C"
+
+namespace swgpu {
+
+long long eps_threshold(float eps) {
+  if (!(eps >= 0.0f)) return -1;  // negative or NaN: not even the point itself
+  if (eps >= 9.0e18f) return LLONG_MAX / 2;
+  return (long long)std::floor((double)eps);
+}
+
+// Distance of one pair of raw strings (the drop-in score()); codes are the
+// raw bytes, which keeps equality exact without a code table.
+swe_status score_raw(swe_ctx* ctx, const char* A, size_t la, const char* B, size_t lb, unsigned* out) {
+  if (!ctx || !out || (!A && la) || (!B && lb)) return SWE_ERR_INVALID;
+  if (la > (size_t)(INT_MAX / 8) || lb > (size_t)(INT_MAX / 8)) return fail(ctx, SWE_ERR_INVALID, "too long");
+  if (swe_status s = select_device(ctx)) return s;
+  const int64_t oa = 0, ob = ((int64_t)la + 15) & ~int64_t(15);
+  std::vector<uint8_t> buf((size_t)(ob + lb + 16), 0);
+  for (size_t r = 0; r < la; ++r) buf[oa + r] = (uint8_t)A[r + 1];
+  for (size_t r = 0; r < lb; ++r) buf[ob + r] = (uint8_t)B[r + 1];
+  const int64_t offs[2] = {oa, ob};
+  const int lens[2] = {(int)la, (int)lb};
+  const int2 pr = make_int2(0, 1);
+  CK(ctx->d_q.alloc(buf.size()));
+  CK(ctx->d_small_off.alloc(2));
+  CK(ctx->d_small_len.alloc(2));
+  CK(ctx->d_pairs.alloc(1));
+  CK(ctx->d_out.alloc(1));
+  const long long need = std::min(la, lb) > (size_t)GEN_CHUNK ? (long long)std::max(la, lb) + 1 : 1;
+  CK(ctx->d_small_scratch.alloc((size_t)8 * need));
+  CK(cpy(ctx, ctx->d_q.p, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->st));
+  CK(cpy(ctx, ctx->d_small_off.p, offs, sizeof(offs), cudaMemcpyHostToDevice, ctx->st));
+  CK(cpy(ctx, ctx->d_small_len.p, lens, sizeof(lens), cudaMemcpyHostToDevice, ctx->st));
+  CK(cpy(ctx, ctx->d_pairs.p, &pr, sizeof(pr), cudaMemcpyHostToDevice, ctx->st));
+  GenParams g{};
+  g.mode = GEN_PAIRS_OUT;
+  g.codes = ctx->d_q.p;
+  g.code_off = ctx->d_small_off.p;
+  g.len = ctx->d_small_len.p;
+  g.n = 2;
+  g.pairs = ctx->d_pairs.p;
+  g.npairs = 1;
+  g.out = ctx->d_out.p;
+  g.scratch = ctx->d_small_scratch.p;
+  g.scratch_stride = need;
+  g.nwarps_total = 8;
+  g.status = ctx->d_ctr.p + 1;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_generic(g, 1, ctx->st));
+  CK(cpy(ctx, out, ctx->d_out.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return SWE_OK;
+}
+
+}  // namespace swgpu

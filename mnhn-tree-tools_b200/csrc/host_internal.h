@@ -1,0 +1,49 @@
+// Host-side pieces shared by the engine, the adaptive driver and the drop-in
+// layer.  No CUDA types here.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "mnhn_dropin.h"
+#include "swgpu.h"
+
+namespace swgpu {
+
+// Integer form of the reference's neighbour test (float)d <= eps
+// (dbscan.c:548-551): d <= T with T = floor(eps) for eps >= 0, and no
+// neighbour at all (T = -1) for negative or NaN eps.  Exact while d < 2^24.
+long long eps_threshold(float eps);
+
+// Order-faithful replay of dbscan_SW (dbscan.c:950-1047, expand_cluster
+// dbscan.c:783-948) over per-point neighbour bitmaps: bit k of row i is set
+// iff k is an eps-neighbour of i; counts[i] is the popcount of row i.
+// The split set is malloc'd reference-style.  Returns 0 or SWE_ERR_OOM.
+int dbscan_replay_bitmap(int n, const uint64_t* bits, int words_per_row, const int* counts, int minpts,
+                         split_set* out);
+
+// One DBSCAN run at eps (split set malloc'd); returns an swe_status.
+using DbscanFn = std::function<int(float eps, split_set* out)>;
+
+// Adaptive sweep of dbscan.c:1117-1380 over a DBSCAN provider.  `fixed_point`
+// (when >= 0) is a threshold at or above which every eps gives the same
+// result, used to stop sweeps that could never reach one cluster (the
+// reference loops forever there).  Kept layers are returned in `kept`
+// (ownership passes to the caller).
+int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
+                   const DbscanFn& fn, long long fixed_point, std::vector<split_set>* kept,
+                   std::string* err);
+
+// FASTA loading with dataset_from_fasta semantics (dataset.c:264-344).
+int fasta_read(FILE* in, dataset* out, std::string* err);
+
+// Distance of one pair of raw strings on the GPU (the drop-in score()).
+swe_status score_raw(swe_ctx* ctx, const char* A, size_t la, const char* B, size_t lb, unsigned* out);
+
+// The eps printed for kept layer i (dbscan.c:1323-1324):
+// epsilon_start + (i+1) * (float)epsilon_inc, evaluated in float.
+float layer_eps(float eps_start, int i, float eps_inc);
+
+}  // namespace swgpu

@@ -1,0 +1,530 @@
+// Smith-Waterman distance kernels for B200 (sm_100a).
+//
+// Scoring follows the reference exactly (smith-waterman.c:16-80): linear gap
+// 3, +4 on symbol equality, -4 otherwise, local floor 0, and the distance
+// 4*max(len_a, len_b) - max H.  Sequences arrive as "effective" symbol codes:
+// position r holds the reference's A[r+1] (the first base never takes part and
+// the terminating NUL does, smith-waterman.c:56-58).
+//
+// Kernels:
+//   fast_all_pairs_kernel  packed 16x2 warp wavefront (two row sequences per
+//                          lane word, one column sequence per lane segment),
+//                          persistent over a cost-ordered tile list;
+//   generic_kernel         32-bit warp wavefront, one pair per warp, any
+//                          length (512-column chunks) and any symbol;
+//   bitmap_kernel          eps threshold of the distance matrix into a
+//                          neighbour bitmap plus per-row counts;
+//   csr_fill_kernel        bitmap -> ascending CSR column lists.
+#include "sw_device.cuh"
+#include "sw_kernels.cuh"
+
+namespace swgpu {
+
+// ---------------------------------------------------------------------------
+// 16x2 wavefront over one column sequence (a lane segment of `lpb` lanes).
+//
+// Lane li of the segment owns columns [li*W, li*W+W) of the column sequence B
+// and, at step s, computes row g = s - li of the row stream (two row
+// sequences per 16-bit half, packs back to back).  Its left boundary arrives
+// from lane li-1 by shuffle; the diagonal boundary is the left boundary of the
+// previous step.  Per cell (d = s + 3 from the PRMT table):
+//   v = max(H[i-1][j-1] + d, max(H[i][j-1], H[i-1][j]))
+//   H = max(v - 3, 0)
+// which is max(0, diag + s, left - 3, up - 3).  Pad columns (beyond len B)
+// and pad rows (code 7) only ever see mismatches, so they can never raise
+// the maximum above the real cells' maximum.
+// ---------------------------------------------------------------------------
+template <int W>
+__device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, int total_rows,
+                                             const int* __restrict__ pstart, int npk,
+                                             const uint8_t* __restrict__ bcodes, int lenB, int lpb,
+                                             int li, unsigned* __restrict__ smax) {
+  uint32_t tlo[W], thi[W], H[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const int col = li * W + k;
+    const int c = (col < lenB) ? (int)bcodes[col] : 0xFF;
+    uint32_t lo = 0xFFFFFFFFu, hi = 0xFFFFFFFFu;  // -1 (mismatch: -4 + 3)
+    if (c < 4) lo ^= (0xF8u << (8 * c));           // 0x07 (match: +4 + 3)
+    else if (c < 8) hi ^= (0xF8u << (8 * (c - 4)));
+    tlo[k] = lo;
+    thi[k] = hi;
+    H[k] = 0u;
+  }
+  const uint32_t M3 = 0xFFFDFFFDu;  // -3 in both halves
+  uint32_t mx = 0u, last = 0u, diag = 0u;
+  int pk = -1, next = 0;
+  const uint32_t lmask = li ? 0xFFFFFFFFu : 0u;
+  const int steps = total_rows + lpb;
+  const uint16_t* sp = sel0 - li;
+  for (int s = 0; s < steps; ++s) {
+    const uint32_t left = __shfl_up_sync(0xFFFFFFFFu, last, 1, lpb) & lmask;
+    const int g = s - li;
+    if (g == next) {  // first row of a new pack (or the end of the stream)
+      if (pk >= 0) {
+        atomicMax(&smax[2 * pk], mx & 0xFFFFu);
+        atomicMax(&smax[2 * pk + 1], mx >> 16);
+      }
+      ++pk;
+      mx = 0u;
+      diag = 0u;
+#pragma unroll
+      for (int k = 0; k < W; ++k) H[k] = 0u;
+      next = (pk < npk) ? pstart[pk + 1] : 0x7FFFFFFF;
+    }
+    const uint32_t sel = sp[s];
+    uint32_t hd = diag;
+    uint32_t x = vmax0(left, H[0]);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const uint32_t d = prmt(tlo[k], thi[k], sel);
+      const uint32_t v = vaddmax(hd, d, x);
+      const uint32_t h = vaddmax0(v, M3, 0u);
+      if (k + 1 < W) x = vaddmax0(v, M3, H[k + 1]);
+      hd = H[k];
+      H[k] = h;
+      mx = vmax0(mx, h);
+    }
+    last = H[W - 1];
+    diag = left;
+  }
+}
+
+__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline size_t fast_sel_bytes(int max_block_rows) {
+  return ((size_t)(32 + max_block_rows + 40) * 2 + 15) & ~(size_t)15;
+}
+
+size_t fast_smem_bytes(int max_block_rows, int max_cols_per_cta, int packs_per_block) {
+  return fast_sel_bytes(max_block_rows) + (size_t)max_cols_per_cta * packs_per_block * 2 * 4 +
+         (size_t)(packs_per_block + 1) * 4 + 16;
+}
+
+template <int W>
+__device__ __forceinline__ void fast_dispatch_one(const uint16_t* sel0, int rows, const int* pstart,
+                                                  int npk, const uint8_t* bc, int lenB, int lpb,
+                                                  int li, unsigned* smax) {
+  fast_segment<W>(sel0, rows, pstart, npk, bc, lenB, lpb, li, smax);
+}
+
+__device__ __noinline__ void fast_dispatch(int W, const uint16_t* sel0, int rows, const int* pstart,
+                                           int npk, const uint8_t* bc, int lenB, int lpb, int li,
+                                           unsigned* smax) {
+  switch (W) {
+#define SWGPU_CASE(w) \
+  case w: fast_dispatch_one<w>(sel0, rows, pstart, npk, bc, lenB, lpb, li, smax); break;
+    SWGPU_CASE(1) SWGPU_CASE(2) SWGPU_CASE(3) SWGPU_CASE(4) SWGPU_CASE(5) SWGPU_CASE(6)
+    SWGPU_CASE(7) SWGPU_CASE(8) SWGPU_CASE(9) SWGPU_CASE(10) SWGPU_CASE(11) SWGPU_CASE(12)
+    SWGPU_CASE(13) SWGPU_CASE(14) SWGPU_CASE(15) SWGPU_CASE(16) SWGPU_CASE(17) SWGPU_CASE(18)
+    SWGPU_CASE(19) SWGPU_CASE(20) SWGPU_CASE(21) SWGPU_CASE(22) SWGPU_CASE(23) SWGPU_CASE(24)
+#undef SWGPU_CASE
+    default: break;
+  }
+}
+
+__global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_tile;
+  __shared__ int s_ok;
+  const int PB = p.packs_per_block;
+  uint16_t* s_sel = reinterpret_cast<uint16_t*>(smem);
+  unsigned* s_max = reinterpret_cast<unsigned*>(smem + fast_sel_bytes(p.max_block_rows));
+  int* s_pstart = reinterpret_cast<int*>(s_max + (size_t)p.max_cols_per_cta * PB * 2);
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = bd >> 5;
+
+  if (tid == 0) mbar_init(&bar, 1);
+  for (int i = tid; i < 32; i += bd) s_sel[i] = SEL_PAD;
+  __syncthreads();
+  uint32_t phase = 0;
+
+  for (;;) {
+    if (tid == 0) s_tile = (int)atomicAdd(p.tile_counter, 1u);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= p.ntiles) break;
+    const FastTile tile = p.tiles[t];
+    const int W = tile.wl & 0xFF, lpb = tile.wl >> 8;
+    const int pk0 = tile.q * PB;
+    const int npk = min(PB, p.npacks - pk0);
+    bool bad = (W < 1 || W > FAST_MAX_W || (lpb != 8 && lpb != 16 && lpb != 32) || npk <= 0 ||
+                tile.nb < 1 || tile.nb > p.max_cols_per_cta || tile.nb > nwarps * (32 / max(lpb, 1)));
+    int row0 = 0, rows = 0, rows8 = 0;
+    if (!bad) {
+      row0 = p.pack_row_off[pk0];
+      rows = p.pack_row_off[pk0 + npk - 1] + p.pack_rows[pk0 + npk - 1] - row0;
+      rows8 = (rows + 7) & ~7;
+      bad = rows8 > p.max_block_rows || (row0 & 7) != 0;
+    }
+    if (bad) {
+      if (tid == 0) atomicOr(p.status, KST_BAD_TILE);
+      __syncthreads();
+      continue;
+    }
+    // test hook: tile 0's copy is never issued, so nothing completes its phase
+    const bool skip_copy = p.inject_timeout && t == 0;
+    if (tid == 0 && !skip_copy) {
+      // order earlier generic-proxy reads of s_sel before the async-proxy write
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_expect_tx(&bar, (uint32_t)rows8 * 2u);
+      bulk_g2s(s_sel + 32, p.sel + row0, (uint32_t)rows8 * 2u, &bar);
+    }
+    for (int i = tid; i <= npk; i += bd)
+      s_pstart[i] = (i < npk ? p.pack_row_off[pk0 + i] : row0 + rows) - row0;
+    for (int i = tid; i < tile.nb * npk * 2; i += bd) s_max[i] = 0u;
+    if (tid == 0) {
+      bool ok = mbar_wait_bounded(&bar, phase, p.wait_limit);
+      if (!ok) {
+        atomicOr(p.status, KST_TIMEOUT);
+        if (!skip_copy) mbar_wait_bounded(&bar, phase, p.wait_limit);  // let the copy in flight land
+      }
+      s_ok = ok ? 1 : 0;
+    }
+    phase ^= 1u;
+    __syncthreads();
+    if (!s_ok) return;
+    for (int i = tid; i < 40; i += bd) s_sel[32 + rows + i] = SEL_PAD;
+    __syncthreads();
+
+    const int spw = 32 / lpb;  // column sequences per warp
+    if (warp * spw < tile.nb) {
+      const int j = min(warp * spw + lane / lpb, tile.nb - 1);  // idle segments repeat the last one
+      const int b = p.order[tile.b0 + j];
+      fast_dispatch(W, s_sel + 32, rows, s_pstart, npk, p.codes + p.code_off[b], p.len[b], lpb,
+                    lane % lpb, s_max + (size_t)j * npk * 2);
+    }
+    __syncthreads();
+
+    // epilogue: distances of this tile's pairs
+    for (int i = tid; i < tile.nb * npk * 2; i += bd) {
+      const int j = i / (npk * 2);
+      const int r = i - j * npk * 2;
+      const int apos = (pk0 + (r >> 1)) * 2 + (r & 1);
+      if (apos >= p.nfast) continue;
+      const int a = p.order[apos], b = p.order[tile.b0 + j];
+      const unsigned m = s_max[i];
+      if ((int)m >= p.sat_limit) {
+        const unsigned slot = atomicAdd(p.rerun_count, 1u);
+        if (slot < p.rerun_cap) p.rerun[slot] = make_int2(a, b);
+        else atomicOr(p.status, KST_RERUN_OVERFLOW);
+        continue;
+      }
+      const unsigned d = 4u * (unsigned)max(p.len[a], p.len[b]) - m;
+      const size_t ab = (size_t)a * (size_t)p.n + (size_t)b;
+      const size_t ba = (size_t)b * (size_t)p.n + (size_t)a;
+      if (p.D16) {
+        p.D16[ab] = (uint16_t)d;
+        p.D16[ba] = (uint16_t)d;
+      } else {
+        p.D32[ab] = d;
+        p.D32[ba] = d;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t fast_set_smem_limit(size_t bytes) {
+  return cudaFuncSetAttribute(fast_all_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
+}
+
+int fast_occupancy(int block, size_t smem) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fast_all_pairs_kernel, block, smem) !=
+      cudaSuccess)
+    return 0;
+  return nb;
+}
+
+cudaError_t launch_fast(const FastParams& p, int grid, int block, size_t smem, cudaStream_t st) {
+  fast_all_pairs_kernel<<<grid, block, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Row selector stream: one 16-bit PRMT selector per row of each pack.
+// ---------------------------------------------------------------------------
+__global__ void build_sel_kernel(const uint8_t* __restrict__ codes, const int64_t* __restrict__ code_off,
+                                 const int* __restrict__ len, const int* __restrict__ order, int nfast,
+                                 const int* __restrict__ pack_row_off, int npacks, uint16_t* sel) {
+  for (int pk = blockIdx.x; pk < npacks; pk += gridDim.x) {
+    const int pa = 2 * pk, pb = 2 * pk + 1;
+    const int a = order[pa];
+    const int b = pb < nfast ? order[pb] : -1;
+    const int la = len[a], lb = b >= 0 ? len[b] : 0;
+    const uint8_t* ca = codes + code_off[a];
+    const uint8_t* cb = b >= 0 ? codes + code_off[b] : nullptr;
+    const int r0 = pack_row_off[pk], r1 = pack_row_off[pk + 1];
+    for (int r = threadIdx.x; r < r1 - r0; r += blockDim.x) {
+      const int x = r < la ? (int)ca[r] : CODE_ROWPAD;
+      const int y = r < lb ? (int)cb[r] : CODE_ROWPAD;
+      sel[r0 + r] = make_sel(x, y);
+    }
+  }
+}
+
+cudaError_t launch_build_sel(const uint8_t* codes, const int64_t* code_off, const int* len,
+                             const int* order, int nfast, const int* pack_row_off, int npacks,
+                             uint16_t* sel, cudaStream_t st) {
+  if (npacks <= 0) return cudaSuccess;
+  build_sel_kernel<<<min(npacks, 65535), 128, 0, st>>>(codes, code_off, len, order, nfast, pack_row_off,
+                                                       npacks, sel);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Generic 32-bit warp wavefront (one pair per warp, 512-column chunks).
+// ---------------------------------------------------------------------------
+__device__ int sw32_warp(const uint8_t* __restrict__ A, int la, const uint8_t* __restrict__ B, int lb,
+                         int* __restrict__ scratch, int lane) {
+  int mx = 0;
+  const int nchunks = lb > 0 ? (lb + GEN_CHUNK - 1) / GEN_CHUNK : 0;
+  for (int c = 0; c < nchunks; ++c) {
+    const int c0 = c * GEN_CHUNK;
+    int bc[GEN_W], H[GEN_W];
+#pragma unroll
+    for (int k = 0; k < GEN_W; ++k) {
+      const int col = c0 + lane * GEN_W + k;
+      bc[k] = col < lb ? (int)B[col] : 0x1FF;  // never equal to a row code
+      H[k] = 0;
+    }
+    const bool first = (c == 0), lastchunk = (c == nchunks - 1);
+    int last = 0, diag = 0;
+    for (int s = 0; s < la + 32; ++s) {
+      int left = __shfl_up_sync(0xFFFFFFFFu, last, 1);
+      const int r = s - lane;
+      const bool live = (r >= 0 && r < la);
+      if (lane == 0) left = (first || !live) ? 0 : scratch[r];
+      const int a = live ? (int)A[r] : 0x2FF;
+      int hd = diag;
+      int x = __vimax_s32_relu(left, H[0]);
+#pragma unroll
+      for (int k = 0; k < GEN_W; ++k) {
+        const int d = (a == bc[k]) ? 7 : -1;
+        const int v = __viaddmax_s32(hd, d, x);
+        const int h = __viaddmax_s32_relu(v, -3, 0);
+        if (k + 1 < GEN_W) x = __viaddmax_s32_relu(v, -3, H[k + 1]);
+        hd = H[k];
+        H[k] = h;
+        mx = max(mx, h);
+      }
+      last = H[GEN_W - 1];
+      if (lane == 31 && !lastchunk && live) scratch[r] = last;
+      diag = left;
+    }
+    __syncwarp();
+  }
+  return __reduce_max_sync(0xFFFFFFFFu, mx);
+}
+
+__global__ void __launch_bounds__(256) generic_kernel(GenParams p) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  long long total = 0;
+  if (p.mode == GEN_PAIRS || p.mode == GEN_PAIRS_OUT)
+    total = p.npairs_dev ? (long long)*p.npairs_dev : p.npairs;
+  else if (p.mode == GEN_EXC_CROSS)
+    total = (long long)p.nexc * p.n;
+  else
+    total = p.n;
+  int* scratch = p.scratch ? p.scratch + (long long)gw * p.scratch_stride : nullptr;
+  for (long long w = gw; w < total; w += p.nwarps_total) {
+    int ia = -1, ib = -1;
+    const uint8_t *A, *B;
+    int la, lb;
+    if (p.mode == GEN_PAIRS || p.mode == GEN_PAIRS_OUT) {
+      const int2 pr = p.pairs[w];
+      ia = pr.x;
+      ib = pr.y;
+    } else if (p.mode == GEN_EXC_CROSS) {
+      ia = p.exc[w / p.n];
+      ib = (int)(w % p.n);
+      if (p.is_exc[ib] && ib < ia) continue;  // that pair belongs to row ib
+    } else {
+      ib = (int)w;
+    }
+    if (p.mode == GEN_QUERY) {
+      A = p.qcodes;
+      la = p.qlen;
+    } else {
+      A = p.codes + p.code_off[ia];
+      la = p.len[ia];
+    }
+    B = p.codes + p.code_off[ib];
+    lb = p.len[ib];
+    // keep the shorter sequence on the column side (fewer chunks)
+    const uint8_t* R = A;
+    const uint8_t* Cc = B;
+    int lr = la, lc = lb;
+    if (lc > lr) {
+      R = B;
+      Cc = A;
+      lr = lb;
+      lc = la;
+    }
+    const int best = sw32_warp(R, lr, Cc, lc, scratch, lane);
+    if (lane == 0) {
+      const unsigned d = 4u * (unsigned)max(la, lb) - (unsigned)best;
+      if (p.mode == GEN_QUERY || p.mode == GEN_PAIRS_OUT) {
+        p.out[w] = d;
+      } else {
+        const size_t ab = (size_t)ia * (size_t)p.n + (size_t)ib;
+        const size_t ba = (size_t)ib * (size_t)p.n + (size_t)ia;
+        if (p.D16) {
+          p.D16[ab] = (uint16_t)d;
+          p.D16[ba] = (uint16_t)d;
+        } else {
+          p.D32[ab] = d;
+          p.D32[ba] = d;
+        }
+      }
+    }
+  }
+}
+
+cudaError_t launch_generic(const GenParams& p, int grid, cudaStream_t st) {
+  generic_kernel<<<grid, 256, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+__global__ void diag_kernel(uint16_t* D16, uint32_t* D32, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const size_t k = (size_t)i * (size_t)n + (size_t)i;
+    if (D16) D16[k] = 0;
+    else D32[k] = 0u;
+  }
+}
+
+cudaError_t launch_diag(uint16_t* D16, uint32_t* D32, int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  diag_kernel<<<min((n + 255) / 256, 4096), 256, 0, st>>>(D16, D32, n);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Neighbour bitmap: one warp per row, 2048 columns per iteration.
+// ---------------------------------------------------------------------------
+template <typename DT>
+__global__ void __launch_bounds__(256) bitmap_kernel(const DT* __restrict__ D, int n, long long T,
+                                                     uint64_t* __restrict__ bits, int wpr,
+                                                     int* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    const DT* row = D + (size_t)i * (size_t)n;
+    uint64_t* out = bits + (size_t)i * (size_t)wpr;
+    int cnt = 0;
+    for (int base = 0; base < n; base += 2048) {
+      uint64_t mine = 0;
+      uint32_t lo = 0;
+#pragma unroll 4
+      for (int j = 0; j < 64; ++j) {
+        const int col = base + 32 * j + lane;
+        const bool v = col < n && (long long)row[col] <= T;
+        const uint32_t b = __ballot_sync(0xFFFFFFFFu, v);
+        if ((j & 1) == 0) {
+          lo = b;
+        } else if (lane == (j >> 1)) {
+          mine = (uint64_t)lo | ((uint64_t)b << 32);
+        }
+      }
+      const int w = (base >> 6) + lane;
+      if (w < wpr) out[w] = mine;
+      cnt += __popcll(mine);
+    }
+    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+    if (lane == 0) counts[i] = cnt;
+  }
+}
+
+cudaError_t launch_bitmap(const uint16_t* D16, const uint32_t* D32, int n, long long T, uint64_t* bits,
+                          int words_per_row, int* counts, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int grid = min((n + 7) / 8, 148 * 16);
+  if (D16) bitmap_kernel<uint16_t><<<grid, 256, 0, st>>>(D16, n, T, bits, words_per_row, counts);
+  else bitmap_kernel<uint32_t><<<grid, 256, 0, st>>>(D32, n, T, bits, words_per_row, counts);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) csr_fill_kernel(const uint64_t* __restrict__ bits, int n, int wpr,
+                                                       const long long* __restrict__ row_ptr,
+                                                       int* __restrict__ cols) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    long long pos = row_ptr[i];
+    const uint64_t* rb = bits + (size_t)i * (size_t)wpr;
+    for (int w0 = 0; w0 < wpr; w0 += 32) {
+      const int w = w0 + lane;
+      uint64_t word = w < wpr ? rb[w] : 0ull;
+      const int c = __popcll(word);
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      long long q = pos + incl - c;
+      while (word) {
+        const int bit = __ffsll((long long)word) - 1;
+        cols[q++] = w * 64 + bit;
+        word &= word - 1;
+      }
+      pos += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    }
+  }
+}
+
+cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, const long long* row_ptr,
+                            int* cols, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int grid = min((n + 7) / 8, 148 * 16);
+  csr_fill_kernel<<<grid, 256, 0, st>>>(bits, n, words_per_row, row_ptr, cols);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Instruction-mix probe: the per-cell sequence of fast_segment (PRMT, three
+// add-max, one max) on 8 independent chains per thread, so that issue rate,
+// not latency, limits it.  Writes one word per thread so nothing is elided.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) mix_probe_kernel(uint32_t* sink, int iters) {
+  constexpr int C = 8;
+  const uint32_t t = threadIdx.x + blockIdx.x * blockDim.x;
+  uint32_t h[C], x[C], m[C];
+  const uint32_t tlo = 0xFF07FFFFu ^ t, thi = 0xFFFF07FFu + t;
+  uint32_t sel = make_sel(t & 3, (t >> 2) & 3);
+  const uint32_t M3 = 0xFFFDFFFDu;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    h[c] = (t * (c + 3)) & 0x00FF00FFu;
+    x[c] = (t * (c + 7)) & 0x00FF00FFu;
+    m[c] = 0u;
+  }
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const uint32_t d = prmt(tlo, thi, sel);
+      const uint32_t v = vaddmax(h[c], d, x[c]);
+      const uint32_t hn = vaddmax0(v, M3, 0u);
+      x[c] = vaddmax0(v, M3, h[c]);
+      h[c] = hn;
+      m[c] = vmax0(m[c], hn);
+    }
+    sel ^= 0x0101u;
+  }
+  uint32_t acc = 0;
+#pragma unroll
+  for (int c = 0; c < C; ++c) acc ^= m[c] ^ h[c] ^ x[c];
+  sink[t] = acc;
+}
+
+cudaError_t launch_mix_probe(uint32_t* sink, int grid, int block, int iters, cudaStream_t st) {
+  mix_probe_kernel<<<grid, block, 0, st>>>(sink, iters);
+  return cudaGetLastError();
+}
+
+}  // namespace swgpu

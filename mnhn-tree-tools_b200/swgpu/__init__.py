@@ -1,0 +1,324 @@
+"""ctypes binding to libswgpu.so, the B200 engine for MNHN-Tree-Tools'
+all-pairs Smith-Waterman neighbourhood path.
+
+The library is C (include/swgpu.h, include/mnhn_dropin.h); this module is a
+thin host-side wrapper for tests, benchmarks and Python callers.  Every call
+goes to the CUDA path; nothing here computes a distance on the CPU.  Calls
+raise ``SwgpuError`` carrying the C status when the library reports one, and
+importing fails loudly when the shared library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+PKG_ROOT = Path(__file__).resolve().parent.parent          # mnhn-tree-tools_b200/
+LIB_PATH = PKG_ROOT / "lib" / "libswgpu.so"
+BIN_DIR = PKG_ROOT / "bin"
+INCLUDE_DIR = PKG_ROOT.parent / "include"
+
+STATUS = {0: "SWE_OK", 1: "SWE_ERR_INVALID", 2: "SWE_ERR_CUDA", 3: "SWE_ERR_OOM",
+          4: "SWE_ERR_NO_DEVICE", 5: "SWE_ERR_TIMEOUT", 6: "SWE_ERR_RERUN", 7: "SWE_ERR_STATE",
+          8: "SWE_ERR_IO", 9: "SWE_ERR_SWEEP"}
+
+
+class SwgpuError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def build(force: bool = False) -> None:
+    """Compile libswgpu.so and the command-line tools (nvcc, sm_100a)."""
+    if force or not LIB_PATH.exists():
+        subprocess.run(["make", "-s", "-j8", "-C", str(PKG_ROOT)], check=True)
+
+
+# ---------------------------------------------------------------------------
+# structures (include/mnhn_types.h, include/swgpu.h)
+# ---------------------------------------------------------------------------
+class Dataset(C.Structure):
+    _fields_ = [("sequences", C.POINTER(C.c_char_p)), ("sequence_lengths", C.POINTER(C.c_size_t)),
+                ("binary_sequences", C.c_void_p), ("n_values", C.c_int), ("values", C.c_void_p),
+                ("n_dimensions", C.c_int), ("max_sequence_length", C.c_size_t)]
+
+
+class Cluster(C.Structure):
+    _fields_ = [("members", C.POINTER(C.c_int)), ("n_members", C.c_int), ("id", C.c_int)]
+
+
+class SplitSet(C.Structure):
+    _fields_ = [("n_clusters", C.c_int), ("clusters", C.POINTER(Cluster))]
+
+
+class Opts(C.Structure):
+    _fields_ = [("device", C.c_int), ("sat_limit", C.c_int), ("packs_per_block", C.c_int),
+                ("threads", C.c_int), ("inject_timeout", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_sequences", C.c_int64), ("n_fast", C.c_int64), ("n_exceptional", C.c_int64),
+                ("unique_pairs", C.c_int64), ("cells", C.c_double), ("tile_cells", C.c_double),
+                ("reruns", C.c_int64), ("n_tiles", C.c_int64), ("ms_score_pass", C.c_double),
+                ("ms_fast_kernel", C.c_double), ("ms_last_neighbors", C.c_double),
+                ("dist_bytes", C.c_int), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+                ("kernel_launches", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+DBSCANNER = C.CFUNCTYPE(SplitSet, Dataset, C.c_float, C.c_int)
+
+# Every symbol the public headers declare (checked by the CPU test suite).
+EXPORTS = [
+    # include/swgpu.h
+    "swe_strerror", "swe_create", "swe_destroy", "swe_last_error", "swe_upload",
+    "swe_score_all_pairs", "swe_copy_distances", "swe_neighbors", "swe_dbscan", "swe_adaptive",
+    "swe_score_one_to_many", "swe_score_pairs", "swe_get_stats", "swe_free", "swe_dbscan_bitmap",
+    "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop",
+    # include/mnhn_dropin.h
+    "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
+    "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
+    "data_not_in_clusters", "intersection_of_clusters", "generate_split_set_relation",
+    "free_split_set_and_associated_clusters", "swgpu_last_dropin_status",
+]
+
+_lib = None
+
+
+def lib():
+    """Load libswgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {PKG_ROOT}`")
+        L = C.CDLL(str(LIB_PATH))
+        L.swe_strerror.restype = C.c_char_p
+        L.swe_strerror.argtypes = [C.c_int]
+        L.swe_create.restype = C.c_int
+        L.swe_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Opts)]
+        L.swe_destroy.argtypes = [C.c_void_p]
+        L.swe_last_error.restype = C.c_char_p
+        L.swe_last_error.argtypes = [C.c_void_p]
+        L.swe_upload.restype = C.c_int
+        L.swe_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.swe_score_all_pairs.restype = C.c_int
+        L.swe_score_all_pairs.argtypes = [C.c_void_p]
+        L.swe_copy_distances.restype = C.c_int
+        L.swe_copy_distances.argtypes = [C.c_void_p, C.c_void_p]
+        L.swe_neighbors.restype = C.c_int
+        L.swe_neighbors.argtypes = [C.c_void_p, C.c_float, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.swe_dbscan.restype = C.c_int
+        L.swe_dbscan.argtypes = [C.c_void_p, C.c_float, C.c_int, C.POINTER(SplitSet)]
+        L.swe_adaptive.restype = C.c_int
+        L.swe_adaptive.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_void_p,
+                                   C.POINTER(C.POINTER(SplitSet)), C.POINTER(C.c_int)]
+        L.swe_score_one_to_many.restype = C.c_int
+        L.swe_score_one_to_many.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p]
+        L.swe_score_pairs.restype = C.c_int
+        L.swe_score_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.swe_get_stats.restype = C.c_int
+        L.swe_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.swe_free.argtypes = [C.c_void_p]
+        L.swe_measure_mix_peak.restype = C.c_int
+        L.swe_measure_mix_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.swe_timer_start.restype = C.c_int
+        L.swe_timer_start.argtypes = [C.c_void_p]
+        L.swe_timer_stop.restype = C.c_int
+        L.swe_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.swe_dbscan_bitmap.restype = C.c_int
+        L.swe_dbscan_bitmap.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(SplitSet)]
+        L.score.restype = C.c_uint
+        L.score.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, C.c_size_t, C.c_void_p]
+        L.dbscan_SW.restype = SplitSet
+        L.dbscan_SW.argtypes = [Dataset, C.c_float, C.c_int]
+        L.adaptive_dbscan.restype = None
+        L.adaptive_dbscan.argtypes = [C.c_void_p, Dataset, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_int]
+        L.free_split_set_and_associated_clusters.argtypes = [SplitSet]
+        L.store_split_set.argtypes = [C.c_char_p, SplitSet]
+        L.read_split_set.restype = SplitSet
+        L.read_split_set.argtypes = [C.c_char_p]
+        L.swgpu_last_dropin_status.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(st: int, ctx=None):
+    if st != 0:
+        msg = lib().swe_last_error(ctx).decode() if ctx else ""
+        raise SwgpuError(st, msg)
+
+
+def split_set_to_lists(s: SplitSet):
+    return [[s.clusters[c].members[k] for k in range(s.clusters[c].n_members)]
+            for c in range(s.n_clusters)]
+
+
+class SeqBuffer:
+    """Sequences held as NUL-terminated C buffers (kept alive with the object)."""
+
+    def __init__(self, seqs):
+        self.bufs = [C.create_string_buffer(bytes(s), len(s) + 1) for s in seqs]
+        self.n = len(seqs)
+        self.ptrs = (C.c_char_p * max(1, self.n))(*[C.addressof(b) for b in self.bufs])
+        self.lens = (C.c_size_t * max(1, self.n))(*[len(s) for s in seqs])
+
+    def dataset(self) -> Dataset:
+        mx = max((len(b) - 1 for b in self.bufs), default=0)
+        return Dataset(C.cast(self.ptrs, C.POINTER(C.c_char_p)), C.cast(self.lens, C.POINTER(C.c_size_t)),
+                       None, self.n, None, 0, mx)
+
+
+class Engine:
+    """One engine context (one CUDA stream on one device)."""
+
+    def __init__(self, device: int = 0, sat_limit: int = 0, packs_per_block: int = 0, threads: int = 0,
+                 inject_timeout: int = 0):
+        self.ctx = C.c_void_p()
+        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout)
+        _check(lib().swe_create(C.byref(self.ctx), C.byref(opts)))
+        self.n = 0
+        self._buf = None
+
+    def close(self):
+        if self.ctx:
+            lib().swe_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, seqs):
+        self._buf = SeqBuffer(seqs)
+        _check(lib().swe_upload(self.ctx, self._buf.ptrs, self._buf.lens, self._buf.n), self.ctx)
+        self.n = self._buf.n
+
+    def score_all_pairs(self):
+        _check(lib().swe_score_all_pairs(self.ctx), self.ctx)
+
+    def distances(self) -> np.ndarray:
+        out = np.zeros((self.n, self.n), dtype=np.uint32)
+        _check(lib().swe_copy_distances(self.ctx, out.ctypes.data), self.ctx)
+        return out
+
+    def neighbors(self, eps: float):
+        rp, cols = C.c_void_p(), C.c_void_p()
+        _check(lib().swe_neighbors(self.ctx, C.c_float(eps), C.byref(rp), C.byref(cols)), self.ctx)
+        row_ptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int64)), shape=(self.n + 1,)).copy()
+        E = int(row_ptr[-1])
+        c = (np.ctypeslib.as_array(C.cast(cols, C.POINTER(C.c_int32)), shape=(max(E, 1),))[:E].copy()
+             if E else np.zeros(0, dtype=np.int32))
+        lib().swe_free(rp)
+        lib().swe_free(cols)
+        return row_ptr, c
+
+    def dbscan(self, eps: float, minpts: int):
+        s = SplitSet()
+        _check(lib().swe_dbscan(self.ctx, C.c_float(eps), minpts, C.byref(s)), self.ctx)
+        out = split_set_to_lists(s)
+        lib().free_split_set_and_associated_clusters(s)
+        return out
+
+    def adaptive(self, eps_start: float, eps_inc: float, minpts: int, prefix: str | None = None,
+                 log_path: str | None = None):
+        """Runs the sweep; returns (log text, kept split sets as lists)."""
+        libc = C.CDLL(None)
+        libc.fopen.restype = C.c_void_p
+        libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+        libc.fclose.argtypes = [C.c_void_p]
+        import tempfile
+        tmp = None
+        if log_path is None:
+            fd, tmp = tempfile.mkstemp(prefix="swgpu_log_")
+            os.close(fd)
+            log_path = tmp
+        f = libc.fopen(log_path.encode(), b"w")
+        sets = C.POINTER(SplitSet)()
+        nsets = C.c_int()
+        st = lib().swe_adaptive(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts,
+                                prefix.encode() if prefix else None, f, C.byref(sets), C.byref(nsets))
+        libc.fclose(f)
+        text = Path(log_path).read_text()
+        if tmp:
+            os.unlink(tmp)
+        _check(st, self.ctx)
+        kept = [split_set_to_lists(sets[k]) for k in range(nsets.value)]
+        for k in range(nsets.value):
+            lib().free_split_set_and_associated_clusters(sets[k])
+        lib().swe_free(sets)
+        return text, kept
+
+    def one_to_many(self, q: bytes, qlen: int | None = None) -> np.ndarray:
+        qlen = len(q) if qlen is None else qlen
+        buf = C.create_string_buffer(bytes(q), max(len(q), qlen) + 1)
+        out = np.zeros(self.n, dtype=np.uint32)
+        _check(lib().swe_score_one_to_many(self.ctx, buf, qlen, out.ctypes.data), self.ctx)
+        return out
+
+    def score_pairs(self, a, b) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.int32)
+        out = np.zeros(len(a), dtype=np.uint32)
+        _check(lib().swe_score_pairs(self.ctx, a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data),
+               self.ctx)
+        return out
+
+    def timer_start(self):
+        _check(lib().swe_timer_start(self.ctx), self.ctx)
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        _check(lib().swe_timer_stop(self.ctx, C.byref(ms)), self.ctx)
+        return ms.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().swe_get_stats(self.ctx, C.byref(s)))
+        return s.as_dict()
+
+
+def dbscan_from_matrix(D: np.ndarray, eps: float, minpts: int):
+    """DBSCAN replay (host) on neighbourhoods thresholded from a distance matrix
+    the caller already holds: (float)D[i][k] <= eps."""
+    D = np.asarray(D)
+    n = D.shape[0]
+    nb = D.astype(np.float32) <= np.float32(eps)
+    wpr = (n + 63) // 64
+    padded = np.zeros((n, wpr * 64), dtype=bool)
+    padded[:, :n] = nb
+    bits = np.packbits(padded.reshape(n, wpr, 64)[:, :, ::-1], axis=2).reshape(n, wpr * 8)
+    words = np.ascontiguousarray(bits).view(">u8").astype(np.uint64).reshape(n, wpr)
+    counts = np.ascontiguousarray(nb.sum(axis=1), dtype=np.int32)
+    s = SplitSet()
+    _check(lib().swe_dbscan_bitmap(n, words.ctypes.data, wpr, counts.ctypes.data, minpts, C.byref(s)))
+    out = split_set_to_lists(s)
+    lib().free_split_set_and_associated_clusters(s)
+    return out
+
+
+def measure_mix_peak(device: int = 0):
+    """(DP cells/s, lane instructions/s) of the 16x2 per-cell instruction mix."""
+    c, i = C.c_double(), C.c_double()
+    _check(lib().swe_measure_mix_peak(device, C.byref(c), C.byref(i)))
+    return c.value, i.value
+
+
+def score(a: bytes, b: bytes, la: int | None = None, lb: int | None = None) -> int:
+    """The drop-in score() (one pair on the GPU)."""
+    la = len(a) if la is None else la
+    lb = len(b) if lb is None else lb
+    ab = C.create_string_buffer(bytes(a), max(len(a), la) + 1)
+    bb = C.create_string_buffer(bytes(b), max(len(b), lb) + 1)
+    d = lib().score(ab, bb, la, lb, None)
+    st = lib().swgpu_last_dropin_status()
+    if d == 0xFFFFFFFF and st:
+        raise SwgpuError(st, "score failed")
+    return d

@@ -1,0 +1,295 @@
+"""Generates the golden fixtures in tests/golden/ from the REFERENCE itself.
+
+Every expected value below comes from the reference's own C code, compiled
+from its sources into oracle/_ref by ``make -C oracle ref`` (score(),
+dataset_from_fasta(), dbscan_SW(), the cluster_dbscan_SW /
+adaptive_clustering_SW / find_closest_sequence_SW tools, and the
+score-substitution builds of those tools).  Inputs are seeded synthetic data.
+
+Run from the repository root (needs the reference sources, i.e. this
+container, not the GPU box):
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import base64
+import gzip
+import hashlib
+import json
+import os
+import sys
+import tempfile
+import zlib
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle"))
+sys.path.insert(0, str(ROOT / "mnhn-tree-tools_b200"))
+import oracle as O  # noqa: E402
+from swgpu import workloads as W  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+IUPAC = b"RYKMSWBDHV"
+
+
+def rand_seq(rng, n, alphabet=b"ACGT"):
+    a = np.frombuffer(alphabet, dtype=np.uint8)
+    return a[rng.integers(0, len(a), size=n)].tobytes()
+
+
+def with_n_runs(rng, s, frac=0.05):
+    b = bytearray(s)
+    for _ in range(rng.poisson(frac * len(b) / 8 + 0.5)):
+        st = int(rng.integers(0, max(1, len(b))))
+        ln = int(rng.geometric(0.15))
+        b[st:st + ln] = b"N" * len(b[st:st + ln])
+    return bytes(b)
+
+
+def revcomp(s):
+    return s[::-1].translate(bytes.maketrans(b"ACGTN", b"TGCAN"))
+
+
+def mutate(rng, s, sub=0.05, indel=0.02):
+    arr = np.frombuffer(s, dtype=np.uint8).copy()
+    return W._mutate(rng, arr, sub, indel).tobytes()
+
+
+def score_pairs():
+    rng = np.random.default_rng(1234)
+    pairs = []
+    kat = [(b"ACGT", b"ACGT"), (b"ACGT", b"TCGT"), (b"ACGT", b"ACGA"), (b"ACGT", b"GGGG"),
+           (b"NNNN", b"NNNN"), (b"ACGTACGTAC", b"ACGTAC"), (b"ACGTAC", b"ACGTACGTAC"), (b"", b""),
+           (b"", b"ACG"), (b"ACG", b""), (b"A", b"A"), (b"A", b"C"), (b"AC", b"CA"), (b"acgt", b"ACGT"),
+           (b"ACGT", b"acgt"), (b"RYKM", b"RYKM"), (b"ACGTRYACGT", b"ACGTRYACGT"), (b"A-C-G", b"A-C-G"),
+           (b"NNNNACGTNNNN", b"ACGT"), (b"GATTACA" * 20, b"GATTACA" * 20), (b"T" * 100, b"T" * 99)]
+    for a, b in kat:
+        pairs.append((a, b, len(a), len(b)))
+    for _ in range(300):  # plain DNA, related and unrelated
+        la = int(rng.integers(1, 300))
+        a = rand_seq(rng, la)
+        b = mutate(rng, a, rng.uniform(0, 0.3), rng.uniform(0, 0.05)) if rng.random() < 0.6 else \
+            rand_seq(rng, int(rng.integers(1, 300)))
+        pairs.append((a, b, len(a), len(b)))
+    for _ in range(150):  # N masking runs
+        a = with_n_runs(rng, rand_seq(rng, int(rng.integers(20, 400))))
+        b = with_n_runs(rng, mutate(rng, a, 0.1, 0.02))
+        pairs.append((a, b, len(a), len(b)))
+    for _ in range(80):  # other IUPAC letters and rare symbols
+        a = rand_seq(rng, int(rng.integers(10, 200)), b"ACGT" * 6 + IUPAC + b"-*")
+        b = mutate(rng, a.replace(b"-", b"A").replace(b"*", b"C"), 0.1, 0.0) if rng.random() < 0.5 else \
+            rand_seq(rng, int(rng.integers(10, 200)), b"ACGTN" * 4 + IUPAC)
+        pairs.append((a, b, len(a), len(b)))
+    for _ in range(40):  # reverse complements
+        a = rand_seq(rng, int(rng.integers(50, 300)))
+        pairs.append((a, revcomp(mutate(rng, a, 0.05, 0.01)), 0, 0))
+    for _ in range(30):  # long pairs across 512/768-column boundaries
+        la = int(rng.integers(480, 1300))
+        a = rand_seq(rng, la)
+        b = mutate(rng, a, 0.08, 0.02) if rng.random() < 0.7 else rand_seq(rng, int(rng.integers(480, 1300)))
+        pairs.append((a, b, len(a), len(b)))
+    for _ in range(20):  # claimed length below the string length (find_closest's record-0 length)
+        a = rand_seq(rng, int(rng.integers(20, 200)))
+        b = rand_seq(rng, int(rng.integers(20, 200)))
+        pairs.append((a, b, len(a), int(rng.integers(1, len(b) + 1))))
+    out = []
+    for a, b, la, lb in pairs:
+        la = la or len(a)
+        lb = lb or len(b)
+        out.append([a.decode("latin-1"), b.decode("latin-1"), la, lb, O.ref_score(a, b, la, lb)])
+    with gzip.open(OUT / "score_pairs.json.gz", "wt") as f:
+        json.dump(out, f)
+    print("score_pairs", len(out))
+
+
+FASTA_CASES = {
+    "simple": ">a\nACGT\n>b\nGGCCTA\n",
+    "multiline": ">a\nACGTACGT\nTTGA\nCC\n>b\nA\n",
+    "blank_middle": ">a\nACGT\n\nTTT\n>b\nGG\n",
+    "trailing_blank": ">a\nACGT\n>b\nGGCC\n\n",
+    "blank_after_header": ">a\nACG\n>b\n\nTT\n",
+    "lowercase": ">a\nacgtNn\n>b\nAcGt\n",
+    "crlf": ">a\r\nACGT\r\nTT\r\n>b\r\nGG\r\n",
+    "leading_space": ">a\n  ACGT\n\tTT\n",
+    "two_tokens": ">a\nACGT TTTT\nGG\n",
+    "empty_record": ">a\n>b\nACGT\n>c\n",
+    "no_final_newline": ">a\nACGT\n>b\nTTGG",
+    "long_line": ">a\n" + "ACGT" * 375 + "\n>b\nA\n",
+    "iupac": ">a\nACGTRYKMSWBDHVN\n>b\n-*.\n",
+}
+
+
+def fasta_cases():
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        for name, text in FASTA_CASES.items():
+            p = Path(td) / f"{name}.fa"
+            p.write_bytes(text.encode())
+            out[name] = {"text": text, "expected": [s.decode("latin-1") for s in O.ref_fasta_load(p)]}
+    (OUT / "fasta_cases.json").write_text(json.dumps(out, indent=1))
+    print("fasta_cases", len(out))
+
+
+def small_family_set(seed, n_fam, per_fam, root_len, sub=(0.01, 0.10), indel=0.01):
+    rng = np.random.default_rng(seed)
+    roots = [rng.integers(0, 4, size=root_len) for _ in range(n_fam)]
+    seqs = []
+    for f in range(n_fam):
+        r = W.BASES[roots[f]]
+        for _ in range(per_fam):
+            seqs.append(W._mutate(rng, r, rng.uniform(*sub), indel).tobytes())
+    order = rng.permutation(len(seqs))
+    return [seqs[i] for i in order]
+
+
+def hier_set(seed, n_top=2, n_sub=3, per_sub=30, root_len=120):
+    """Two-level families: sub-roots are 15% mutants of a top root, reads are
+    1-8% mutants of a sub-root, so an eps sweep merges in several layers."""
+    rng = np.random.default_rng(seed)
+    seqs = []
+    for _ in range(n_top):
+        top = W.BASES[rng.integers(0, 4, size=root_len)]
+        for _ in range(n_sub):
+            sub = W._mutate(rng, top, 0.15, 0.01)
+            for _ in range(per_sub):
+                seqs.append(W._mutate(rng, sub, rng.uniform(0.01, 0.08), 0.01).tobytes())
+    order = rng.permutation(len(seqs))
+    return [seqs[i] for i in order]
+
+
+def dbscan_small():
+    seqs = small_family_set(7, 4, 60, 150)
+    D = O.ref_score_rows(seqs)
+    cases = []
+    for eps, minpts in [(60.0, 5), (60.0, 3), (95.5, 10), (150.0, 5), (-1.0, -1), (30.0, 2)]:
+        cl = O.ref_dbscan(seqs, eps, minpts)
+        cases.append({"eps": eps, "minpts": minpts, "clusters": cl})
+    doc = {"seqs": [s.decode() for s in seqs], "cases": cases,
+           "dist_sha256": hashlib.sha256(D.astype("<u2").tobytes()).hexdigest()}
+    (OUT / "dbscan_small.json").write_text(json.dumps(doc))
+    print("dbscan_small", [len(c["clusters"]) for c in cases])
+
+
+def run_tool(name, args, cwd, env=None):
+    r = O.run_ref_tool(name, args, cwd, env)
+    return r.returncode, r.stdout.decode("latin-1")
+
+
+def files_b64(d: Path, prefix: str):
+    return {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(d.glob(prefix + "*"))}
+
+
+def adaptive_small():
+    seqs = hier_set(11)
+    doc = {"seqs": [s.decode() for s in seqs], "runs": []}
+    for eps_start, inc, minpts in [(20.0, 15.0, 5), (400.0, 25.0, 4), (30.0, 12.5, 5), (45.0, 7.3, 3)]:
+        with tempfile.TemporaryDirectory() as td:
+            W.write_fasta(Path(td) / "in.fa", seqs)
+            rc, out = run_tool("adaptive_clustering_SW", ["in.fa", eps_start, inc, minpts, "layer", 1], td)
+            doc["runs"].append({"eps_start": eps_start, "eps_inc": inc, "minpts": minpts, "rc": rc,
+                                "stdout": out, "files": files_b64(Path(td), "layer")})
+    (OUT / "adaptive_small.json").write_text(json.dumps(doc))
+    print("adaptive_small", [r["rc"] for r in doc["runs"]])
+
+
+def cluster_tool_small():
+    seqs = small_family_set(13, 3, 40, 100)
+    with tempfile.TemporaryDirectory() as td:
+        W.write_fasta(Path(td) / "in.fa", seqs)
+        rc, out = run_tool("cluster_dbscan_SW", ["in.fa", 45.0, 4, "cl"], td)
+        doc = {"seqs": [s.decode() for s in seqs], "eps": 45.0, "minpts": 4, "rc": rc, "stdout": out,
+               "files": files_b64(Path(td), "cl-")}
+    (OUT / "cluster_tool_small.json").write_text(json.dumps(doc))
+    print("cluster_tool_small", out.strip())
+
+
+def find_closest_small():
+    rng = np.random.default_rng(17)
+    db = [rand_seq(rng, int(rng.integers(60, 160))) for _ in range(120)]
+    q1 = mutate(rng, db[37], 0.05, 0.01)[:90]
+    q2 = mutate(rng, db[81], 0.1, 0.02) + rand_seq(rng, 10)
+    q3 = db[5]
+    queries = [q1, q2, q3]
+    runs = []
+    with tempfile.TemporaryDirectory() as td:
+        W.write_fasta(Path(td) / "db.fa", db)
+        W.write_fasta(Path(td) / "q.fa", queries)
+        for idx in (1, 2, 3):
+            if len(queries[idx - 1]) < len(queries[0]):
+                continue  # the reference reads past the string there
+            rc, out = run_tool("find_closest_sequence_SW", ["db.fa", "q.fa", idx, 4, f"out{idx}.fa"], td)
+            runs.append({"idx": idx, "rc": rc, "stdout": out, "out": (Path(td) / f"out{idx}.fa").read_text()})
+    doc = {"db": [s.decode() for s in db], "queries": [s.decode() for s in queries], "runs": runs}
+    (OUT / "find_closest_small.json").write_text(json.dumps(doc))
+    print("find_closest_small", [r["stdout"].strip() for r in runs])
+
+
+def row_crcs(D16):
+    return [zlib.crc32(D16[i].tobytes()) for i in range(D16.shape[0])]
+
+
+def matrix_golden(name, seqs, extra=None):
+    D = O.ref_score_rows(seqs)
+    D16 = D.astype("<u2")
+    doc = {"n": len(seqs), "sha256": hashlib.sha256(D16.tobytes()).hexdigest(), "row_crc32": row_crcs(D16),
+           "max": int(D.max()), "cells": W.cells(seqs)}
+    if extra:
+        doc.update(extra(D))
+    (OUT / f"{name}.json").write_text(json.dumps(doc))
+    print(name, doc["sha256"][:16], doc["max"])
+    return D
+
+
+def config1_golden():
+    seqs, _ = W.config1()
+
+    def extra(D):
+        out = {}
+        with tempfile.TemporaryDirectory() as td:
+            td = Path(td)
+            W.write_fasta(td / "c1.fa", seqs)
+            O.write_dist_file(td / "d.bin", D)
+            env = {"SWGPU_SUBST_DIST": str(td / "d.bin")}
+            rc, so = run_tool("cluster_dbscan_SW_subst", ["c1.fa", 130.0, 5, "c1"], td, env)
+            files = sorted(td.glob("c1-*"))
+            out["dbscan"] = {"eps": 130.0, "minpts": 5, "rc": rc, "stdout": so,
+                             "files_sha256": {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in files}}
+            rc, so = run_tool("adaptive_clustering_SW_subst", ["c1.fa", 100.0, 60.0, 5, "lay", 1], td, env)
+            files = sorted(td.glob("lay*"))
+            out["adaptive"] = {"eps_start": 100.0, "eps_inc": 60.0, "minpts": 5, "rc": rc, "stdout": so,
+                               "files_sha256": {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in files}}
+        return out
+
+    matrix_golden("config1_golden", seqs, extra)
+
+
+def subset_goldens():
+    s2, _ = W.config2()
+    matrix_golden("config2_head1500_golden", s2[:1500])
+    s3, _ = W.config3()
+    matrix_golden("config3_head1500_golden", s3[:1500])
+
+
+if __name__ == "__main__":
+    if not O.ref_available():
+        O.build()
+    which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets"]
+    if "score" in which:
+        score_pairs()
+    if "fasta" in which:
+        fasta_cases()
+    if "dbscan" in which:
+        dbscan_small()
+    if "adaptive" in which:
+        adaptive_small()
+    if "cluster" in which:
+        cluster_tool_small()
+    if "closest" in which:
+        find_closest_small()
+    if "config1" in which:
+        config1_golden()
+    if "subsets" in which:
+        subset_goldens()

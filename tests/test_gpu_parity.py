@@ -1,0 +1,320 @@
+"""GPU engine parity: every distance, neighbour list, cluster label, log line
+and file must equal the reference's (golden vectors produced by the
+reference itself) or the oracle's on the same seeded inputs.  Integer work:
+the bar is bit-exact."""
+from __future__ import annotations
+
+import base64
+import hashlib
+import math
+import subprocess
+import zlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+import swgpu
+from conftest import load_golden
+from swgpu import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = swgpu.Engine()
+    yield e
+    e.close()
+
+
+def _matrix(eng, seqs):
+    eng.upload(seqs)
+    eng.score_all_pairs()
+    return eng.distances()
+
+
+def _row_diag(D, golden):
+    D16 = D.astype("<u2")
+    bad = [i for i in range(D.shape[0]) if zlib.crc32(D16[i].tobytes()) != golden["row_crc32"][i]]
+    return bad[:10]
+
+
+# ---------------------------------------------------------------------------
+# single pairs
+# ---------------------------------------------------------------------------
+def test_dropin_score_matches_reference_pairs():
+    pairs = load_golden("score_pairs.json.gz")
+    bad = []
+    for a, b, la, lb, d in pairs:
+        got = swgpu.score(a.encode("latin-1"), b.encode("latin-1"), la, lb)
+        if got != d:
+            bad.append((a[:20], b[:20], la, lb, d, got))
+    assert not bad, bad[:5]
+
+
+def test_engine_pairs_and_matrix_match_reference_pairs(eng):
+    """The golden pairs scored as one dataset: explicit pairs (32-bit kernel)
+    and the all-pairs matrix (16x2 kernel plus the 32-bit path for rare
+    symbols, empty and long sequences) agree with the reference."""
+    import ctypes as C
+    pairs = load_golden("score_pairs.json.gz")
+    P = len(pairs)
+    # full strings with their claimed lengths: the engine reads s[1..len], so a
+    # claimed length below the string length keeps the character at s[len]
+    seqs = [a.encode("latin-1") for a, b, la, lb, d in pairs] + [b.encode("latin-1") for a, b, la, lb, d in pairs]
+    lens = [la for a, b, la, lb, d in pairs] + [lb for a, b, la, lb, d in pairs]
+    bufs = [C.create_string_buffer(s, len(s) + 1) for s in seqs]
+    ptrs = (C.c_char_p * len(bufs))(*[C.addressof(x) for x in bufs])
+    lens_c = (C.c_size_t * len(bufs))(*lens)
+    swgpu._check(swgpu.lib().swe_upload(eng.ctx, ptrs, lens_c, len(bufs)), eng.ctx)
+    eng.n = len(bufs)
+    want = np.array([d for a, b, la, lb, d in pairs], dtype=np.uint32)
+    got = eng.score_pairs(np.arange(P), np.arange(P) + P)
+    assert np.array_equal(got, want), np.nonzero(got != want)[0][:10]
+    eng.score_all_pairs()
+    D = eng.distances()
+    diag = D[np.arange(P), np.arange(P) + P]
+    assert np.array_equal(diag, want), np.nonzero(diag != want)[0][:10]
+    assert np.array_equal(D, D.T)
+
+
+# ---------------------------------------------------------------------------
+# full matrices against the reference
+# ---------------------------------------------------------------------------
+def test_config1_matrix_bit_exact(eng):
+    seqs, _ = W.config1()
+    g = load_golden("config1_golden.json")
+    D = _matrix(eng, seqs)
+    assert hashlib.sha256(D.astype("<u2").tobytes()).hexdigest() == g["sha256"], _row_diag(D, g)
+    st = eng.stats()
+    assert st["reruns"] == 0 and st["n_fast"] == 2000
+
+
+@pytest.mark.parametrize("name,gen", [("config2_head1500_golden", lambda: W.config2()[0][:1500]),
+                                      ("config3_head1500_golden", lambda: W.config3()[0][:1500])])
+def test_subset_matrices_bit_exact(eng, name, gen):
+    seqs = gen()
+    g = load_golden(name + ".json")
+    D = _matrix(eng, seqs)
+    assert hashlib.sha256(D.astype("<u2").tobytes()).hexdigest() == g["sha256"], _row_diag(D, g)
+
+
+def test_forced_saturation_rerun_is_exact():
+    """With the saturation guard lowered, pairs whose 16-bit maximum reaches it
+    are rescored by the 32-bit kernel; the matrix must not change."""
+    seqs, _ = W.config1()
+    seqs = seqs[:600]
+    ref = O.all_pairs(seqs)
+    e = swgpu.Engine(sat_limit=400)
+    D = _matrix(e, seqs)
+    st = e.stats()
+    e.close()
+    assert st["reruns"] > 1000
+    assert np.array_equal(D, ref)
+
+
+def _mixed_set(rng):
+    seqs = []
+    for L in list(range(1, 40)) + [63, 64, 65, 127, 128, 129, 191, 192, 193, 255, 256, 383, 384, 385,
+                                   511, 512, 513, 700, 767, 768, 769, 900, 1030, 1600]:
+        seqs.append(W.BASES[rng.integers(0, 4, size=L)].tobytes())
+    base = seqs[-5]
+    seqs += [base, base[:300] + b"N" * 40 + base[340:], base.lower(), b"", b"", b"A", b"N",
+             b"ACGTRYKMACGT" * 5, b"-" * 30, b"ACGT" * 50 + b"Z"]
+    for _ in range(40):
+        s = bytearray(W.BASES[rng.integers(0, 4, size=int(rng.integers(80, 400)))].tobytes())
+        for _ in range(int(rng.integers(0, 4))):
+            p = int(rng.integers(0, len(s)))
+            s[p:p + 12] = b"N" * len(s[p:p + 12])
+        seqs.append(bytes(s))
+    return seqs
+
+
+@pytest.mark.parametrize("ppb,threads", [(32, 256), (1, 32), (3, 96), (7, 128)])
+def test_mixed_lengths_symbols_and_tile_shapes(ppb, threads):
+    rng = np.random.default_rng(21)
+    seqs = _mixed_set(rng)
+    ref = O.all_pairs(seqs)
+    e = swgpu.Engine(packs_per_block=ppb, threads=threads)
+    D = _matrix(e, seqs)
+    st = e.stats()
+    e.close()
+    assert st["n_exceptional"] > 0 and st["n_fast"] > 0
+    bad = np.argwhere(D != ref)
+    assert len(bad) == 0, [(int(i), int(j), int(D[i, j]), int(ref[i, j])) for i, j in bad[:5]]
+
+
+def test_long_sequences_need_uint32_matrix():
+    rng = np.random.default_rng(5)
+    seqs = [W.BASES[rng.integers(0, 4, size=17000)].tobytes()]
+    seqs.append(W._mutate(rng, np.frombuffer(seqs[0], dtype=np.uint8).copy(), 0.02, 0.0).tobytes())
+    seqs.append(W.BASES[rng.integers(0, 4, size=300)].tobytes())
+    e = swgpu.Engine()
+    D = _matrix(e, seqs)
+    assert e.stats()["dist_bytes"] == 4
+    e.close()
+    for i in range(3):
+        for k in range(3):
+            assert D[i, k] == O.score(seqs[k], seqs[i]), (i, k)
+
+
+# ---------------------------------------------------------------------------
+# neighbourhoods, DBSCAN, adaptive sweep
+# ---------------------------------------------------------------------------
+def test_neighbors_csr_matches_threshold(eng):
+    seqs, _ = W.config1()
+    seqs = seqs[:700]
+    D = _matrix(eng, seqs)
+    for eps in [130.0, 0.0, 0.5, 90.0, 129.99, 1e9, -0.5, float("nan"), -1.0]:
+        rp, cols = eng.neighbors(eps)
+        for i in range(0, 700, 37):
+            want = np.nonzero(D[i].astype(np.float32) <= np.float32(eps))[0]
+            assert np.array_equal(cols[rp[i]:rp[i + 1]], want), (eps, i)
+
+
+def test_dbscan_matches_reference_small(eng):
+    doc = load_golden("dbscan_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    _matrix(eng, seqs)
+    for case in doc["cases"]:
+        assert eng.dbscan(case["eps"], case["minpts"]) == case["clusters"], case["eps"]
+
+
+def test_dbscan_config1_matches_oracle(eng):
+    seqs, _ = W.config1()
+    D = _matrix(eng, seqs)
+    for eps, mp in [(130.0, 5), (250.0, 10), (700.0, 5), (60.0, 2)]:
+        assert eng.dbscan(eps, mp) == O.dbscan(D, eps, mp), (eps, mp)
+
+
+def test_adaptive_matches_reference_small(eng, tmp_path):
+    doc = load_golden("adaptive_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    _matrix(eng, seqs)
+    for k, run in enumerate(doc["runs"]):
+        d = tmp_path / f"r{k}"
+        d.mkdir()
+        text, kept = eng.adaptive(run["eps_start"], run["eps_inc"], run["minpts"], prefix=str(d / "layer"))
+        assert "Dataset read!\n" + text == run["stdout"]
+        got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(d.glob("layer*"))}
+        assert got == run["files"]
+
+
+def test_sweep_that_cannot_end_returns_error(eng):
+    seqs, _ = W.config1()
+    _matrix(eng, seqs[:5])  # 5 points, minpts 5: never one cluster
+    with pytest.raises(swgpu.SwgpuError) as e:
+        eng.adaptive(10.0, 50.0, 5)
+    assert e.value.status == 9
+
+
+def test_bounded_wait_timeout_is_reported_and_context_survives():
+    seqs, _ = W.config1()
+    seqs = seqs[:300]
+    e = swgpu.Engine(inject_timeout=1)
+    e.upload(seqs)
+    with pytest.raises(swgpu.SwgpuError) as err:
+        e.score_all_pairs()
+    assert err.value.status == 5
+    e.close()
+    ok = swgpu.Engine()
+    D = _matrix(ok, seqs)
+    ok.close()
+    assert np.array_equal(D, O.all_pairs(seqs))
+
+
+def test_one_to_many_and_query_length_quirk(eng):
+    rng = np.random.default_rng(9)
+    seqs, _ = W.config1()
+    db = seqs[:500] + [W.BASES[rng.integers(0, 4, size=900)].tobytes()]
+    eng.upload(db)
+    q = W._mutate(rng, np.frombuffer(db[7], dtype=np.uint8).copy(), 0.05, 0.01).tobytes()
+    want = np.array([O.score(s, q) for s in db], dtype=np.uint32)
+    assert np.array_equal(eng.one_to_many(q), want)
+    want = np.array([O.score(s, q, len(s), 120) for s in db], dtype=np.uint32)
+    assert np.array_equal(eng.one_to_many(q, 120), want)
+
+
+# ---------------------------------------------------------------------------
+# drop-in command-line tools against the reference tools
+# ---------------------------------------------------------------------------
+def _tool(name, args, cwd):
+    r = subprocess.run([str(swgpu.BIN_DIR / name)] + [str(a) for a in args], cwd=cwd, capture_output=True,
+                       timeout=1200)
+    return r.returncode, r.stdout.decode("latin-1"), r.stderr.decode("latin-1")
+
+
+def test_cluster_dbscan_tool_config1(tmp_path):
+    seqs, _ = W.config1()
+    g = load_golden("config1_golden.json")["dbscan"]
+    W.write_fasta(tmp_path / "c1.fa", seqs)
+    rc, out, err = _tool("cluster_dbscan_SW", ["c1.fa", g["eps"], g["minpts"], "c1"], tmp_path)
+    assert rc == g["rc"] == 0, err
+    assert out == g["stdout"]
+    got = {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in sorted(tmp_path.glob("c1-*"))}
+    assert got == g["files_sha256"]
+
+
+def test_adaptive_tool_config1(tmp_path):
+    seqs, _ = W.config1()
+    g = load_golden("config1_golden.json")["adaptive"]
+    W.write_fasta(tmp_path / "c1.fa", seqs)
+    rc, out, err = _tool("adaptive_clustering_SW", ["c1.fa", g["eps_start"], g["eps_inc"], g["minpts"], "lay", 1],
+                         tmp_path)
+    assert rc == g["rc"] == 0, err
+    assert out == g["stdout"]
+    got = {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in sorted(tmp_path.glob("lay*"))}
+    assert got == g["files_sha256"]
+
+
+def test_cluster_tool_small(tmp_path):
+    doc = load_golden("cluster_tool_small.json")
+    W.write_fasta(tmp_path / "in.fa", [s.encode() for s in doc["seqs"]])
+    rc, out, err = _tool("cluster_dbscan_SW", ["in.fa", doc["eps"], doc["minpts"], "cl"], tmp_path)
+    assert rc == 0, err
+    assert out == doc["stdout"]
+    got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(tmp_path.glob("cl-*"))}
+    assert got == doc["files"]
+
+
+def test_find_closest_tool(tmp_path):
+    doc = load_golden("find_closest_small.json")
+    W.write_fasta(tmp_path / "db.fa", [s.encode() for s in doc["db"]])
+    W.write_fasta(tmp_path / "q.fa", [s.encode() for s in doc["queries"]])
+    for run in doc["runs"]:
+        rc, out, err = _tool("find_closest_sequence_SW", ["db.fa", "q.fa", run["idx"], 4, "o.fa"], tmp_path)
+        assert rc == 0, err
+        assert out == run["stdout"]
+        assert (tmp_path / "o.fa").read_text() == run["out"]
+
+
+def test_adaptive_tool_small(tmp_path):
+    doc = load_golden("adaptive_small.json")
+    W.write_fasta(tmp_path / "in.fa", [s.encode() for s in doc["seqs"]])
+    for k, run in enumerate(doc["runs"]):
+        d = tmp_path / f"r{k}"
+        d.mkdir()
+        rc, out, err = _tool("adaptive_clustering_SW", [tmp_path / "in.fa", run["eps_start"], run["eps_inc"],
+                                                        run["minpts"], "layer", 1], d)
+        assert rc == run["rc"], err
+        assert out == run["stdout"]
+        got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(d.glob("layer*"))}
+        assert got == run["files"]
+
+
+# ---------------------------------------------------------------------------
+# size-independent properties at the full config-2 size
+# ---------------------------------------------------------------------------
+@pytest.mark.slow
+def test_config2_full_properties_and_sampled_rows(eng):
+    seqs, _ = W.config2()
+    D = _matrix(eng, seqs)
+    L = np.array([len(s) for s in seqs])
+    assert np.array_equal(D, D.T)
+    assert not D.diagonal().any()
+    assert (D <= 4 * np.maximum(L[:, None], L[None, :])).all()
+    rows = list(range(0, 20000, 1999))
+    R = O.score_rows(seqs, rows)
+    assert np.array_equal(D[rows], R)

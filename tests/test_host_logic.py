@@ -1,0 +1,216 @@
+"""Host logic of libswgpu.so that runs without a GPU: the C ABI's exports,
+the FASTA loader, split-set and cluster-file formats, layer relations, the
+order-faithful DBSCAN replay and the adaptive driver.  No kernel is launched
+here; where distances are needed they come from the oracle."""
+from __future__ import annotations
+
+import base64
+import ctypes as C
+import json
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+import swgpu
+from conftest import ROOT, gpu_available, load_golden
+
+
+def _declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", text, flags=re.M):
+            name = m.group(1)
+            if name not in {"if", "while", "for", "return", "sizeof"}:
+                names.add(name)
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = swgpu.lib()
+    declared = _declared_functions()
+    assert set(swgpu.EXPORTS) <= declared | {"adaptive_dbscan"}
+    for name in sorted(declared):
+        assert hasattr(L, name), f"{name} declared in include/ but not exported"
+    out = subprocess.run(["nm", "-D", "--defined-only", str(swgpu.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert declared <= exported
+
+
+def test_cli_tools_built():
+    for t in ("cluster_dbscan_SW", "adaptive_clustering_SW", "find_closest_sequence_SW"):
+        assert (swgpu.BIN_DIR / t).exists()
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
+def test_create_fails_loudly_without_gpu():
+    with pytest.raises(swgpu.SwgpuError) as e:
+        swgpu.Engine()
+    assert e.value.status == 4  # SWE_ERR_NO_DEVICE
+
+
+def _load_with_lib(path):
+    L = swgpu.lib()
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    L.dataset_from_fasta.restype = swgpu.Dataset
+    L.dataset_from_fasta.argtypes = [C.c_void_p]
+    L.free_sequences_from_dataset.argtypes = [swgpu.Dataset]
+    f = libc.fopen(str(path).encode(), b"r")
+    ds = L.dataset_from_fasta(f)
+    libc.fclose(f)
+    out = [C.string_at(ds.sequences[k], ds.sequence_lengths[k]).decode("latin-1") for k in range(ds.n_values)]
+    mx = ds.max_sequence_length
+    L.free_sequences_from_dataset(ds)
+    return out, mx
+
+
+def test_fasta_loader_matches_reference(tmp_path):
+    cases = load_golden("fasta_cases.json")
+    for name, case in cases.items():
+        p = tmp_path / f"{name}.fa"
+        p.write_bytes(case["text"].encode("latin-1"))
+        got, mx = _load_with_lib(p)
+        assert got == case["expected"], name
+        assert mx == max((len(s) for s in got), default=0)
+
+
+def _make_split_set(clusters):
+    arr = (swgpu.Cluster * max(1, len(clusters)))()
+    keep = []
+    for i, cl in enumerate(clusters):
+        m = (C.c_int * max(1, len(cl)))(*cl)
+        keep.append(m)
+        arr[i] = swgpu.Cluster(C.cast(m, C.POINTER(C.c_int)), len(cl), i)
+    return swgpu.SplitSet(len(clusters), C.cast(arr, C.POINTER(swgpu.Cluster))), (arr, keep)
+
+
+def test_split_set_bytes_and_roundtrip(tmp_path):
+    rng = np.random.default_rng(3)
+    clusters = [sorted(rng.choice(500, size=int(rng.integers(1, 40)), replace=False).tolist())
+                for _ in range(7)]
+    s, _keep = _make_split_set(clusters)
+    p = tmp_path / "ss"
+    swgpu.lib().store_split_set(str(p).encode(), s)
+    assert p.read_bytes() == O.split_set_bytes(clusters)
+    back = swgpu.lib().read_split_set(str(p).encode())
+    assert swgpu.split_set_to_lists(back) == clusters
+    swgpu.lib().free_split_set_and_associated_clusters(back)
+
+
+def test_store_split_set_keeps_tail_like_reference(tmp_path):
+    # cluster_io.c:644-645 opens without O_TRUNC
+    p = tmp_path / "ss"
+    p.write_bytes(b"X" * 200)
+    s, _keep = _make_split_set([[1, 2, 3]])
+    swgpu.lib().store_split_set(str(p).encode(), s)
+    body = O.split_set_bytes([[1, 2, 3]])
+    assert p.read_bytes() == body + b"X" * (200 - len(body))
+
+
+def test_relation_sorts_in_place_like_reference():
+    L = swgpu.lib()
+
+    class Conn(C.Structure):
+        _fields_ = [("connections", C.POINTER(C.c_int)), ("n_connections", C.c_int)]
+
+    L.generate_split_set_relation.restype = C.POINTER(Conn)
+    L.generate_split_set_relation.argtypes = [swgpu.SplitSet, swgpu.SplitSet]
+    rng = np.random.default_rng(5)
+    for trial in range(20):
+        n = 300
+        perm = rng.permutation(n).tolist()
+        cuts = sorted(rng.choice(np.arange(1, n), size=5, replace=False).tolist())
+        anc = [perm[a:b] for a, b in zip([0] + cuts, cuts + [n])]
+        perm2 = rng.permutation(n).tolist()
+        cuts2 = sorted(rng.choice(np.arange(1, n), size=3, replace=False).tolist())
+        new = [perm2[a:b] for a, b in zip([0] + cuts2, cuts2 + [n])]
+        # mix: some new clusters are unions of ancient ones
+        new[0] = anc[0] + anc[1][: len(anc[1]) // 2]
+        sa, ka = _make_split_set(anc)
+        sn, kn = _make_split_set(new)
+        conns = L.generate_split_set_relation(sa, sn)
+        got = [[conns[i].connections[k] for k in range(conns[i].n_connections)] for i in range(len(new))]
+        anc_py = [list(c) for c in anc]
+        new_py = [list(c) for c in new]
+        want = O.relation(anc_py, new_py)
+        assert got == want
+        # the in-place sorts are visible in the member arrays
+        assert [list(ka[1][i][: len(anc[i])]) for i in range(len(anc))] == anc_py
+        assert [list(kn[1][i][: len(new[i])]) for i in range(len(new))] == new_py
+
+
+def test_replay_matches_oracle_dbscan():
+    doc = load_golden("dbscan_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    D = O.all_pairs(seqs)
+    for case in doc["cases"]:
+        eps = 0.015 if case["eps"] == -1 else case["eps"]
+        got = swgpu.dbscan_from_matrix(D, eps, case["minpts"])
+        assert got == case["clusters"], case
+
+
+def test_replay_random_graphs():
+    rng = np.random.default_rng(11)
+    for trial in range(30):
+        n = int(rng.integers(1, 400))
+        pts = rng.normal(size=(n, 2)) * rng.uniform(0.5, 5)
+        D = np.round(np.sqrt(((pts[:, None] - pts[None]) ** 2).sum(-1)) * 10).astype(np.uint32)
+        eps = float(rng.uniform(0, 15))
+        mp = int(rng.integers(0, 8))
+        assert swgpu.dbscan_from_matrix(D, eps, mp) == O.dbscan(D, eps, mp), (trial, n, eps, mp)
+
+
+@pytest.fixture(scope="module")
+def host_driver(tmp_path_factory):
+    exe = tmp_path_factory.mktemp("drv") / "adaptive_host_driver"
+    subprocess.run(["gcc", "-O1", "-std=c11", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests/c/adaptive_host_driver.c"), "-o", str(exe),
+                    "-L", str(swgpu.LIB_PATH.parent), "-lswgpu", f"-Wl,-rpath,{swgpu.LIB_PATH.parent}"],
+                   check=True)
+    return exe
+
+
+def test_adaptive_driver_matches_reference(tmp_path, host_driver):
+    """libswgpu's adaptive_dbscan driving a caller-supplied dbscanner (the
+    function-pointer seam of dbscan.h:72-81) reproduces the reference's log and
+    split-set files byte for byte."""
+    from swgpu import workloads as W
+    doc = load_golden("adaptive_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    D = O.all_pairs(seqs)
+    W.write_fasta(tmp_path / "in.fa", seqs)
+    O.write_dist_file(tmp_path / "d.swd", D)
+    for k, run in enumerate(doc["runs"]):
+        d = tmp_path / f"run{k}"
+        d.mkdir()
+        r = subprocess.run([str(host_driver), str(tmp_path / "in.fa"), str(tmp_path / "d.swd"),
+                            repr(run["eps_start"]), repr(run["eps_inc"]), str(run["minpts"]), "layer"],
+                           cwd=d, capture_output=True, timeout=600)
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        assert r.stdout.decode("latin-1") == run["stdout"]
+        got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(d.glob("layer*"))}
+        assert got == run["files"]
+
+
+def test_cluster_files_match_reference(tmp_path):
+    doc = load_golden("cluster_tool_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    D = O.all_pairs(seqs)
+    cl = swgpu.dbscan_from_matrix(D, doc["eps"], doc["minpts"])
+    s, _keep = _make_split_set(cl)
+    buf = swgpu.SeqBuffer(seqs)
+    L = swgpu.lib()
+    L.create_cluster_files.argtypes = [C.c_char_p, swgpu.SplitSet, swgpu.Dataset]
+    L.create_cluster_files(str(tmp_path / "cl").encode(), s, buf.dataset())
+    got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(tmp_path.glob("cl-*"))}
+    assert got == doc["files"]

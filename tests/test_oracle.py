@@ -1,0 +1,106 @@
+"""The oracle (oracle/sw_oracle.c + oracle/oracle.py) pinned against golden
+vectors that the reference itself produced (tests/golden/make_golden.py)."""
+from __future__ import annotations
+
+import base64
+import hashlib
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden
+
+
+def test_score_kats():
+    # smith-waterman.c quirks: first base ignored, terminator counts, N == N
+    assert O.score(b"ACGT", b"ACGT") == 0
+    assert O.score(b"ACGT", b"TCGT") == 0
+    assert O.score(b"ACGT", b"ACGA") == 8
+    assert O.score(b"ACGT", b"GGGG") == 11
+    assert O.score(b"NNNN", b"NNNN") == 0
+    assert O.score(b"ACGTACGTAC", b"ACGTAC") == 16 == O.score(b"ACGTAC", b"ACGTACGTAC")
+
+
+def test_score_golden_pairs():
+    pairs = load_golden("score_pairs.json.gz")
+    bad = [(a, b, la, lb, d) for a, b, la, lb, d in pairs
+           if O.score(a.encode("latin-1"), b.encode("latin-1"), la, lb) != d]
+    assert not bad, bad[:3]
+
+
+def test_fasta_golden(tmp_path):
+    cases = load_golden("fasta_cases.json")
+    for name, case in cases.items():
+        p = tmp_path / f"{name}.fa"
+        p.write_bytes(case["text"].encode("latin-1"))
+        got = [s.decode("latin-1") for s in O.fasta_load(p)]
+        assert got == case["expected"], name
+
+
+def _small_matrix(doc):
+    seqs = [s.encode() for s in doc["seqs"]]
+    return seqs, O.all_pairs(seqs)
+
+
+def test_dbscan_golden():
+    doc = load_golden("dbscan_small.json")
+    seqs, D = _small_matrix(doc)
+    assert hashlib.sha256(D.astype("<u2").tobytes()).hexdigest() == doc["dist_sha256"]
+    for case in doc["cases"]:
+        assert O.dbscan(D, case["eps"], case["minpts"]) == case["clusters"], case["eps"]
+
+
+def test_adaptive_golden():
+    doc = load_golden("adaptive_small.json")
+    seqs, D = _small_matrix(doc)
+    for run in doc["runs"]:
+        text, kept = O.adaptive(D, run["eps_start"], run["eps_inc"], run["minpts"])
+        assert "Dataset read!\n" + text == run["stdout"]
+        files = {f"layer{i:04d}": O.split_set_bytes(s) for i, s in enumerate(kept)}
+        assert set(files) == set(run["files"])
+        for k, v in files.items():
+            assert v == base64.b64decode(run["files"][k]), k
+
+
+def test_cluster_tool_golden():
+    doc = load_golden("cluster_tool_small.json")
+    seqs, D = _small_matrix(doc)
+    cl = O.dbscan(D, doc["eps"], doc["minpts"])
+    assert doc["stdout"] == "%u clusters obtained \n" % len(cl)
+    for i, c in enumerate(cl):
+        assert base64.b64decode(doc["files"][f"cl-{i:03d}"]).decode() == O.cluster_fasta_text(c, seqs)
+
+
+def test_find_closest_golden():
+    doc = load_golden("find_closest_small.json")
+    db = [s.encode() for s in doc["db"]]
+    qs = [s.encode() for s in doc["queries"]]
+    for run in doc["runs"]:
+        d, i = O.find_closest(db, qs, run["idx"])
+        assert run["stdout"] == "Smith Waterman distance = %i \n" % d
+        assert run["out"] == O.cluster_fasta_text([i], db)
+
+
+def test_config_generators_are_seeded():
+    from swgpu import workloads as W
+    a, _ = W.config1()
+    b, _ = W.config1()
+    assert a == b and len(a) == 2000
+    g = load_golden("config1_golden.json")
+    assert g["n"] == 2000 and g["cells"] == W.cells(a)
+
+
+@pytest.mark.slow
+def test_config1_rows_match_reference_golden():
+    """Sampled rows of the oracle's config-1 matrix against the reference's row CRCs."""
+    import zlib
+    from swgpu import workloads as W
+    seqs, _ = W.config1()
+    g = load_golden("config1_golden.json")
+    rows = list(range(0, 2000, 97))
+    R = O.score_rows(seqs, rows).astype("<u2")
+    for k, r in enumerate(rows):
+        assert zlib.crc32(R[k].tobytes()) == g["row_crc32"][r], r

@@ -504,7 +504,8 @@ static swe_status build_score_graph(swe_ctx* ctx) {
   cudaError_t e = cudaMemsetAsync(ctx->d_ctr.p, 0, 4 * sizeof(unsigned), st);
   ctx->graph_kernels = 1;
   if (e == cudaSuccess) e = launch_diag(ctx->d_D16.p, ctx->d_D32.p, ctx->n, st);
-  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], st);
+  // inside a capture only an external record becomes a real event node
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev[0], st, cudaEventRecordExternal);
   if (e == cudaSuccess && !ctx->tiles.empty()) {
     FastParams p{};
     p.codes = ctx->d_codes.p;
@@ -535,7 +536,7 @@ static swe_status build_score_graph(swe_ctx* ctx) {
     e = launch_fast(p, ctx->fast_grid, ctx->threads, ctx->smem, st);
     ctx->graph_kernels++;
   }
-  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], st);
+  if (e == cudaSuccess) e = cudaEventRecordWithFlags(ctx->ev[1], st, cudaEventRecordExternal);
   GenParams g{};
   g.codes = ctx->d_codes.p;
   g.code_off = ctx->d_off.p;
@@ -594,8 +595,8 @@ swe_status swe_score_all_pairs(swe_ctx* ctx) {
   CK(cpy(ctx, ctr, ctx->d_ctr.p, sizeof(ctr), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   float ms = 0, msf = 0;
-  cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
-  cudaEventElapsedTime(&msf, ctx->ev[0], ctx->ev[1]);
+  CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+  CK(cudaEventElapsedTime(&msf, ctx->ev[0], ctx->ev[1]));
   ctx->stats.ms_score_pass = ms;
   ctx->stats.ms_fast_kernel = msf;
   ctx->stats.reruns = std::min(ctr[2], ctx->rerun_cap);
@@ -651,7 +652,7 @@ static swe_status ensure_bitmap(swe_ctx* ctx, long long T) {
   CK(cpy(ctx, ctx->h_counts.p, ctx->d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   float ms = 0;
-  cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+  CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
   ctx->stats.ms_last_neighbors = ms;
   ctx->bits_T = T;
   return SWE_OK;

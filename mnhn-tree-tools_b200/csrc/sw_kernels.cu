@@ -234,8 +234,10 @@ cudaError_t fast_set_smem_limit(size_t bytes) {
 int fast_occupancy(int block, size_t smem) {
   int nb = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fast_all_pairs_kernel, block, smem) !=
-      cudaSuccess)
+      cudaSuccess) {
+    cudaGetLastError();  // do not leave the query's error for the next launch check
     return 0;
+  }
   return nb;
 }
 

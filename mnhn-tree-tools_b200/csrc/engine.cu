@@ -841,7 +841,7 @@ swe_status swe_measure_mix_peak(int device, double* cells_per_s, double* lane_in
   CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
   const double updates = (double)grid * block * iters * 8.0;  // packed cell updates (8 chains)
   *cells_per_s = 2.0 * updates / (ms * 1e-3);
-  *lane_instr_per_s = 5.0 * updates / (ms * 1e-3);
+  *lane_instr_per_s = 4.5 * updates / (ms * 1e-3);  // PRMT, 2 adds, 3-input max, half a max
   return SWE_OK;
 }
 

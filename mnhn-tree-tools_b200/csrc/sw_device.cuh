@@ -54,6 +54,17 @@ __device__ __forceinline__ uint32_t vaddmax0(uint32_t a, uint32_t b, uint32_t c)
 __device__ __forceinline__ uint32_t vmax3_0(uint32_t a, uint32_t b, uint32_t c) {
   return __vimax3_s16x2_relu(a, b, c);
 }
+// Per-halfword max(a, b, c).
+__device__ __forceinline__ uint32_t vmax3(uint32_t a, uint32_t b, uint32_t c) {
+  return __vimax3_s16x2(a, b, c);
+}
+// Per-halfword wrapping add.  Measured on B200 this issues on the FMA pipe,
+// leaving the ALU pipe (PRMT and the packed maxima) free.
+__device__ __forceinline__ uint32_t vadd(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("add.s16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
 
 // ---------------------------------------------------------------------------
 // mbarrier + bulk copy (TMA engine, non-tensor form)

@@ -27,19 +27,26 @@ namespace swgpu {
 // and, at step s, computes row g = s - li of the row stream (two row
 // sequences per 16-bit half, packs back to back).  Its left boundary arrives
 // from lane li-1 by shuffle; the diagonal boundary is the left boundary of the
-// previous step.  Per cell (d = s + 3 from the PRMT table):
-//   v = max(H[i-1][j-1] + d, max(H[i][j-1], H[i-1][j]))
-//   H = max(v - 3, 0)
-// which is max(0, diag + s, left - 3, up - 3).  Pad columns (beyond len B)
-// and pad rows (code 7) only ever see mismatches, so they can never raise
-// the maximum above the real cells' maximum.
+// previous step.
+//
+// Each column keeps E = H - 3 of the previous row, so one stored value feeds
+// all three uses of a cell: left and up need H - 3 = E, and the diagonal needs
+// H + s = E + d with d = s + 3 from the PRMT table.  Per cell:
+//   t = E_diag + d               (packed add, FMA pipe)
+//   H = max(t, E_left, E_up, 0)  (3-input packed max, ALU pipe)
+//   E = H - 3                    (packed add, FMA pipe)
+// i.e. H = max(0, diag + s, left - 3, up - 3).  The running maximum takes two
+// cells per 3-input max.  Pad columns (beyond len B) and pad rows (code 7) only
+// ever see mismatches, so they can never raise the maximum above the real
+// cells' maximum.
 // ---------------------------------------------------------------------------
 template <int W>
 __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, int total_rows,
                                              const int* __restrict__ pstart, int npk,
                                              const uint8_t* __restrict__ bcodes, int lenB, int lpb,
                                              int li, unsigned* __restrict__ smax) {
-  uint32_t tlo[W], thi[W], H[W];
+  const uint32_t M3 = 0xFFFDFFFDu;  // -3 in both halves (E of a zero cell)
+  uint32_t tlo[W], thi[W], E[W];
 #pragma unroll
   for (int k = 0; k < W; ++k) {
     const int col = li * W + k;
@@ -49,16 +56,16 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
     else if (c < 8) hi ^= (0xF8u << (8 * (c - 4)));
     tlo[k] = lo;
     thi[k] = hi;
-    H[k] = 0u;
+    E[k] = M3;
   }
-  const uint32_t M3 = 0xFFFDFFFDu;  // -3 in both halves
-  uint32_t mx = 0u, last = 0u, diag = 0u;
+  uint32_t mx = 0u, last = M3, diag = M3;
   int pk = -1, next = 0;
-  const uint32_t lmask = li ? 0xFFFFFFFFu : 0u;
+  const bool lead = (li == 0);
   const int steps = total_rows + lpb;
   const uint16_t* sp = sel0 - li;
   for (int s = 0; s < steps; ++s) {
-    const uint32_t left = __shfl_up_sync(0xFFFFFFFFu, last, 1, lpb) & lmask;
+    uint32_t left = __shfl_up_sync(0xFFFFFFFFu, last, 1, lpb);
+    left = lead ? M3 : left;  // column 0 boundary: H = 0
     const int g = s - li;
     if (g == next) {  // first row of a new pack (or the end of the stream)
       if (pk >= 0) {
@@ -67,25 +74,26 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
       }
       ++pk;
       mx = 0u;
-      diag = 0u;
+      diag = M3;
 #pragma unroll
-      for (int k = 0; k < W; ++k) H[k] = 0u;
+      for (int k = 0; k < W; ++k) E[k] = M3;
       next = (pk < npk) ? pstart[pk + 1] : 0x7FFFFFFF;
     }
     const uint32_t sel = sp[s];
-    uint32_t hd = diag;
-    uint32_t x = vmax0(left, H[0]);
+    uint32_t ed = diag, el = left, hprev = 0u;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const uint32_t d = prmt(tlo[k], thi[k], sel);
-      const uint32_t v = vaddmax(hd, d, x);
-      const uint32_t h = vaddmax0(v, M3, 0u);
-      if (k + 1 < W) x = vaddmax0(v, M3, H[k + 1]);
-      hd = H[k];
-      H[k] = h;
-      mx = vmax0(mx, h);
+      const uint32_t t = vadd(ed, d);
+      const uint32_t h = vmax3_0(t, el, E[k]);
+      ed = E[k];
+      el = vadd(h, M3);
+      E[k] = el;
+      if (k & 1) mx = vmax3_0(mx, hprev, h);
+      else if (k == W - 1) mx = vmax0(mx, h);
+      hprev = h;
     }
-    last = H[W - 1];
+    last = E[W - 1];
     diag = left;
   }
 }
@@ -496,8 +504,7 @@ cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, cons
 __global__ void __launch_bounds__(256) mix_probe_kernel(uint32_t* sink, int iters) {
   constexpr int C = 8;
   const uint32_t t = threadIdx.x + blockIdx.x * blockDim.x;
-  uint32_t h[C], x[C], m[C];
-  const uint32_t tlo = 0xFF07FFFFu ^ t, thi = 0xFFFF07FFu + t;
+  uint32_t h[C], x[C], m[C], tlo[C], thi[C];
   uint32_t sel = make_sel(t & 3, (t >> 2) & 3);
   const uint32_t M3 = 0xFFFDFFFDu;
 #pragma unroll
@@ -505,16 +512,22 @@ __global__ void __launch_bounds__(256) mix_probe_kernel(uint32_t* sink, int iter
     h[c] = (t * (c + 3)) & 0x00FF00FFu;
     x[c] = (t * (c + 7)) & 0x00FF00FFu;
     m[c] = 0u;
+    // a distinct table per chain, as each column has its own in the kernel,
+    // so no chain can reuse another chain's permute
+    tlo[c] = (0xFF07FFFFu ^ t) + 0x01010101u * (uint32_t)c;
+    thi[c] = (0xFFFF07FFu + t) ^ (0x00010000u * (uint32_t)c);
   }
+  // per packed cell update, as in fast_segment: PRMT, add, 3-input max, add,
+  // and half a 3-input max for the running maximum (two chains share one)
   for (int it = 0; it < iters; ++it) {
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const uint32_t d = prmt(tlo, thi, sel);
-      const uint32_t v = vaddmax(h[c], d, x[c]);
-      const uint32_t hn = vaddmax0(v, M3, 0u);
-      x[c] = vaddmax0(v, M3, h[c]);
+      const uint32_t d = prmt(tlo[c], thi[c], sel);
+      const uint32_t t = vadd(h[c], d);
+      const uint32_t hn = vmax3_0(t, x[c], h[c]);
+      x[c] = vadd(hn, M3);
       h[c] = hn;
-      m[c] = vmax0(m[c], hn);
+      if (c & 1) m[c] = vmax3_0(m[c], h[c - 1], hn);
     }
     sel ^= 0x0101u;
   }

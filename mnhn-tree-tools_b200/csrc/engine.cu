@@ -367,7 +367,8 @@ swe_status swe_upload(swe_ctx* ctx, const char* const* seqs, const size_t* lens,
     for (int pk = q * PB; pk < std::min(npacks, (q + 1) * PB); ++pk) {
       const int a = ctx->order[2 * pk];
       const int b = (2 * pk + 1 < nfast) ? ctx->order[2 * pk + 1] : -1;
-      const int R = std::max(ctx->len[a], b >= 0 ? ctx->len[b] : 0);
+      // an even row count: the 16x2 kernel processes two rows per step
+      const int R = (std::max(ctx->len[a], b >= 0 ? ctx->len[b] : 0) + 1) & ~1;
       pack_off[pk] = (int)row;
       pack_rows[pk] = R;
       row += R;

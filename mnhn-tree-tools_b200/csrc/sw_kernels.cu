@@ -35,11 +35,38 @@ namespace swgpu {
 //   t = E_diag + d               (packed add, FMA pipe)
 //   H = max(t, E_left, E_up, 0)  (3-input packed max, ALU pipe)
 //   E = H - 3                    (packed add, FMA pipe)
-// i.e. H = max(0, diag + s, left - 3, up - 3).  The running maximum takes two
-// cells per 3-input max.  Pad columns (beyond len B) and pad rows (code 7) only
-// ever see mismatches, so they can never raise the maximum above the real
-// cells' maximum.
+// i.e. H = max(0, diag + s, left - 3, up - 3).
+//
+// The running maximum is taken over t, two cells per 3-input max: the largest
+// H of a matrix is always reached on a diagonal step (a gap step only lowers
+// the score), so max(0, max t) = max H, and t - unlike H - is off the
+// left-neighbour dependency chain.
+//
+// A step processes two rows (packs have an even number of rows), which gives
+// every lane two interleavable dependency chains and halves the per-row
+// shuffle, selector-load and bookkeeping cost.  Pad columns (beyond len B) and
+// pad rows (code 7) only ever see mismatches, so they can never raise the
+// maximum above the real cells' maximum.
 // ---------------------------------------------------------------------------
+template <int W>
+__device__ __forceinline__ void fast_row(uint32_t (&E)[W], const uint32_t (&tlo)[W], const uint32_t (&thi)[W],
+                                         uint32_t sel, uint32_t ed, uint32_t el, uint32_t& mx) {
+  const uint32_t M3 = 0xFFFDFFFDu;
+  uint32_t tprev = 0u;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const uint32_t d = prmt(tlo[k], thi[k], sel);
+    const uint32_t t = vadd(ed, d);
+    const uint32_t h = vmax3_0(t, el, E[k]);
+    ed = E[k];
+    el = vadd(h, M3);
+    E[k] = el;
+    if (k & 1) mx = vmax3_0(mx, tprev, t);
+    else if (k == W - 1) mx = vmax0(mx, t);
+    tprev = t;
+  }
+}
+
 template <int W>
 __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, int total_rows,
                                              const int* __restrict__ pstart, int npk,
@@ -58,15 +85,18 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
     thi[k] = hi;
     E[k] = M3;
   }
-  uint32_t mx = 0u, last = M3, diag = M3;
+  uint32_t mx = 0u, last_a = M3, last_b = M3, diag = M3;
   int pk = -1, next = 0;
   const bool lead = (li == 0);
-  const int steps = total_rows + lpb;
-  const uint16_t* sp = sel0 - li;
+  const int steps = total_rows / 2 + lpb;
+  // two selectors per 32-bit word: rows 2q (low half) and 2q+1 (high half)
+  const uint32_t* sp = reinterpret_cast<const uint32_t*>(sel0) - li;
   for (int s = 0; s < steps; ++s) {
-    uint32_t left = __shfl_up_sync(0xFFFFFFFFu, last, 1, lpb);
-    left = lead ? M3 : left;  // column 0 boundary: H = 0
-    const int g = s - li;
+    uint32_t la = __shfl_up_sync(0xFFFFFFFFu, last_a, 1, lpb);
+    uint32_t lb = __shfl_up_sync(0xFFFFFFFFu, last_b, 1, lpb);
+    la = lead ? M3 : la;  // column 0 boundary: H = 0
+    lb = lead ? M3 : lb;
+    const int g = 2 * (s - li);  // first of the two rows
     if (g == next) {  // first row of a new pack (or the end of the stream)
       if (pk >= 0) {
         atomicMax(&smax[2 * pk], mx & 0xFFFFu);
@@ -79,29 +109,22 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
       for (int k = 0; k < W; ++k) E[k] = M3;
       next = (pk < npk) ? pstart[pk + 1] : 0x7FFFFFFF;
     }
-    const uint32_t sel = sp[s];
-    uint32_t ed = diag, el = left, hprev = 0u;
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const uint32_t d = prmt(tlo[k], thi[k], sel);
-      const uint32_t t = vadd(ed, d);
-      const uint32_t h = vmax3_0(t, el, E[k]);
-      ed = E[k];
-      el = vadd(h, M3);
-      E[k] = el;
-      if (k & 1) mx = vmax3_0(mx, hprev, h);
-      else if (k == W - 1) mx = vmax0(mx, h);
-      hprev = h;
-    }
-    last = E[W - 1];
-    diag = left;
+    const uint32_t sel2 = sp[s];
+    fast_row<W>(E, tlo, thi, sel2 & 0xFFFFu, diag, la, mx);
+    last_a = E[W - 1];
+    fast_row<W>(E, tlo, thi, sel2 >> 16, la, lb, mx);  // the diagonal of row b is row a's left
+    last_b = E[W - 1];
+    diag = lb;
   }
 }
 
-__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+// Shared selector buffer: SEL_FRONT pad rows before row 0 (lanes that have not
+// started read rows down to -2*(lanes-1) = -62) and SEL_TAIL after the last row
+// (lanes that have finished read up to rows + 2*lanes - 1).
+constexpr int SEL_FRONT = 64, SEL_TAIL = 80;
 
 __host__ __device__ inline size_t fast_sel_bytes(int max_block_rows) {
-  return ((size_t)(32 + max_block_rows + 40) * 2 + 15) & ~(size_t)15;
+  return ((size_t)(SEL_FRONT + max_block_rows + SEL_TAIL) * 2 + 15) & ~(size_t)15;
 }
 
 size_t fast_smem_bytes(int max_block_rows, int max_cols_per_cta, int packs_per_block) {
@@ -144,7 +167,7 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
   const int warp = tid >> 5, lane = tid & 31, nwarps = bd >> 5;
 
   if (tid == 0) mbar_init(&bar, 1);
-  for (int i = tid; i < 32; i += bd) s_sel[i] = SEL_PAD;
+  for (int i = tid; i < SEL_FRONT; i += bd) s_sel[i] = SEL_PAD;
   __syncthreads();
   uint32_t phase = 0;
 
@@ -177,7 +200,7 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
       // order earlier generic-proxy reads of s_sel before the async-proxy write
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive_expect_tx(&bar, (uint32_t)rows8 * 2u);
-      bulk_g2s(s_sel + 32, p.sel + row0, (uint32_t)rows8 * 2u, &bar);
+      bulk_g2s(s_sel + SEL_FRONT, p.sel + row0, (uint32_t)rows8 * 2u, &bar);
     }
     for (int i = tid; i <= npk; i += bd)
       s_pstart[i] = (i < npk ? p.pack_row_off[pk0 + i] : row0 + rows) - row0;
@@ -193,14 +216,14 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
     phase ^= 1u;
     __syncthreads();
     if (!s_ok) return;
-    for (int i = tid; i < 40; i += bd) s_sel[32 + rows + i] = SEL_PAD;
+    for (int i = tid; i < SEL_TAIL; i += bd) s_sel[SEL_FRONT + rows + i] = SEL_PAD;
     __syncthreads();
 
     const int spw = 32 / lpb;  // column sequences per warp
     if (warp * spw < tile.nb) {
       const int j = min(warp * spw + lane / lpb, tile.nb - 1);  // idle segments repeat the last one
       const int b = p.order[tile.b0 + j];
-      fast_dispatch(W, s_sel + 32, rows, s_pstart, npk, p.codes + p.code_off[b], p.len[b], lpb,
+      fast_dispatch(W, s_sel + SEL_FRONT, rows, s_pstart, npk, p.codes + p.code_off[b], p.len[b], lpb,
                     lane % lpb, s_max + (size_t)j * npk * 2);
     }
     __syncthreads();
@@ -527,7 +550,7 @@ __global__ void __launch_bounds__(256) mix_probe_kernel(uint32_t* sink, int iter
       const uint32_t hn = vmax3_0(t, x[c], h[c]);
       x[c] = vadd(hn, M3);
       h[c] = hn;
-      if (c & 1) m[c] = vmax3_0(m[c], h[c - 1], hn);
+      if (c & 1) m[c] = vmax3_0(m[c], x[c - 1], t);
     }
     sel ^= 0x0101u;
   }

@@ -304,6 +304,41 @@ def test_adaptive_tool_small(tmp_path):
         assert got == run["files"]
 
 
+def _ref_main(name):
+    exe = O.REF_DIR / f"{name}_on_swgpu"
+    if not exe.exists():
+        pytest.skip("reference mains relinked on libswgpu were not built (make -C oracle ref-dropin)")
+    return exe
+
+
+def test_reference_mains_linked_on_libswgpu(tmp_path):
+    """The reference's own cluster_dbscan_SW.c / adaptive_clustering.c /
+    find_closest_sequence_SW.c, compiled with the reference headers and linked
+    against libswgpu, reproduce the reference tools' outputs."""
+    seqs, _ = W.config1()
+    W.write_fasta(tmp_path / "c1.fa", seqs)
+    g = load_golden("config1_golden.json")
+    r = subprocess.run([str(_ref_main("cluster_dbscan_SW")), "c1.fa", "130", "5", "c1"], cwd=tmp_path,
+                       capture_output=True, timeout=1200)
+    assert r.returncode == 0 and r.stdout.decode() == g["dbscan"]["stdout"]
+    got = {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in sorted(tmp_path.glob("c1-*"))}
+    assert got == g["dbscan"]["files_sha256"]
+    a = g["adaptive"]
+    r = subprocess.run([str(_ref_main("adaptive_clustering_SW")), "c1.fa", str(a["eps_start"]), str(a["eps_inc"]),
+                        str(a["minpts"]), "lay", "1"], cwd=tmp_path, capture_output=True, timeout=1200)
+    assert r.returncode == 0 and r.stdout.decode() == a["stdout"]
+    got = {p.name: hashlib.sha256(p.read_bytes()).hexdigest() for p in sorted(tmp_path.glob("lay*"))}
+    assert got == a["files_sha256"]
+    doc = load_golden("find_closest_small.json")
+    W.write_fasta(tmp_path / "db.fa", [s.encode() for s in doc["db"]])
+    W.write_fasta(tmp_path / "q.fa", [s.encode() for s in doc["queries"]])
+    for run in doc["runs"]:
+        r = subprocess.run([str(_ref_main("find_closest_sequence_SW")), "db.fa", "q.fa", str(run["idx"]), "4",
+                            "o.fa"], cwd=tmp_path, capture_output=True, timeout=600)
+        assert r.returncode == 0 and r.stdout.decode() == run["stdout"]
+        assert (tmp_path / "o.fa").read_text() == run["out"]
+
+
 # ---------------------------------------------------------------------------
 # size-independent properties at the full config-2 size
 # ---------------------------------------------------------------------------

@@ -134,6 +134,38 @@ swe_status swe_measure_mix_peak(int device, double* cells_per_s, double* lane_in
 swe_status swe_timer_start(swe_ctx* ctx);
 swe_status swe_timer_stop(swe_ctx* ctx, double* ms);
 
+/* Allocation-free scoring of explicit pairs.  No counterpart in the reference
+   (which has no device API at all).
+
+   For callers that cannot allocate device memory: code running while a CUDA
+   graph is being captured, real-time or embedded hosts that must not call the
+   device allocator after start-up, and programs whose device memory belongs to
+   a pool this library cannot see.  The caller passes device buffers it already
+   owns; this call calls no cudaMalloc, cudaFree or other allocating routine.
+
+   seqs         device bytes; sequence i is the C string at seqs + off[i] of
+                length len[i] (readable at [0 .. len[i]], scored like score())
+   off, len     device arrays indexed by sequence
+   pairs        device int array of 2*npairs indices (a, b)
+   out          device array of npairs distances (0xFFFFFFFF for a pair whose
+                sequence is longer than max_len)
+   max_len      upper bound on every len[i] the pairs reference,
+                at most SWE_NOALLOC_MAX_LEN (larger values: SWE_ERR_INVALID)
+   stream       cudaStream_t to enqueue on (NULL: the default stream)
+
+   The work is only enqueued; synchronise the stream before reading `out`.
+   Long sequences need scratch, which is one fixed 4 MiB device array per GPU
+   (kept until the process exits), so a call runs at most 2^20/(max_len+1)
+   warps.  Every call on a device shares that array and it keeps the last
+   call's contents (each call writes every word before reading it): calls that
+   overlap on the GPU - on different streams or threads - race and must be
+   serialised by the caller.  The first call on a device looks up the array's
+   device address with that device current; make that first call before any
+   stream capture. */
+#define SWE_NOALLOC_MAX_LEN 65535
+swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* off, const int* len, const int* pairs,
+                                   int64_t npairs, unsigned* out, int max_len, void* stream);
+
 void swe_free(void* p);
 
 #ifdef __cplusplus

@@ -1,0 +1,131 @@
+// Allocation-free pair scoring: swe_score_pairs_noalloc.
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
+// being captured, real-time or embedded callers that must not touch the
+// device allocator after start-up, and hosts whose device memory is owned by a
+// pooling allocator that this library cannot see.  They already hold their
+// inputs and outputs on the device; this entry point scores pairs from those
+// buffers and allocates nothing.
+//
+// The 32-bit wavefront needs one scratch column per warp for sequences longer
+// than one 512-column chunk.  Here that scratch is a file-scope device array of
+// SWE_NOALLOC_SCRATCH_INTS ints (4 MiB, held by every GPU that loads the
+// library until the process exits).  Each warp gets max_len + 1 ints of it, so
+// a call runs min(1024, 2^20 / (max_len + 1)) warps; the longest sequence a
+// call may reference is SWE_NOALLOC_MAX_LEN symbols.
+//
+// Host code cannot pass the array's name to a kernel (on the host it is only a
+// stand-in for the device symbol), so the device address is looked up once per
+// device with cudaGetSymbolAddress, with that device current, on the first
+// call made on it.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "swgpu.h"
+#include "sw_kernels.cuh"
+#include "sw_wavefront32.cuh"
+
+namespace swgpu {
+
+constexpr int NOALLOC_SCRATCH_INTS = 1 << 20;
+static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_SCRATCH_INTS];
+
+struct NoAllocParams {
+  const char* seqs;      // sequence bytes; sequence i starts at seqs + off[i]
+  const int64_t* off;
+  const int* len;
+  const int* pairs;      // 2 * npairs indices (a, b)
+  long long npairs;
+  unsigned* out;         // npairs distances
+  int max_len;
+  int* scratch;          // device address of g_noalloc_scratch
+  long long stride;      // ints per warp = max_len + 1
+  int nwarps;
+};
+
+// One warp per pair, like the explicit-pair mode of generic_kernel, but the
+// sequences are caller-owned C strings (the effective symbols are s[1..len])
+// and the boundary columns live in the static scratch array.
+__global__ void __launch_bounds__(256) noalloc_pairs_kernel(NoAllocParams p) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  if (gw >= p.nwarps) return;
+  int* scratch = p.scratch + (long long)gw * p.stride;
+  for (long long w = gw; w < p.npairs; w += p.nwarps) {
+    const int ia = p.pairs[2 * w], ib = p.pairs[2 * w + 1];
+    const int la = p.len[ia], lb = p.len[ib];
+    if (la > p.max_len || lb > p.max_len || la < 0 || lb < 0) {
+      // longer than the caller declared: the scratch slice would overflow
+      if (lane == 0) p.out[w] = 0xFFFFFFFFu;
+      continue;
+    }
+    const uint8_t* A = reinterpret_cast<const uint8_t*>(p.seqs + p.off[ia]) + 1;
+    const uint8_t* B = reinterpret_cast<const uint8_t*>(p.seqs + p.off[ib]) + 1;
+    const uint8_t* R = A;
+    const uint8_t* Cc = B;
+    int lr = la, lc = lb;
+    if (lc > lr) {
+      R = B;
+      Cc = A;
+      lr = lb;
+      lc = la;
+    }
+    const int best = sw32_warp(R, lr, Cc, lc, scratch, lane);
+    if (lane == 0) p.out[w] = 4u * (unsigned)max(la, lb) - (unsigned)best;
+  }
+}
+
+namespace {
+std::mutex g_setup_mu;
+int* g_scratch_addr[64] = {nullptr};
+}  // namespace
+
+}  // namespace swgpu
+
+extern "C" swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* off, const int* len,
+                                              const int* pairs, int64_t npairs, unsigned* out, int max_len,
+                                              void* stream) {
+  using namespace swgpu;
+  if (npairs < 0 || max_len < 0 || max_len > SWE_NOALLOC_MAX_LEN) return SWE_ERR_INVALID;
+  if (npairs == 0) return SWE_OK;
+  if (!seqs || !off || !len || !pairs || !out) return SWE_ERR_INVALID;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return SWE_ERR_NO_DEVICE;
+  }
+  int* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!g_scratch_addr[dev]) {
+      void* addr = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+      if (e != cudaSuccess || !addr) {
+        cudaGetLastError();
+        return SWE_ERR_CUDA;
+      }
+      g_scratch_addr[dev] = static_cast<int*>(addr);
+    }
+    scratch = g_scratch_addr[dev];
+  }
+  NoAllocParams p;
+  p.seqs = seqs;
+  p.off = off;
+  p.len = len;
+  p.pairs = pairs;
+  p.npairs = npairs;
+  p.out = out;
+  p.max_len = max_len;
+  p.scratch = scratch;
+  p.stride = (long long)max_len + 1;
+  long long warps = NOALLOC_SCRATCH_INTS / p.stride;
+  if (warps > 1024) warps = 1024;
+  if (warps > npairs) warps = npairs;
+  p.nwarps = (int)warps;
+  const int blocks = (p.nwarps + 7) / 8;
+  noalloc_pairs_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  if (cudaGetLastError() != cudaSuccess) return SWE_ERR_CUDA;
+  return SWE_OK;
+}

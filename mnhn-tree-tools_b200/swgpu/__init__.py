@@ -80,7 +80,7 @@ EXPORTS = [
     "swe_strerror", "swe_create", "swe_destroy", "swe_last_error", "swe_upload",
     "swe_score_all_pairs", "swe_copy_distances", "swe_neighbors", "swe_dbscan", "swe_adaptive",
     "swe_score_one_to_many", "swe_score_pairs", "swe_get_stats", "swe_free", "swe_dbscan_bitmap",
-    "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop",
+    "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop", "swe_score_pairs_noalloc",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -131,6 +131,9 @@ def lib():
         L.swe_timer_start.argtypes = [C.c_void_p]
         L.swe_timer_stop.restype = C.c_int
         L.swe_timer_stop.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.swe_score_pairs_noalloc.restype = C.c_int
+        L.swe_score_pairs_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                              C.c_void_p, C.c_int, C.c_void_p]
         L.swe_dbscan_bitmap.restype = C.c_int
         L.swe_dbscan_bitmap.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(SplitSet)]
         L.score.restype = C.c_uint

@@ -44,13 +44,43 @@ static int not_covered_count(const split_set& s, int n) {
 
 static float coverage(int not_covered, int n) { return 1.f - (float)not_covered / (float)n; }
 
+split_set copy_split_set(const split_set& s) {
+  split_set c;
+  c.n_clusters = s.n_clusters;
+  c.clusters = (cluster*)malloc(sizeof(cluster) * (size_t)(s.n_clusters > 0 ? s.n_clusters : 1));
+  for (int i = 0; i < s.n_clusters; ++i) {
+    c.clusters[i] = s.clusters[i];
+    const size_t k = (size_t)(s.clusters[i].n_members > 0 ? s.clusters[i].n_members : 1);
+    c.clusters[i].members = (int*)malloc(sizeof(int) * k);
+    if (s.clusters[i].n_members > 0)
+      memcpy(c.clusters[i].members, s.clusters[i].members, sizeof(int) * (size_t)s.clusters[i].n_members);
+  }
+  return c;
+}
+
 int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
-                   const DbscanFn& fn, long long fixed_point, std::vector<split_set>* kept,
-                   std::string* err) {
+                   const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
+                   std::vector<split_set>* kept, std::string* err) {
   std::vector<split_set> sets;
   auto cleanup = [&]() {
     for (auto& s : sets) free_split_set_and_associated_clusters(s);
     sets.clear();
+  };
+  // dbscan.c:980-989, printed when the reference's dbscanner would run
+  auto warn = [&](float eps) {
+    if (!dbscan_sw_warnings) return;
+    if (eps == -1) {
+      fprintf(log, "Warning @dbscan: epsilon value is: %f\n", eps);
+      fprintf(log, "Warning @dbscan: epsilon was changed to: %f\n", 0.015f);
+    }
+    if (minpts == -1) {
+      fprintf(log, "Warning @dbscan: minpts value is: %i\n", minpts);
+      fprintf(log, "Warning @dbscan: minpts was changed to: %i\n", 5);
+    }
+  };
+  auto fn = [&](float eps, split_set* o) {
+    warn(eps);
+    return prov.run(&eps, 1, o);
   };
   fprintf(log,
           "Performing adaptive clustering with parameters: \n"
@@ -89,25 +119,41 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
 
   float eps_now = eps_start + eps_inc;
   int stop = -1;
-  for (;;) {
-    const float eps = eps_now;
-    eps_now = eps_now + eps_inc;
-    split_set s;
-    rc = fn(eps, &s);
+  const int batch = prov.batch > 0 ? prov.batch : 1;
+  while (stop < 0) {
+    // the next eps values of the sweep, evaluated together; a value past the
+    // largest distance (every later eps gives the same result) or an increment
+    // too small to move eps ends the batch, since the reference would loop
+    // forever after it
+    std::vector<float> eps;
+    bool terminal = false;
+    while ((int)eps.size() < batch) {
+      const float e = eps_now;
+      eps_now = eps_now + eps_inc;
+      eps.push_back(e);
+      if ((fixed_point >= 0 && eps_threshold(e) >= fixed_point) || !(eps_now > e)) {
+        terminal = true;
+        break;
+      }
+    }
+    std::vector<split_set> res(eps.size());
+    rc = prov.run(eps.data(), (int)eps.size(), res.data());
     if (rc) {
       cleanup();
       *err = "dbscan failed";
       return rc;
     }
-    sets.push_back(s);
-    if (s.n_clusters == 1) {
-      stop = (int)sets.size() - 1;
-      break;
+    size_t k = 0;
+    for (; k < eps.size(); ++k) {
+      warn(eps[k]);
+      sets.push_back(res[k]);
+      if (res[k].n_clusters == 1) {
+        stop = (int)sets.size() - 1;
+        break;
+      }
     }
-    // Past the largest distance every later eps gives this same result, and
-    // the reference would loop forever; so would an increment too small to
-    // move eps.
-    if ((fixed_point >= 0 && eps_threshold(eps) >= fixed_point) || !(eps_now > eps)) {
+    for (size_t j = k + 1; j < eps.size(); ++j) free_split_set_and_associated_clusters(res[j]);
+    if (stop < 0 && terminal) {
       cleanup();
       *err = "the sweep can never reach one cluster";
       return SWE_ERR_SWEEP;

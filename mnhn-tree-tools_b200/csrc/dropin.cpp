@@ -140,33 +140,36 @@ void adaptive_dbscan(split_set (*dbscanner)(dataset, float, int), dataset ds, fl
   (void)n_threads;  // layers are always produced in eps order
   std::lock_guard<std::mutex> lk(g_mu);
   g_status = 0;
-  swgpu::DbscanFn fn;
+  swgpu::DbscanProvider prov;
   long long fixed = -1;
+  bool engine = false;
   if (dbscanner == &dbscan_SW || dbscanner == nullptr) {
+    // one score pass; the sweep's DBSCAN runs share it (dbscan_SW's warnings
+    // are printed by the sweep for each run it consumes)
     swe_ctx* ctx = default_ctx();
     if (!ctx) return;
     if (int s = ensure_scored(ctx, ds)) {
       g_status = s;
       return;
     }
-    fn = [&ds, minpts](float eps, split_set* o) {
-      *o = dbscan_locked(ds, eps, minpts);
-      return g_status;
+    prov.run = [ctx, minpts](const float* e, int c, split_set* o) {
+      return swgpu::engine_dbscan_batch(ctx, e, c, minpts, o);
     };
+    prov.batch = swgpu::engine_batch_size(ctx);
     size_t mx = 0;
     for (int i = 0; i < ds.n_values; ++i) mx = ds.sequence_lengths[i] > mx ? ds.sequence_lengths[i] : mx;
     fixed = 4LL * (long long)mx;
+    engine = true;
   } else {
-    fn = [&ds, dbscanner, minpts](float eps, split_set* o) {
-      *o = dbscanner(ds, eps, minpts);
+    prov.run = [&ds, dbscanner, minpts](const float* e, int c, split_set* o) {
+      for (int k = 0; k < c; ++k) o[k] = dbscanner(ds, e[k], minpts);
       return 0;
     };
   }
   std::vector<split_set> kept;
   std::string err;
-  const int rc =
-      swgpu::adaptive_sweep(ds.n_values, epsilon_start, epsilon_inc, minpts, split_files_prefix, stdout, fn, fixed,
-                            &kept, &err);
+  const int rc = swgpu::adaptive_sweep(ds.n_values, epsilon_start, epsilon_inc, minpts, split_files_prefix,
+                                       stdout, prov, engine, fixed, &kept, &err);
   for (auto& s : kept) free_split_set_and_associated_clusters(s);
   if (rc) {
     if (rc != SWE_ERR_SWEEP) fprintf(stderr, "swgpu: adaptive_dbscan failed: %s\n", err.c_str());

@@ -14,6 +14,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "host_internal.h"
@@ -134,6 +135,11 @@ struct swe_ctx {
   HostPinned<uint64_t> h_bits;
   HostPinned<int> h_counts;
   long long bits_T = LLONG_MIN;
+  // batched sweeps: one bitmap slot per distinct threshold
+  DevBuf<uint64_t> d_bbits;
+  DevBuf<int> d_bcounts;
+  HostPinned<uint64_t> h_bbits;
+  HostPinned<int> h_bcounts;
 
   // small transfers
   DevBuf<uint8_t> d_q;
@@ -720,12 +726,14 @@ swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts
                         FILE* log, split_set** out_sets, int* out_n_sets) {
   if (!ctx) return SWE_ERR_INVALID;
   if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
-  DbscanFn fn = [ctx, minpts](float eps, split_set* o) { return (int)swe_dbscan(ctx, eps, minpts, o); };
+  DbscanProvider prov;
+  prov.run = [ctx, minpts](const float* e, int c, split_set* o) { return engine_dbscan_batch(ctx, e, c, minpts, o); };
+  prov.batch = engine_batch_size(ctx);
   std::vector<split_set> kept;
   std::string err;
   const long long fixed = 4LL * ctx->max_len;  // every distance is <= 4*max_len
-  const int rc = adaptive_sweep(ctx->n, eps_start, eps_inc, minpts, prefix, log ? log : stdout, fn, fixed,
-                                &kept, &err);
+  const int rc = adaptive_sweep(ctx->n, eps_start, eps_inc, minpts, prefix, log ? log : stdout, prov, true,
+                                fixed, &kept, &err);
   if (rc) {
     for (auto& s : kept) free_split_set_and_associated_clusters(s);
     return fail(ctx, (swe_status)rc, err);
@@ -873,6 +881,84 @@ swe_status swe_get_stats(const swe_ctx* ctx, swe_stats* out) {
 }  // extern "C"
 
 namespace swgpu {
+
+int engine_batch_size(const swe_ctx* ctx) {
+  const double bytes = (double)ctx->n * (double)((ctx->n + 63) / 64) * 8.0;
+  const double budget = 2.0 * 1024 * 1024 * 1024;  // device and pinned host bytes for one batch
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::max(1.0, std::min({8.0, (double)hw, budget / std::max(bytes, 1.0)}));
+}
+
+int engine_dbscan_batch(swe_ctx* ctx, const float* eps, int count, int minpts, split_set* out) {
+  for (int k = 0; k < count; ++k) out[k] = split_set{0, nullptr};
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  if (minpts == -1) minpts = 5;  // dbscan.c:985-989
+  const int n = ctx->n;
+  const int wpr = (n + 63) / 64;
+  const size_t words = (size_t)n * (size_t)wpr;
+  // distinct thresholds (eps == -1 means 0.015, dbscan.c:980-984)
+  std::vector<long long> uniq;
+  std::vector<int> slot(count);
+  for (int k = 0; k < count; ++k) {
+    const long long T = eps_threshold(eps[k] == -1 ? 0.015f : eps[k]);
+    const auto it = std::find(uniq.begin(), uniq.end(), T);
+    slot[k] = (int)(it - uniq.begin());
+    if (it == uniq.end()) uniq.push_back(T);
+  }
+  const int U = (int)uniq.size();
+  CK(ctx->h_bbits.alloc(std::max<size_t>(words * U, 1)));
+  CK(ctx->h_bcounts.alloc(std::max<size_t>((size_t)n * U, 1)));
+  bool any_gpu = false;
+  for (int u = 0; u < U; ++u) any_gpu |= (uniq[u] >= 0 && n > 0);
+  if (any_gpu) {
+    CK(ctx->d_bbits.alloc(words * U));
+    CK(ctx->d_bcounts.alloc((size_t)n * U));
+  }
+  CK(cudaEventRecord(ctx->ev[2], ctx->st));
+  for (int u = 0; u < U; ++u) {
+    uint64_t* hb = ctx->h_bbits.p + words * u;
+    int* hc = ctx->h_bcounts.p + (size_t)n * u;
+    if (uniq[u] < 0 || n == 0) {  // no neighbour at all, not even the point itself
+      if (words) memset(hb, 0, words * 8);
+      if (n) memset(hc, 0, sizeof(int) * n);
+      continue;
+    }
+    ctx->stats.kernel_launches += 1;
+    CK(launch_bitmap(ctx->d_D16.p, ctx->d_D32.p, n, uniq[u], ctx->d_bbits.p + words * u, wpr,
+                     ctx->d_bcounts.p + (size_t)n * u, ctx->st));
+    CK(cpy(ctx, hb, ctx->d_bbits.p + words * u, words * 8, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cpy(ctx, hc, ctx->d_bcounts.p + (size_t)n * u, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
+  }
+  CK(cudaEventRecord(ctx->ev[3], ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+  ctx->stats.ms_last_neighbors = ms;
+  // one order-faithful replay per distinct threshold, in parallel
+  std::vector<split_set> res(U, split_set{0, nullptr});
+  std::vector<int> rc(U, 0);
+  std::vector<std::thread> th;
+  for (int u = 0; u < U; ++u)
+    th.emplace_back([&, u]() {
+      rc[u] = dbscan_replay_bitmap(n, ctx->h_bbits.p + words * u, wpr, ctx->h_bcounts.p + (size_t)n * u, minpts,
+                                   &res[u]);
+    });
+  for (auto& t : th) t.join();
+  int bad = 0;
+  for (int u = 0; u < U; ++u) bad = bad ? bad : rc[u];
+  if (bad) {
+    for (auto& s : res) free_split_set_and_associated_clusters(s);
+    return fail(ctx, (swe_status)bad, "dbscan replay");
+  }
+  std::vector<bool> used(U, false);
+  for (int k = 0; k < count; ++k) {
+    const int u = slot[k];
+    out[k] = used[u] ? copy_split_set(res[u]) : res[u];
+    used[u] = true;
+  }
+  return SWE_OK;
+}
 
 long long eps_threshold(float eps) {
   if (!(eps >= 0.0f)) return -1;  // negative or NaN: not even the point itself

@@ -24,17 +24,35 @@ long long eps_threshold(float eps);
 int dbscan_replay_bitmap(int n, const uint64_t* bits, int words_per_row, const int* counts, int minpts,
                          split_set* out);
 
-// One DBSCAN run at eps (split set malloc'd); returns an swe_status.
-using DbscanFn = std::function<int(float eps, split_set* out)>;
+// DBSCAN runs for `count` eps values (split sets malloc'd, in the given
+// order); returns an swe_status.  `batch` is how many eps values the provider
+// prefers per call: the sweep evaluates that many upcoming eps values at once
+// and discards the ones past the one-cluster stop.
+struct DbscanProvider {
+  std::function<int(const float* eps, int count, split_set* out)> run;
+  int batch = 1;
+};
 
-// Adaptive sweep of dbscan.c:1117-1380 over a DBSCAN provider.  `fixed_point`
-// (when >= 0) is a threshold at or above which every eps gives the same
-// result, used to stop sweeps that could never reach one cluster (the
-// reference loops forever there).  Kept layers are returned in `kept`
+// Adaptive sweep of dbscan.c:1117-1380 over a DBSCAN provider.  With
+// `dbscan_sw_warnings` the warnings dbscan_SW prints for eps == -1 or
+// minpts == -1 (dbscan.c:980-989) are printed for every DBSCAN result the
+// sweep consumes, where the reference's dbscanner calls would print them.
+// `fixed_point` (when >= 0) is a threshold at or above which every eps gives
+// the same result, used to stop sweeps that could never reach one cluster
+// (the reference loops forever there).  Kept layers are returned in `kept`
 // (ownership passes to the caller).
 int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
-                   const DbscanFn& fn, long long fixed_point, std::vector<split_set>* kept,
-                   std::string* err);
+                   const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
+                   std::vector<split_set>* kept, std::string* err);
+
+// The engine's batched DBSCAN over its scored matrix: the GPU builds one
+// neighbour bitmap per distinct threshold and host threads replay them in
+// parallel.  Semantics of swe_dbscan for each eps.
+int engine_dbscan_batch(swe_ctx* ctx, const float* eps, int count, int minpts, split_set* out);
+int engine_batch_size(const swe_ctx* ctx);
+
+// Deep copy of a split set (malloc'd like the original).
+split_set copy_split_set(const split_set& s);
 
 // FASTA loading with dataset_from_fasta semantics (dataset.c:264-344).
 int fasta_read(FILE* in, dataset* out, std::string* err);

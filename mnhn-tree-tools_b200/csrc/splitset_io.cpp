@@ -4,6 +4,8 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -170,10 +172,70 @@ cluster intersection_of_clusters(cluster a, cluster b) {
   return out;
 }
 
-// cluster_io.c:407-444.
+// True when no index appears twice in the set (no duplicate inside a cluster,
+// no overlap between clusters) and all indices are >= 0; *max_id receives the
+// largest index.
+static bool partition_like(const split_set& s, std::vector<uint8_t>& seen, int* max_id) {
+  for (int c = 0; c < s.n_clusters; ++c)
+    for (int k = 0; k < s.clusters[c].n_members; ++k) {
+      const int m = s.clusters[c].members[k];
+      if (m < 0) return false;
+      if ((size_t)m >= seen.size()) seen.resize((size_t)m + 1 + seen.size() / 2, 0);
+      if (seen[m]) return false;
+      seen[m] = 1;
+      if (m > *max_id) *max_id = m;
+    }
+  return true;
+}
+
+// cluster_io.c:407-444.  The reference calls intersection_of_clusters for
+// every (new, ancient) pair, which sorts the larger cluster of the pair in
+// place when it has more than 20 members (cluster_io.c:467-469).  For split
+// sets that are partitions (every DBSCAN result is) the same connections and
+// the same sorted clusters come from one pass over the members: ancient
+// cluster j ends up sorted iff some new cluster is no larger than it, new
+// cluster i iff some ancient cluster is smaller.  Other inputs use the
+// pairwise computation.
 cluster_connections* generate_split_set_relation(split_set ancient, split_set new_set) {
   cluster_connections* c =
       (cluster_connections*)malloc(sizeof(cluster_connections) * (size_t)(new_set.n_clusters > 0 ? new_set.n_clusters : 1));
+  int max_id = -1;
+  std::vector<uint8_t> seen_a, seen_n;
+  if (ancient.n_clusters > 0 && new_set.n_clusters > 0 && partition_like(ancient, seen_a, &max_id) &&
+      partition_like(new_set, seen_n, &max_id)) {
+    std::vector<int> anc_of((size_t)max_id + 1, -1);
+    int min_a = INT_MAX, min_n = INT_MAX;
+    for (int j = 0; j < ancient.n_clusters; ++j) {
+      min_a = std::min(min_a, ancient.clusters[j].n_members);
+      for (int k = 0; k < ancient.clusters[j].n_members; ++k) anc_of[ancient.clusters[j].members[k]] = j;
+    }
+    for (int i = 0; i < new_set.n_clusters; ++i) min_n = std::min(min_n, new_set.clusters[i].n_members);
+    std::vector<int> cnt(ancient.n_clusters, 0), touched;
+    for (int i = 0; i < new_set.n_clusters; ++i) {
+      touched.clear();
+      for (int k = 0; k < new_set.clusters[i].n_members; ++k) {
+        const int j = anc_of[new_set.clusters[i].members[k]];
+        if (j < 0) continue;
+        if (cnt[j]++ == 0) touched.push_back(j);
+      }
+      std::sort(touched.begin(), touched.end());
+      std::vector<int> conn;
+      for (int j : touched) {
+        if ((double)cnt[j] > (double)ancient.clusters[j].n_members * (double)0.8) conn.push_back(j);
+        cnt[j] = 0;
+      }
+      c[i].n_connections = (int)conn.size();
+      c[i].connections = conn.empty() ? nullptr : (int*)malloc(sizeof(int) * conn.size());
+      if (c[i].connections) memcpy(c[i].connections, conn.data(), sizeof(int) * conn.size());
+    }
+    for (int j = 0; j < ancient.n_clusters; ++j)
+      if (ancient.clusters[j].n_members > 20 && ancient.clusters[j].n_members >= min_n)
+        qsort(ancient.clusters[j].members, (size_t)ancient.clusters[j].n_members, sizeof(int), cmp_int);
+    for (int i = 0; i < new_set.n_clusters; ++i)
+      if (new_set.clusters[i].n_members > 20 && new_set.clusters[i].n_members > min_a)
+        qsort(new_set.clusters[i].members, (size_t)new_set.clusters[i].n_members, sizeof(int), cmp_int);
+    return c;
+  }
   for (int i = 0; i < new_set.n_clusters; ++i) {
     std::vector<int> conn;
     for (int j = 0; j < ancient.n_clusters; ++j) {

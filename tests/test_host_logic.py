@@ -149,6 +149,48 @@ def test_relation_sorts_in_place_like_reference():
         assert [list(kn[1][i][: len(new[i])]) for i in range(len(new))] == new_py
 
 
+def test_relation_on_partitions_matches_pairwise_reference():
+    """Partitions (every DBSCAN result) take the one-pass relation; connections
+    and the in-place sorts must equal the reference's pairwise computation."""
+    L = swgpu.lib()
+
+    class Conn(C.Structure):
+        _fields_ = [("connections", C.POINTER(C.c_int)), ("n_connections", C.c_int)]
+
+    L.generate_split_set_relation.restype = C.POINTER(Conn)
+    L.generate_split_set_relation.argtypes = [swgpu.SplitSet, swgpu.SplitSet]
+    rng = np.random.default_rng(9)
+    for trial in range(40):
+        n = int(rng.integers(30, 900))
+
+        def partition(k, cover):
+            pts = rng.permutation(n)[: max(k, int(n * cover))]
+            cuts = sorted(rng.choice(np.arange(1, len(pts)), size=k - 1, replace=False).tolist())
+            return [pts[a:b].tolist() for a, b in zip([0] + cuts, cuts + [len(pts)])]
+
+        anc = partition(int(rng.integers(1, 25)), rng.uniform(0.3, 1.0))
+        if trial % 3 == 0:  # new layer = unions of ancient clusters plus strays
+            new, cur = [], []
+            for cl in anc:
+                cur = cur + cl
+                if rng.random() < 0.4:
+                    new.append(cur)
+                    cur = []
+            if cur:
+                new.append(cur)
+        else:
+            new = partition(int(rng.integers(1, 20)), rng.uniform(0.3, 1.0))
+        sa, ka = _make_split_set(anc)
+        sn, kn = _make_split_set(new)
+        conns = L.generate_split_set_relation(sa, sn)
+        got = [[conns[i].connections[k] for k in range(conns[i].n_connections)] for i in range(len(new))]
+        anc_py = [list(c) for c in anc]
+        new_py = [list(c) for c in new]
+        assert got == O.relation(anc_py, new_py), trial
+        assert [list(ka[1][i][: len(anc[i])]) for i in range(len(anc))] == anc_py, trial
+        assert [list(kn[1][i][: len(new[i])]) for i in range(len(new))] == new_py, trial
+
+
 def test_replay_matches_oracle_dbscan():
     doc = load_golden("dbscan_small.json")
     seqs = [s.encode() for s in doc["seqs"]]

@@ -176,6 +176,31 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def measured_traffic(kernel: str, workload: str):
+    """DRAM bytes (read + write) of one launch of `kernel` on `workload`, from
+    the committed ncu summary profiles/<kernel>_traffic.txt (lines
+    `<workload> <read bytes> <write bytes>`), or None."""
+    p = ROOT / "profiles" / f"{kernel}_traffic.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        parts = ln.split()
+        if len(parts) == 3 and parts[0] == workload:
+            return int(float(parts[1]) + float(parts[2]))
+    return None
+
+
+def hbm_peak_gbs():
+    """(GB/s, source) of the measured HBM copy bandwidth of this GPU pool."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "of measured (copy bandwidth)"
+        except Exception:
+            pass
+    return 6650.0, "of fallback"
+
+
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
@@ -254,6 +279,14 @@ def run_gpu(args):
     value = cells * world / (ms_per_step * 1e-3) / 1e9
     launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
 
+    # the eps threshold kernel alone (HBM-bound): one launch per distinct
+    # threshold, timed by the engine's CUDA events around the launch
+    thr_ms = []
+    for k in range(3):
+        eng.dbscan((wl.get("eps") or wl["eps_start"]) + k, wl["minpts"])
+        thr_ms.append(eng.stats()["ms_last_neighbors"])
+    thr_ms = statistics.median(thr_ms)
+
     # e2e through the C ABI with host buffers: upload + score + sweep + results on the host
     e2e_ms = []
     b0 = eng.stats()
@@ -282,13 +315,11 @@ def run_gpu(args):
         # R = 2 * P_int / K: P_int = lane instructions/s of the per-cell mix at full
         # issue on this GPU, K = 4.5 instructions per packed cell pair in that mix
         roof_peak = 2.0 * peak_instr / 4.5 / 1e9
-        prof = ROOT / "profiles" / "traffic.json"
-        traffic = None
-        if prof.exists():
-            try:
-                traffic = json.loads(prof.read_text()).get("fast_all_pairs_kernel_config2_bytes_per_launch")
-            except Exception:
-                traffic = None
+        traffic = measured_traffic("fast_all_pairs_kernel", f"config{args.config}") if not args.n else None
+        n = len(seqs)
+        dist_bytes = st1["dist_bytes"]
+        thr_bytes = n * n * dist_bytes + n * ((n + 63) // 64) * 8 + n * 4
+        hbm_peak = hbm_peak_gbs()
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             g, info = reference_sample(seqs, target_s=args.ref_seconds)
@@ -312,6 +343,10 @@ def run_gpu(args):
                          "peak_source": "measured on this GPU: issue rate of the kernel's per-cell 16x2 "
                                         "instruction mix on independent chains, R = 2*P_int/4.5",
                          "traffic": traffic},
+            "threshold_roofline": {"bound": "hbm", "kernel": "bitmap_kernel", "achieved": round(
+                thr_bytes / (thr_ms * 1e-3) / 1e9, 1), "peak": hbm_peak[0], "unit": "GB/s",
+                "frac": round(thr_bytes / (thr_ms * 1e-3) / 1e9 / hbm_peak[0], 4), "peak_source": hbm_peak[1],
+                "bytes_per_launch": thr_bytes, "ms_per_launch": round(thr_ms, 4)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -61,7 +61,8 @@ typedef struct {
   int64_t n_tiles;
   double ms_score_pass;    /* device time of the last score pass */
   double ms_fast_kernel;   /* device time of the 16x2 kernel inside it */
-  double ms_last_neighbors;/* device time of the last eps threshold pass */
+  double ms_last_neighbors;/* device time of the last eps threshold kernels */
+  int64_t last_neighbor_launches; /* threshold kernels timed in ms_last_neighbors */
   int dist_bytes;          /* 2 (uint16 matrix) or 4 */
   int64_t h2d_bytes;       /* host->device bytes since the last upload began */
   int64_t d2h_bytes;       /* device->host bytes since the last upload began */
@@ -80,9 +81,26 @@ const char* swe_last_error(const swe_ctx* ctx);
    does (it is the NUL terminator for C strings), as in smith-waterman.c:56-58. */
 swe_status swe_upload(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n);
 
+/* Copies n sequences forming n_sets independent sets: set k holds the
+   sequences [set_first[k], set_first[k+1]) (set_first has n_sets+1 entries,
+   set_first[0] = 0, set_first[n_sets] = n, non-decreasing).  One score pass
+   then scores every pair inside each set and no pair across sets: the many
+   split sets of one cluster-tree level in one launch.  swe_upload is this call
+   with one set.  The single-set calls below (swe_copy_distances, swe_neighbors,
+   swe_dbscan, swe_adaptive) refuse an upload of several sets with
+   SWE_ERR_STATE; their _set forms take the set index, and inside a set
+   sequence indices are relative to set_first[set]. */
+swe_status swe_upload_sets(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n,
+                           const int* set_first, int n_sets);
+int swe_set_count(const swe_ctx* ctx);
+
 /* Scores every pair of the uploaded sequences into the device distance matrix
    (one pass; later neighbour/DBSCAN calls reuse it). */
 swe_status swe_score_all_pairs(swe_ctx* ctx);
+
+/* n_s x n_s distance matrix of one set (n_s = its size), row-major in the
+   set's index order. */
+swe_status swe_copy_set_distances(swe_ctx* ctx, int set, uint32_t* out);
 
 /* Copies the n x n distance matrix to host memory (out holds n*n entries). */
 swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out);
@@ -104,6 +122,12 @@ swe_status swe_dbscan(swe_ctx* ctx, float eps, int minpts, split_set* out);
    free_split_set_and_associated_clusters, then the array with swe_free). */
 swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, const char* prefix,
                         FILE* log, split_set** out_sets, int* out_n_sets);
+
+/* The same three calls on one set of a several-set upload. */
+swe_status swe_neighbors_set(swe_ctx* ctx, int set, float eps, int64_t** row_ptr, int** cols);
+swe_status swe_dbscan_set(swe_ctx* ctx, int set, float eps, int minpts, split_set* out);
+swe_status swe_adaptive_set(swe_ctx* ctx, int set, float eps_start, float eps_inc, int minpts, const char* prefix,
+                            FILE* log, split_set** out_sets, int* out_n_sets);
 
 /* Distances of one query to every uploaded sequence (out holds n entries).
    q must be readable at [0 .. qlen]. */

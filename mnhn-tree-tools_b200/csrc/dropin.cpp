@@ -153,9 +153,9 @@ void adaptive_dbscan(split_set (*dbscanner)(dataset, float, int), dataset ds, fl
       return;
     }
     prov.run = [ctx, minpts](const float* e, int c, split_set* o) {
-      return swgpu::engine_dbscan_batch(ctx, e, c, minpts, o);
+      return swgpu::engine_dbscan_batch(ctx, 0, e, c, minpts, o);
     };
-    prov.batch = swgpu::engine_batch_size(ctx);
+    prov.batch = swgpu::engine_batch_size(ctx, 0);
     size_t mx = 0;
     for (int i = 0; i < ds.n_values; ++i) mx = ds.sequence_lengths[i] > mx ? ds.sequence_lengths[i] : mx;
     fixed = 4LL * (long long)mx;

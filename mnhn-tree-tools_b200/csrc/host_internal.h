@@ -47,9 +47,9 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
 
 // The engine's batched DBSCAN over its scored matrix: the GPU builds one
 // neighbour bitmap per distinct threshold and host threads replay them in
-// parallel.  Semantics of swe_dbscan for each eps.
-int engine_dbscan_batch(swe_ctx* ctx, const float* eps, int count, int minpts, split_set* out);
-int engine_batch_size(const swe_ctx* ctx);
+// parallel.  Semantics of swe_dbscan_set for each eps.
+int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int minpts, split_set* out);
+int engine_batch_size(const swe_ctx* ctx, int set);
 
 // Deep copy of a split set (malloc'd like the original).
 split_set copy_split_set(const split_set& s);

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_tile;
   __shared__ int s_ok;
-  const int PB = p.packs_per_block;
+  const int PB = p.max_packs_per_block;
   uint16_t* s_sel = reinterpret_cast<uint16_t*>(smem);
   unsigned* s_max = reinterpret_cast<unsigned*>(smem + fast_sel_bytes(p.max_block_rows));
   int* s_pstart = reinterpret_cast<int*>(s_max + (size_t)p.max_cols_per_cta * PB * 2);
@@ -179,9 +179,9 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
     if (t >= p.ntiles) break;
     const FastTile tile = p.tiles[t];
     const int W = tile.wl & 0xFF, lpb = tile.wl >> 8;
-    const int pk0 = tile.q * PB;
-    const int npk = min(PB, p.npacks - pk0);
-    bool bad = (W < 1 || W > FAST_MAX_W || (lpb != 8 && lpb != 16 && lpb != 32) || npk <= 0 ||
+    const int pk0 = p.block_first[tile.q];
+    const int npk = p.block_npacks[tile.q];
+    bool bad = (W < 1 || W > FAST_MAX_W || (lpb != 8 && lpb != 16 && lpb != 32) || npk <= 0 || npk > PB ||
                 tile.nb < 1 || tile.nb > p.max_cols_per_cta || tile.nb > nwarps * (32 / max(lpb, 1)));
     int row0 = 0, rows = 0, rows8 = 0;
     if (!bad) {
@@ -223,36 +223,47 @@ __global__ void __launch_bounds__(256, 2) fast_all_pairs_kernel(FastParams p) {
     const int spw = 32 / lpb;  // column sequences per warp
     if (warp * spw < tile.nb) {
       const int j = min(warp * spw + lane / lpb, tile.nb - 1);  // idle segments repeat the last one
-      const int b = p.order[tile.b0 + j];
+      const int b = p.L.orig[tile.b0 + j];
       fast_dispatch(W, s_sel + SEL_FRONT, rows, s_pstart, npk, p.codes + p.code_off[b], p.len[b], lpb,
                     lane % lpb, s_max + (size_t)j * npk * 2);
     }
     __syncthreads();
 
-    // epilogue: distances of this tile's pairs
-    for (int i = tid; i < tile.nb * npk * 2; i += bd) {
-      const int j = i / (npk * 2);
-      const int r = i - j * npk * 2;
-      const int apos = (pk0 + (r >> 1)) * 2 + (r & 1);
-      if (apos >= p.nfast) continue;
-      const int a = p.order[apos], b = p.order[tile.b0 + j];
+    // epilogue: this tile's distances.  Row sequences of a block and column
+    // sequences of a tile are consecutive in the set's sorted order, so the
+    // first pass (row sequence fastest) writes contiguous runs of row b of the
+    // set's matrix and the second pass (column sequence fastest) contiguous
+    // runs of row a.
+    const int s = tile.set;
+    const int first = p.L.set_first[s], ns = p.L.set_n[s];
+    const long long base = p.L.set_base[s];
+    const int nr = npk * 2;
+    for (int i = tid; i < tile.nb * nr; i += bd) {
+      const int j = i / nr, r = i - j * nr;
+      const int pk = pk0 + (r >> 1);
+      if ((r & 1) && !p.pack_pair[pk]) continue;
+      const int ga = p.pack_first[pk] + (r & 1), gb = tile.b0 + j;
+      const int a = p.L.orig[ga], b = p.L.orig[gb];
       const unsigned m = s_max[i];
       if ((int)m >= p.sat_limit) {
         const unsigned slot = atomicAdd(p.rerun_count, 1u);
-        if (slot < p.rerun_cap) p.rerun[slot] = make_int2(a, b);
+        if (slot < p.rerun_cap) p.rerun[slot] = make_int2(ga, gb);
         else atomicOr(p.status, KST_RERUN_OVERFLOW);
         continue;
       }
-      const unsigned d = 4u * (unsigned)max(p.len[a], p.len[b]) - m;
-      const size_t ab = (size_t)a * (size_t)p.n + (size_t)b;
-      const size_t ba = (size_t)b * (size_t)p.n + (size_t)a;
-      if (p.D16) {
-        p.D16[ab] = (uint16_t)d;
-        p.D16[ba] = (uint16_t)d;
-      } else {
-        p.D32[ab] = d;
-        p.D32[ba] = d;
-      }
+      store_dist(p.L, base + (long long)(gb - first) * ns + (ga - first),
+                 4u * (unsigned)max(p.len[a], p.len[b]) - m);
+    }
+    for (int i = tid; i < tile.nb * nr; i += bd) {
+      const int r = i / tile.nb, j = i - r * tile.nb;
+      const int pk = pk0 + (r >> 1);
+      if ((r & 1) && !p.pack_pair[pk]) continue;
+      const unsigned m = s_max[j * nr + r];
+      if ((int)m >= p.sat_limit) continue;  // queued for the 32-bit rerun above
+      const int ga = p.pack_first[pk] + (r & 1), gb = tile.b0 + j;
+      const int a = p.L.orig[ga], b = p.L.orig[gb];
+      store_dist(p.L, base + (long long)(ga - first) * ns + (gb - first),
+                 4u * (unsigned)max(p.len[a], p.len[b]) - m);
     }
     __syncthreads();
   }
@@ -281,18 +292,21 @@ cudaError_t launch_fast(const FastParams& p, int grid, int block, size_t smem, c
 // ---------------------------------------------------------------------------
 // Row selector stream: one 16-bit PRMT selector per row of each pack.
 // ---------------------------------------------------------------------------
+// Rows of a pack beyond both sequences (the even-row padding) get the pad
+// selector; rows between blocks are filled with it by the host's memset.
 __global__ void build_sel_kernel(const uint8_t* __restrict__ codes, const int64_t* __restrict__ code_off,
-                                 const int* __restrict__ len, const int* __restrict__ order, int nfast,
-                                 const int* __restrict__ pack_row_off, int npacks, uint16_t* sel) {
+                                 const int* __restrict__ len, const int* __restrict__ orig,
+                                 const int* __restrict__ pack_first, const uint8_t* __restrict__ pack_pair,
+                                 const int* __restrict__ pack_row_off, const int* __restrict__ pack_rows,
+                                 int npacks, uint16_t* sel) {
   for (int pk = blockIdx.x; pk < npacks; pk += gridDim.x) {
-    const int pa = 2 * pk, pb = 2 * pk + 1;
-    const int a = order[pa];
-    const int b = pb < nfast ? order[pb] : -1;
+    const int a = orig[pack_first[pk]];
+    const int b = pack_pair[pk] ? orig[pack_first[pk] + 1] : -1;
     const int la = len[a], lb = b >= 0 ? len[b] : 0;
     const uint8_t* ca = codes + code_off[a];
     const uint8_t* cb = b >= 0 ? codes + code_off[b] : nullptr;
-    const int r0 = pack_row_off[pk], r1 = pack_row_off[pk + 1];
-    for (int r = threadIdx.x; r < r1 - r0; r += blockDim.x) {
+    const int r0 = pack_row_off[pk], R = pack_rows[pk];
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
       const int x = r < la ? (int)ca[r] : CODE_ROWPAD;
       const int y = r < lb ? (int)cb[r] : CODE_ROWPAD;
       sel[r0 + r] = make_sel(x, y);
@@ -300,12 +314,12 @@ __global__ void build_sel_kernel(const uint8_t* __restrict__ codes, const int64_
   }
 }
 
-cudaError_t launch_build_sel(const uint8_t* codes, const int64_t* code_off, const int* len,
-                             const int* order, int nfast, const int* pack_row_off, int npacks,
-                             uint16_t* sel, cudaStream_t st) {
+cudaError_t launch_build_sel(const uint8_t* codes, const int64_t* code_off, const int* len, const int* orig,
+                             const int* pack_first, const uint8_t* pack_pair, const int* pack_row_off,
+                             const int* pack_rows, int npacks, uint16_t* sel, cudaStream_t st) {
   if (npacks <= 0) return cudaSuccess;
-  build_sel_kernel<<<min(npacks, 65535), 128, 0, st>>>(codes, code_off, len, order, nfast, pack_row_off,
-                                                       npacks, sel);
+  build_sel_kernel<<<min(npacks, 65535), 128, 0, st>>>(codes, code_off, len, orig, pack_first, pack_pair,
+                                                       pack_row_off, pack_rows, npacks, sel);
   return cudaGetLastError();
 }
 
@@ -316,24 +330,43 @@ __global__ void __launch_bounds__(256) generic_kernel(GenParams p) {
   if (p.mode == GEN_PAIRS || p.mode == GEN_PAIRS_OUT)
     total = p.npairs_dev ? (long long)*p.npairs_dev : p.npairs;
   else if (p.mode == GEN_EXC_CROSS)
-    total = (long long)p.nexc * p.n;
+    total = p.exc_pre[p.nexc];
   else
     total = p.n;
   int* scratch = p.scratch ? p.scratch + (long long)gw * p.scratch_stride : nullptr;
   for (long long w = gw; w < total; w += p.nwarps_total) {
-    int ia = -1, ib = -1;
+    int ia = -1, ib = -1;  // original indices
+    int ga = -1, gb = -1;  // global sorted indices (matrix modes)
     const uint8_t *A, *B;
     int la, lb;
-    if (p.mode == GEN_PAIRS || p.mode == GEN_PAIRS_OUT) {
+    if (p.mode == GEN_PAIRS_OUT) {
       const int2 pr = p.pairs[w];
       ia = pr.x;
       ib = pr.y;
+    } else if (p.mode == GEN_PAIRS) {
+      const int2 pr = p.pairs[w];
+      ga = pr.x;
+      gb = pr.y;
     } else if (p.mode == GEN_EXC_CROSS) {
-      ia = p.exc[w / p.n];
-      ib = (int)(w % p.n);
-      if (p.is_exc[ib] && ib < ia) continue;  // that pair belongs to row ib
+      // exceptional sequence e pairs with every sequence of its set
+      int lo = 0, hi = p.nexc - 1;
+      while (lo < hi) {  // last e with exc_pre[e] <= w
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.exc_pre[mid] <= w) lo = mid;
+        else hi = mid - 1;
+      }
+      ga = p.exc[lo];
+      const int s = p.L.set_of[p.L.orig[ga]];
+      const int first = p.L.set_first[s];
+      gb = first + (int)(w - p.exc_pre[lo]);
+      // a pair of two exceptional sequences belongs to the lower one
+      if (gb - first >= p.L.set_nfast[s] && gb < ga) continue;
     } else {
       ib = (int)w;
+    }
+    if (ga >= 0) {
+      ia = p.L.orig[ga];
+      ib = p.L.orig[gb];
     }
     if (p.mode == GEN_QUERY) {
       A = p.qcodes;
@@ -360,15 +393,11 @@ __global__ void __launch_bounds__(256) generic_kernel(GenParams p) {
       if (p.mode == GEN_QUERY || p.mode == GEN_PAIRS_OUT) {
         p.out[w] = d;
       } else {
-        const size_t ab = (size_t)ia * (size_t)p.n + (size_t)ib;
-        const size_t ba = (size_t)ib * (size_t)p.n + (size_t)ia;
-        if (p.D16) {
-          p.D16[ab] = (uint16_t)d;
-          p.D16[ba] = (uint16_t)d;
-        } else {
-          p.D32[ab] = d;
-          p.D32[ba] = d;
-        }
+        const int s = p.L.set_of[ia];
+        const int first = p.L.set_first[s], ns = p.L.set_n[s];
+        const long long base = p.L.set_base[s];
+        store_dist(p.L, base + (long long)(ga - first) * ns + (gb - first), d);
+        store_dist(p.L, base + (long long)(gb - first) * ns + (ga - first), d);
       }
     }
   }
@@ -379,62 +408,108 @@ cudaError_t launch_generic(const GenParams& p, int grid, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-__global__ void diag_kernel(uint16_t* D16, uint32_t* D32, int n) {
+// Self-distances are 0 (a sequence aligns with itself on the diagonal).
+__global__ void diag_kernel(DistLayout L, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const size_t k = (size_t)i * (size_t)n + (size_t)i;
-    if (D16) D16[k] = 0;
-    else D32[k] = 0u;
+    const int s = L.set_of[i], q = L.pos[i];
+    store_dist(L, L.set_base[s] + (long long)q * L.set_n[s] + q, 0u);
   }
 }
 
-cudaError_t launch_diag(uint16_t* D16, uint32_t* D32, int n, cudaStream_t st) {
+cudaError_t launch_diag(const DistLayout& L, int n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  diag_kernel<<<min((n + 255) / 256, 4096), 256, 0, st>>>(D16, D32, n);
+  diag_kernel<<<min((n + 255) / 256, 4096), 256, 0, st>>>(L, n);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Neighbour bitmap: one warp per row, 2048 columns per iteration.
+// Neighbour bitmap of one set.  One CTA per row i (original order): the row
+// pos[i] of the set's sorted matrix is staged in shared memory when it fits,
+// then each warp builds 64-bit words of the row's bits in original column
+// order by gathering through pos[].
 // ---------------------------------------------------------------------------
-template <typename DT>
-__global__ void __launch_bounds__(256) bitmap_kernel(const DT* __restrict__ D, int n, long long T,
-                                                     uint64_t* __restrict__ bits, int wpr,
+constexpr int BITMAP_STAGE_MAX = 200 * 1024;
+
+size_t bitmap_smem_bytes(int n_s, int dist_bytes) {
+  const size_t b = (size_t)n_s * (size_t)dist_bytes;
+  return b <= (size_t)BITMAP_STAGE_MAX ? ((b + 15) & ~(size_t)15) : 0;
+}
+
+template <typename DT, bool STAGE>
+__global__ void __launch_bounds__(256) bitmap_kernel(const DT* __restrict__ Dset, const int* __restrict__ pos,
+                                                     int ns, long long T, uint64_t* __restrict__ bits, int wpr,
                                                      int* __restrict__ counts) {
-  const int lane = threadIdx.x & 31;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-    const DT* row = D + (size_t)i * (size_t)n;
-    uint64_t* out = bits + (size_t)i * (size_t)wpr;
-    int cnt = 0;
-    for (int base = 0; base < n; base += 2048) {
-      uint64_t mine = 0;
-      uint32_t lo = 0;
-#pragma unroll 4
-      for (int j = 0; j < 64; ++j) {
-        const int col = base + 32 * j + lane;
-        const bool v = col < n && (long long)row[col] <= T;
-        const uint32_t b = __ballot_sync(0xFFFFFFFFu, v);
-        if ((j & 1) == 0) {
-          lo = b;
-        } else if (lane == (j >> 1)) {
-          mine = (uint64_t)lo | ((uint64_t)b << 32);
-        }
-      }
-      const int w = (base >> 6) + lane;
-      if (w < wpr) out[w] = mine;
-      cnt += __popcll(mine);
+  extern __shared__ __align__(16) uint8_t bm_smem[];
+  DT* srow = reinterpret_cast<DT*>(bm_smem);
+  __shared__ int s_cnt[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int i = blockIdx.x; i < ns; i += gridDim.x) {
+    const DT* row = Dset + (long long)pos[i] * ns;
+    if (STAGE) {
+      for (int k = threadIdx.x; k < ns; k += blockDim.x) srow[k] = row[k];
+      __syncthreads();
     }
-    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
-    if (lane == 0) counts[i] = cnt;
+    const DT* src = STAGE ? srow : row;
+    int cnt = 0;
+    for (int w = warp; w < wpr; w += nwarps) {
+      const int c0 = w * 64 + lane, c1 = c0 + 32;
+      const bool v0 = c0 < ns && (long long)src[pos[c0]] <= T;
+      const bool v1 = c1 < ns && (long long)src[pos[c1]] <= T;
+      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, v0), hi = __ballot_sync(0xFFFFFFFFu, v1);
+      if (lane == 0) bits[(size_t)i * wpr + w] = (uint64_t)lo | ((uint64_t)hi << 32);
+      cnt += __popc(lo) + __popc(hi);
+    }
+    if (lane == 0) s_cnt[warp] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c = 0;
+      for (int k = 0; k < nwarps; ++k) c += s_cnt[k];
+      counts[i] = c;
+    }
+    __syncthreads();  // srow and s_cnt are reused by the next row
   }
 }
 
-cudaError_t launch_bitmap(const uint16_t* D16, const uint32_t* D32, int n, long long T, uint64_t* bits,
-                          int words_per_row, int* counts, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  const int grid = min((n + 7) / 8, 148 * 16);
-  if (D16) bitmap_kernel<uint16_t><<<grid, 256, 0, st>>>(D16, n, T, bits, words_per_row, counts);
-  else bitmap_kernel<uint32_t><<<grid, 256, 0, st>>>(D32, n, T, bits, words_per_row, counts);
+cudaError_t bitmap_set_smem_limit(size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(bitmap_kernel<uint16_t, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(bitmap_kernel<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes);
+  return e;
+}
+
+cudaError_t launch_bitmap_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s,
+                              long long T, uint64_t* bits, int words_per_row, int* counts, cudaStream_t st) {
+  if (n_s <= 0) return cudaSuccess;
+  const int grid = min(n_s, 148 * 8);
+  const size_t smem = bitmap_smem_bytes(n_s, D16set ? 2 : 4);
+  if (D16set) {
+    if (smem) bitmap_kernel<uint16_t, true><<<grid, 256, smem, st>>>(D16set, pos, n_s, T, bits, words_per_row, counts);
+    else bitmap_kernel<uint16_t, false><<<grid, 256, 0, st>>>(D16set, pos, n_s, T, bits, words_per_row, counts);
+  } else {
+    if (smem) bitmap_kernel<uint32_t, true><<<grid, 256, smem, st>>>(D32set, pos, n_s, T, bits, words_per_row, counts);
+    else bitmap_kernel<uint32_t, false><<<grid, 256, 0, st>>>(D32set, pos, n_s, T, bits, words_per_row, counts);
+  }
+  return cudaGetLastError();
+}
+
+// Set matrix in original index order, widened to 32 bits.
+template <typename DT>
+__global__ void __launch_bounds__(256) unpermute_kernel(const DT* __restrict__ Dset, const int* __restrict__ pos,
+                                                        int ns, int r0, int r1, uint32_t* __restrict__ out) {
+  for (int i = r0 + blockIdx.x; i < r1; i += gridDim.x) {
+    const DT* row = Dset + (long long)pos[i] * ns;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) out[(size_t)(i - r0) * ns + k] = (uint32_t)row[pos[k]];
+  }
+}
+
+cudaError_t launch_unpermute_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s, int r0,
+                                 int r1, uint32_t* out, cudaStream_t st) {
+  if (n_s <= 0 || r1 <= r0) return cudaSuccess;
+  const int grid = min(r1 - r0, 148 * 8);
+  if (D16set) unpermute_kernel<uint16_t><<<grid, 256, 0, st>>>(D16set, pos, n_s, r0, r1, out);
+  else unpermute_kernel<uint32_t><<<grid, 256, 0, st>>>(D32set, pos, n_s, r0, r1, out);
   return cudaGetLastError();
 }
 

@@ -11,31 +11,53 @@ constexpr int FAST_MAX_LEN = 768;  // 32 lanes x 24 columns
 constexpr int GEN_W = 16;          // columns per lane in the 32-bit kernel (chunk = 512)
 constexpr int GEN_CHUNK = 32 * GEN_W;
 
-// Tile of the 16x2 all-pairs kernel: up to `nb` column sequences (sorted
-// positions b0..b0+nb-1) against A-block `q` (packs q*PB .. q*PB+PB-1).
+// Distance storage.  An upload holds one or more independent sets (contiguous
+// ranges of original indices).  Inside a set, sequences are ordered by
+// length (packed-path sequences longest first, then the 32-bit-path ones), and
+// the set's n_s x n_s matrix is stored in that sorted order, so a tile of
+// neighbouring sorted sequences writes contiguous runs.  A global sorted
+// index g = set_first[s] + position runs over all sets.
+struct DistLayout {
+  const int* orig;            // global sorted index -> original index
+  const int* pos;             // original index -> position in its set's sorted order
+  const int* set_of;          // original index -> set
+  const int* set_first;       // set -> first index (original and global sorted alike)
+  const int* set_n;           // set -> size
+  const int* set_nfast;       // set -> sequences on the packed path (positions 0..nfast-1)
+  const long long* set_base;  // set -> offset of its matrix in D
+  uint16_t* D16;              // one of D16 / D32 is non-null
+  uint32_t* D32;
+};
+
+__device__ __forceinline__ void store_dist(const DistLayout& L, long long idx, unsigned d) {
+  if (L.D16) L.D16[idx] = (uint16_t)d;
+  else L.D32[idx] = d;
+}
+
+// Tile of the 16x2 all-pairs kernel: `nb` column sequences (global sorted
+// indices b0..b0+nb-1, all in set `set`) against row block `q`.
 // wl = W | (lanes per column sequence << 8).
 struct FastTile {
-  int b0, nb, q, wl;
+  int b0, nb, q, wl, set;
 };
 
 struct FastParams {
   const uint8_t* codes;      // effective symbol codes, all sequences
   const int64_t* code_off;   // per original index
   const int* len;            // per original index
-  const int* order;          // sorted fast position -> original index
-  int nfast;                 // number of fast sequences
+  DistLayout L;
   const uint16_t* sel;       // row selectors, packs back to back
-  const int* pack_row_off;   // [npacks+1] start row of each pack (blocks 8-row aligned)
-  const int* pack_rows;      // [npacks] rows of each pack
-  int npacks;
-  int packs_per_block;       // PB
+  const int* pack_first;     // [npacks] global sorted index of a pack's first sequence
+  const uint8_t* pack_pair;  // [npacks] 1 when the pack has a second sequence (pack_first + 1)
+  const int* pack_row_off;   // [npacks] start row of each pack (blocks 8-row aligned)
+  const int* pack_rows;      // [npacks] rows of each pack (even)
+  const int* block_first;    // [nblocks] first pack of each row block
+  const int* block_npacks;   // [nblocks] packs in each row block
+  int max_packs_per_block;   // PB
   const FastTile* tiles;
   int ntiles;
   unsigned* tile_counter;
-  uint16_t* D16;             // n x n output (one of D16 / D32 is non-null)
-  uint32_t* D32;
-  int n;
-  int2* rerun;               // pairs whose 16-bit maximum reached sat_limit
+  int2* rerun;               // global sorted index pairs whose 16-bit maximum reached sat_limit
   unsigned* rerun_count;
   unsigned rerun_cap;
   int sat_limit;
@@ -48,10 +70,10 @@ struct FastParams {
 
 // Generic 32-bit kernel: one warp per pair, any length, any symbols.
 enum GenMode : int {
-  GEN_PAIRS = 0,     // explicit (a, b) list; results to the matrix
-  GEN_EXC_CROSS = 1, // every exceptional sequence against every sequence
-  GEN_QUERY = 2,     // external query against sequences [0, n); results to out[]
-  GEN_PAIRS_OUT = 3, // explicit (a, b) list; results to out[]
+  GEN_PAIRS = 0,     // explicit pairs of global sorted indices; results to the matrix
+  GEN_EXC_CROSS = 1, // every 32-bit-path sequence against every sequence of its set
+  GEN_QUERY = 2,     // external query against original indices [0, n); results to out[]
+  GEN_PAIRS_OUT = 3, // explicit pairs of original indices; results to out[]
 };
 
 struct GenParams {
@@ -60,16 +82,15 @@ struct GenParams {
   const int64_t* code_off;
   const int* len;
   int n;
+  DistLayout L;                 // GEN_PAIRS / GEN_EXC_CROSS
   const int2* pairs;            // GEN_PAIRS / GEN_PAIRS_OUT
   long long npairs;             // used when npairs_dev == nullptr
   const unsigned* npairs_dev;   // device-resident pair count (rerun queue)
-  const int* exc;               // GEN_EXC_CROSS
+  const int* exc;               // GEN_EXC_CROSS: global sorted indices, ascending
+  const long long* exc_pre;     // GEN_EXC_CROSS: [nexc+1] prefix sums of the sets' sizes
   int nexc;
-  const uint8_t* is_exc;
   const uint8_t* qcodes;        // GEN_QUERY: effective query codes
   int qlen;
-  uint16_t* D16;
-  uint32_t* D32;
   unsigned* out;                // GEN_QUERY / GEN_PAIRS_OUT
   int* scratch;                 // per-warp boundary column, scratch_stride ints each
   long long scratch_stride;
@@ -78,23 +99,33 @@ struct GenParams {
 };
 
 // Launchers (stream-ordered; no synchronisation).
-cudaError_t launch_build_sel(const uint8_t* codes, const int64_t* code_off, const int* len,
-                             const int* order, int nfast, const int* pack_row_off, int npacks,
-                             uint16_t* sel, cudaStream_t st);
+cudaError_t launch_build_sel(const uint8_t* codes, const int64_t* code_off, const int* len, const int* orig,
+                             const int* pack_first, const uint8_t* pack_pair, const int* pack_row_off,
+                             const int* pack_rows, int npacks, uint16_t* sel, cudaStream_t st);
 cudaError_t launch_fast(const FastParams& p, int grid, int block, size_t smem, cudaStream_t st);
 size_t fast_smem_bytes(int max_block_rows, int max_cols_per_cta, int packs_per_block);
 cudaError_t fast_set_smem_limit(size_t bytes);
 int fast_occupancy(int block, size_t smem);
 cudaError_t launch_generic(const GenParams& p, int grid, cudaStream_t st);
-cudaError_t launch_diag(uint16_t* D16, uint32_t* D32, int n, cudaStream_t st);
-// Neighbour bitmap for threshold T: bit k of row i set iff D[i][k] <= T.
-cudaError_t launch_bitmap(const uint16_t* D16, const uint32_t* D32, int n, long long T,
-                          uint64_t* bits, int words_per_row, int* counts, cudaStream_t st);
+// Zero self-distances of every sequence.
+cudaError_t launch_diag(const DistLayout& L, int n, cudaStream_t st);
+// Neighbour bitmap of one set for threshold T, rows and columns in the set's
+// original index order: bit k of row i is set iff D_s[pos i][pos k] <= T;
+// counts[i] is row i's popcount.  D16set / D32set point at the set's matrix
+// (one is null) and pos at the set's slice of the position table.
+cudaError_t launch_bitmap_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s,
+                              long long T, uint64_t* bits, int words_per_row, int* counts, cudaStream_t st);
+size_t bitmap_smem_bytes(int n_s, int dist_bytes);
+cudaError_t bitmap_set_smem_limit(size_t bytes);
+// Rows [r0, r1) of one set's matrix in original index order, widened to 32
+// bits (out holds (r1 - r0) x n_s entries).
+cudaError_t launch_unpermute_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s, int r0,
+                                 int r1, uint32_t* out, cudaStream_t st);
 // CSR from a bitmap: ascending column indices per row at row_ptr[i].
 cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, const long long* row_ptr,
                             int* cols, cudaStream_t st);
-// Throughput probe of the 16x2 cell instruction mix (PRMT + 3 add-max + max)
-// over independent chains; each thread runs `iters` cells on each of 8 chains.
+// Throughput probe of the 16x2 per-cell instruction mix over independent
+// chains; each thread runs `iters` cells on each of 8 chains.
 cudaError_t launch_mix_probe(uint32_t* sink, int grid, int block, int iters, cudaStream_t st);
 
 }  // namespace swgpu

@@ -65,6 +65,7 @@ class Stats(C.Structure):
                 ("unique_pairs", C.c_int64), ("cells", C.c_double), ("tile_cells", C.c_double),
                 ("reruns", C.c_int64), ("n_tiles", C.c_int64), ("ms_score_pass", C.c_double),
                 ("ms_fast_kernel", C.c_double), ("ms_last_neighbors", C.c_double),
+                ("last_neighbor_launches", C.c_int64),
                 ("dist_bytes", C.c_int), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
                 ("kernel_launches", C.c_int64)]
 
@@ -81,6 +82,8 @@ EXPORTS = [
     "swe_score_all_pairs", "swe_copy_distances", "swe_neighbors", "swe_dbscan", "swe_adaptive",
     "swe_score_one_to_many", "swe_score_pairs", "swe_get_stats", "swe_free", "swe_dbscan_bitmap",
     "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop", "swe_score_pairs_noalloc",
+    "swe_upload_sets", "swe_set_count", "swe_copy_set_distances", "swe_neighbors_set", "swe_dbscan_set",
+    "swe_adaptive_set",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -118,6 +121,20 @@ def lib():
         L.swe_adaptive.restype = C.c_int
         L.swe_adaptive.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_void_p,
                                    C.POINTER(C.POINTER(SplitSet)), C.POINTER(C.c_int)]
+        L.swe_upload_sets.restype = C.c_int
+        L.swe_upload_sets.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.swe_set_count.restype = C.c_int
+        L.swe_set_count.argtypes = [C.c_void_p]
+        L.swe_copy_set_distances.restype = C.c_int
+        L.swe_copy_set_distances.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.swe_neighbors_set.restype = C.c_int
+        L.swe_neighbors_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p)]
+        L.swe_dbscan_set.restype = C.c_int
+        L.swe_dbscan_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.POINTER(SplitSet)]
+        L.swe_adaptive_set.restype = C.c_int
+        L.swe_adaptive_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_int, C.c_char_p,
+                                       C.c_void_p, C.POINTER(C.POINTER(SplitSet)), C.POINTER(C.c_int)]
         L.swe_score_one_to_many.restype = C.c_int
         L.swe_score_one_to_many.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p]
         L.swe_score_pairs.restype = C.c_int
@@ -203,19 +220,48 @@ class Engine:
         self._buf = SeqBuffer(seqs)
         _check(lib().swe_upload(self.ctx, self._buf.ptrs, self._buf.lens, self._buf.n), self.ctx)
         self.n = self._buf.n
+        self.set_first = [0, self.n]
+
+    def upload_sets(self, sets):
+        """Uploads independent sets (a list of sequence lists); pairs are
+        scored only inside a set."""
+        flat = [q for st in sets for q in st]
+        first = np.zeros(len(sets) + 1, dtype=np.int32)
+        first[1:] = np.cumsum([len(st) for st in sets])
+        self._buf = SeqBuffer(flat)
+        _check(lib().swe_upload_sets(self.ctx, self._buf.ptrs, self._buf.lens, self._buf.n, first.ctypes.data,
+                                     len(sets)), self.ctx)
+        self.n = self._buf.n
+        self.set_first = first.tolist()
+
+    def set_count(self) -> int:
+        return lib().swe_set_count(self.ctx)
+
+    def set_size(self, set: int) -> int:
+        return self.set_first[set + 1] - self.set_first[set]
 
     def score_all_pairs(self):
         _check(lib().swe_score_all_pairs(self.ctx), self.ctx)
 
-    def distances(self) -> np.ndarray:
-        out = np.zeros((self.n, self.n), dtype=np.uint32)
-        _check(lib().swe_copy_distances(self.ctx, out.ctypes.data), self.ctx)
+    def distances(self, set: int | None = None) -> np.ndarray:
+        if set is None:
+            out = np.zeros((self.n, self.n), dtype=np.uint32)
+            _check(lib().swe_copy_distances(self.ctx, out.ctypes.data), self.ctx)
+        else:
+            ns = self.set_size(set)
+            out = np.zeros((ns, ns), dtype=np.uint32)
+            _check(lib().swe_copy_set_distances(self.ctx, set, out.ctypes.data), self.ctx)
         return out
 
-    def neighbors(self, eps: float):
+    def neighbors(self, eps: float, set: int | None = None):
         rp, cols = C.c_void_p(), C.c_void_p()
-        _check(lib().swe_neighbors(self.ctx, C.c_float(eps), C.byref(rp), C.byref(cols)), self.ctx)
-        row_ptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int64)), shape=(self.n + 1,)).copy()
+        if set is None:
+            _check(lib().swe_neighbors(self.ctx, C.c_float(eps), C.byref(rp), C.byref(cols)), self.ctx)
+            n = self.n
+        else:
+            _check(lib().swe_neighbors_set(self.ctx, set, C.c_float(eps), C.byref(rp), C.byref(cols)), self.ctx)
+            n = self.set_size(set)
+        row_ptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int64)), shape=(n + 1,)).copy()
         E = int(row_ptr[-1])
         c = (np.ctypeslib.as_array(C.cast(cols, C.POINTER(C.c_int32)), shape=(max(E, 1),))[:E].copy()
              if E else np.zeros(0, dtype=np.int32))
@@ -223,15 +269,18 @@ class Engine:
         lib().swe_free(cols)
         return row_ptr, c
 
-    def dbscan(self, eps: float, minpts: int):
+    def dbscan(self, eps: float, minpts: int, set: int | None = None):
         s = SplitSet()
-        _check(lib().swe_dbscan(self.ctx, C.c_float(eps), minpts, C.byref(s)), self.ctx)
+        if set is None:
+            _check(lib().swe_dbscan(self.ctx, C.c_float(eps), minpts, C.byref(s)), self.ctx)
+        else:
+            _check(lib().swe_dbscan_set(self.ctx, set, C.c_float(eps), minpts, C.byref(s)), self.ctx)
         out = split_set_to_lists(s)
         lib().free_split_set_and_associated_clusters(s)
         return out
 
     def adaptive(self, eps_start: float, eps_inc: float, minpts: int, prefix: str | None = None,
-                 log_path: str | None = None):
+                 log_path: str | None = None, set: int | None = None):
         """Runs the sweep; returns (log text, kept split sets as lists)."""
         libc = C.CDLL(None)
         libc.fopen.restype = C.c_void_p
@@ -246,8 +295,13 @@ class Engine:
         f = libc.fopen(log_path.encode(), b"w")
         sets = C.POINTER(SplitSet)()
         nsets = C.c_int()
-        st = lib().swe_adaptive(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts,
-                                prefix.encode() if prefix else None, f, C.byref(sets), C.byref(nsets))
+        pre = prefix.encode() if prefix else None
+        if set is None:
+            st = lib().swe_adaptive(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts, pre, f,
+                                    C.byref(sets), C.byref(nsets))
+        else:
+            st = lib().swe_adaptive_set(self.ctx, set, C.c_float(eps_start), C.c_float(eps_inc), minpts, pre, f,
+                                        C.byref(sets), C.byref(nsets))
         libc.fclose(f)
         text = Path(log_path).read_text()
         if tmp:

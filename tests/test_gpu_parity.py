@@ -160,6 +160,53 @@ def test_long_sequences_need_uint32_matrix():
             assert D[i, k] == O.score(seqs[k], seqs[i]), (i, k)
 
 
+def test_many_sets_in_one_upload_match_one_by_one():
+    """Independent sets scored in one pass: each set's matrix equals the oracle's
+    for that set alone (no pair across sets), and per-set neighbourhoods and
+    DBSCAN equal the single-set results.  Sizes include empty and one-sequence
+    sets and sets with 32-bit-path sequences only."""
+    rng = np.random.default_rng(31)
+    mixed = _mixed_set(rng)
+    pool, _ = W.config1()
+    sets = [pool[:150], [], [pool[200]], mixed[:20], [b"", b"N" * 3, b"ACGT" * 300], pool[300:301] * 5,
+            mixed, pool[400:1000], [pool[1100], pool[1101]]]
+    e = swgpu.Engine()
+    e.upload_sets(sets)
+    assert e.set_count() == len(sets)
+    e.score_all_pairs()
+    with pytest.raises(swgpu.SwgpuError):
+        e.distances()
+    with pytest.raises(swgpu.SwgpuError):
+        e.dbscan(100.0, 5)
+    for k, st in enumerate(sets):
+        D = e.distances(set=k)
+        ref = O.all_pairs(st) if st else np.zeros((0, 0), dtype=np.uint32)
+        bad = np.argwhere(D != ref)
+        assert len(bad) == 0, (k, [(int(i), int(j), int(D[i, j]), int(ref[i, j])) for i, j in bad[:5]])
+        for eps, mp in [(130.0, 5), (600.0, 2), (-1.0, 3)]:
+            assert e.dbscan(eps, mp, set=k) == O.dbscan(ref, 0.015 if eps == -1 else eps, mp), (k, eps)
+        rp, cols = e.neighbors(90.0, set=k)
+        for i in range(len(st)):
+            want = np.nonzero(ref[i].astype(np.float32) <= np.float32(90.0))[0]
+            assert np.array_equal(cols[rp[i]:rp[i + 1]], want), (k, i)
+    e.close()
+
+
+def test_adaptive_per_set_matches_single_set_runs(tmp_path):
+    sets, _ = W.config5(n_sets=6, lo=50, hi=400)
+    e = swgpu.Engine()
+    e.upload_sets(sets)
+    e.score_all_pairs()
+    runs = [e.adaptive(150.0, 50.0, 5, set=k) for k in range(len(sets))]
+    e.close()
+    e1 = swgpu.Engine()
+    for k, st in enumerate(sets):
+        e1.upload(st)
+        e1.score_all_pairs()
+        assert e1.adaptive(150.0, 50.0, 5) == runs[k], k
+    e1.close()
+
+
 # ---------------------------------------------------------------------------
 # neighbourhoods, DBSCAN, adaptive sweep
 # ---------------------------------------------------------------------------

@@ -129,6 +129,33 @@ swe_status swe_dbscan_set(swe_ctx* ctx, int set, float eps, int minpts, split_se
 swe_status swe_adaptive_set(swe_ctx* ctx, int set, float eps_start, float eps_inc, int minpts, const char* prefix,
                             FILE* log, split_set** out_sets, int* out_n_sets);
 
+/* Result of one set's sweep in swe_adaptive_sets. */
+typedef struct {
+  int status;          /* swe_status of this set's sweep */
+  int truncated;       /* 1 when max_steps ended the sweep before a one-cluster result */
+  int steps;           /* DBSCAN runs of the sweep phase (after the starting eps) */
+  int n_layers;        /* kept layers */
+  split_set* layers;   /* malloc'd array of the kept layers */
+  char* log;           /* malloc'd NUL-terminated log text of the sweep (the lines
+                          swe_adaptive would print for this set alone) */
+  double done_ms;      /* host milliseconds from the call's start to this set's end */
+} swe_sweep_result;
+
+/* Adaptive sweeps of every uploaded set at once (the cluster tree's split
+   sets of one level).  Each set runs the sweep of swe_adaptive_set with the
+   same parameters, bounded to max_steps DBSCAN runs after the starting eps
+   (0 = unbounded, as in the reference).  The sweeps advance in rounds: each
+   round one threshold launch serves the pending eps values of every active
+   set, then host threads replay the DBSCAN runs and advance the sweeps.  A
+   set's layers and log equal what swe_adaptive_set would produce for it with
+   the same bound.  With prefix not NULL, set k's layers are stored as
+   <prefix><k>_%04d.  results holds swe_set_count() entries; release them
+   with swe_free_sweep_results.  The call fails only on CUDA or allocation
+   errors; a set whose sweep fails has its own status. */
+swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, int max_steps,
+                             const char* prefix, swe_sweep_result* results);
+void swe_free_sweep_results(swe_sweep_result* results, int n);
+
 /* Distances of one query to every uploaded sequence (out holds n entries).
    q must be readable at [0 .. qlen]. */
 swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsigned* out);

@@ -14,7 +14,9 @@
 //     the split sets are stored as <prefix>%04d (dbscan.c:1346-1354).
 // The reference ends the process with _exit(1) on a failed start search; here
 // the same message is printed and SWE_ERR_SWEEP is returned.
+#include <algorithm>
 #include <cmath>
+#include <cstdarg>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -30,7 +32,7 @@ float layer_eps(float eps_start, int i, float eps_inc) {
   return std::fmaf((float)(i + 1), eps_inc, eps_start);
 }
 
-static int not_covered_count(const split_set& s, int n) {
+int not_covered_count(const split_set& s, int n) {
   std::vector<uint8_t> seen(n > 0 ? n : 1, 0);
   for (int c = 0; c < s.n_clusters; ++c)
     for (int k = 0; k < s.clusters[c].n_members; ++k) {
@@ -42,7 +44,7 @@ static int not_covered_count(const split_set& s, int n) {
   return cnt;
 }
 
-static float coverage(int not_covered, int n) { return 1.f - (float)not_covered / (float)n; }
+float coverage(int not_covered, int n) { return 1.f - (float)not_covered / (float)n; }
 
 split_set copy_split_set(const split_set& s) {
   split_set c;
@@ -58,126 +60,164 @@ split_set copy_split_set(const split_set& s) {
   return c;
 }
 
-int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
-                   const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
-                   std::vector<split_set>* kept, std::string* err) {
-  std::vector<split_set> sets;
-  auto cleanup = [&]() {
-    for (auto& s : sets) free_split_set_and_associated_clusters(s);
-    sets.clear();
-  };
-  // dbscan.c:980-989, printed when the reference's dbscanner would run
-  auto warn = [&](float eps) {
-    if (!dbscan_sw_warnings) return;
-    if (eps == -1) {
-      fprintf(log, "Warning @dbscan: epsilon value is: %f\n", eps);
-      fprintf(log, "Warning @dbscan: epsilon was changed to: %f\n", 0.015f);
-    }
-    if (minpts == -1) {
-      fprintf(log, "Warning @dbscan: minpts value is: %i\n", minpts);
-      fprintf(log, "Warning @dbscan: minpts was changed to: %i\n", 5);
-    }
-  };
-  auto fn = [&](float eps, split_set* o) {
-    warn(eps);
-    return prov.run(&eps, 1, o);
-  };
-  fprintf(log,
-          "Performing adaptive clustering with parameters: \n"
-          "minpts: %i\n"
-          "epsilon_start: %f\n"
-          "epsilon_inc: %f\n",
-          minpts, eps_start, eps_inc);
-  split_set first;
-  int rc = fn(eps_start, &first);
-  if (rc) {
-    *err = "dbscan failed";
-    return rc;
+void SweepMachine::say(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  const int k = vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (k > 0) log_.append(buf, (size_t)std::min<int>(k, (int)sizeof buf - 1));
+}
+
+// dbscan.c:980-989, printed where the reference's dbscanner call would print them
+void SweepMachine::warn(float eps) {
+  if (!warnings_) return;
+  if (eps == -1) {
+    say("Warning @dbscan: epsilon value is: %f\n", eps);
+    say("Warning @dbscan: epsilon was changed to: %f\n", 0.015f);
   }
-  fprintf(log, "Initial set obtained with %i clusters\n", first.n_clusters);
-  int counter = 0;
-  while (first.n_clusters == 1) {
-    if (counter == 20 || eps_start == 0) {
-      fprintf(log, "Error did not find a sufficient starting position in 20 tries \n");
+  if (minpts_ == -1) {
+    say("Warning @dbscan: minpts value is: %i\n", minpts_);
+    say("Warning @dbscan: minpts was changed to: %i\n", 5);
+  }
+}
+
+SweepMachine::SweepMachine(int n, float eps_start, float eps_inc, int minpts, int max_steps, int batch,
+                           bool dbscan_sw_warnings, long long fixed_point)
+    : n_(n), eps_start_(eps_start), eps_inc_(eps_inc), minpts_(minpts), max_steps_(max_steps),
+      batch_(batch > 0 ? batch : 1), warnings_(dbscan_sw_warnings), fixed_(fixed_point) {
+  say("Performing adaptive clustering with parameters: \n"
+      "minpts: %i\n"
+      "epsilon_start: %f\n"
+      "epsilon_inc: %f\n",
+      minpts, eps_start, eps_inc);
+  req_.assign(1, eps_start_);
+  phase_ = FIRST;
+}
+
+SweepMachine::~SweepMachine() {
+  for (auto& s : sets_) free_split_set_and_associated_clusters(s);
+}
+
+void SweepMachine::fail(int status, const char* why) {
+  status_ = status;
+  err_ = why;
+  req_.clear();
+  phase_ = DONE;
+}
+
+void SweepMachine::next_sweep_batch() {
+  // the next eps values of the sweep, evaluated together; a value past the
+  // largest distance (every later eps gives the same result) or an increment
+  // too small to move eps ends the batch, since the reference would loop
+  // forever after it
+  req_.clear();
+  terminal_ = false;
+  int room = batch_;
+  if (max_steps_ > 0) room = std::min(room, max_steps_ - steps_);
+  while ((int)req_.size() < room) {
+    const float e = eps_now_;
+    eps_now_ = eps_now_ + eps_inc_;
+    req_.push_back(e);
+    if ((fixed_ >= 0 && eps_threshold(e) >= fixed_) || !(eps_now_ > e)) {
+      terminal_ = true;
+      break;
+    }
+  }
+}
+
+void SweepMachine::consume(split_set* res) {
+  const size_t count = req_.size();
+  if (phase_ == FIRST || phase_ == HALVING) {
+    warn(req_[0]);
+    split_set first = res[0];
+    if (phase_ == FIRST) say("Initial set obtained with %i clusters\n", first.n_clusters);
+    if (first.n_clusters == 1) {
+      if (counter_ == 20 || eps_start_ == 0) {
+        say("Error did not find a sufficient starting position in 20 tries \n");
+        free_split_set_and_associated_clusters(first);
+        fail(SWE_ERR_SWEEP, "no starting eps with more than one cluster");
+        return;
+      }
+      eps_start_ = eps_start_ / 2;
+      say("Trying new starting point \n");
       free_split_set_and_associated_clusters(first);
-      *err = "no starting eps with more than one cluster";
-      return SWE_ERR_SWEEP;
+      counter_++;
+      req_.assign(1, eps_start_);
+      phase_ = HALVING;
+      return;
     }
-    eps_start = eps_start / 2;
-    fprintf(log, "Trying new starting point \n");
-    free_split_set_and_associated_clusters(first);
-    rc = fn(eps_start, &first);
-    if (rc) {
-      *err = "dbscan failed";
-      return rc;
+    say("Sarting with %i clusters\n", first.n_clusters);
+    say("Coverage at initial point: %f\n", coverage(not_covered_count(first, n_), n_));
+    sets_.push_back(first);
+    eps_now_ = eps_start_ + eps_inc_;
+    phase_ = SWEEP;
+    if (max_steps_ > 0 && steps_ >= max_steps_) {
+      truncated_ = true;
+      stop_ = 0;
+      req_.clear();
+      phase_ = DONE;
+      return;
     }
-    counter++;
+    next_sweep_batch();
+    return;
   }
-  fprintf(log, "Sarting with %i clusters\n", first.n_clusters);
-  fprintf(log, "Coverage at initial point: %f\n", coverage(not_covered_count(first, n), n));
-  sets.push_back(first);
-
-  float eps_now = eps_start + eps_inc;
-  int stop = -1;
-  const int batch = prov.batch > 0 ? prov.batch : 1;
-  while (stop < 0) {
-    // the next eps values of the sweep, evaluated together; a value past the
-    // largest distance (every later eps gives the same result) or an increment
-    // too small to move eps ends the batch, since the reference would loop
-    // forever after it
-    std::vector<float> eps;
-    bool terminal = false;
-    while ((int)eps.size() < batch) {
-      const float e = eps_now;
-      eps_now = eps_now + eps_inc;
-      eps.push_back(e);
-      if ((fixed_point >= 0 && eps_threshold(e) >= fixed_point) || !(eps_now > e)) {
-        terminal = true;
-        break;
-      }
-    }
-    std::vector<split_set> res(eps.size());
-    rc = prov.run(eps.data(), (int)eps.size(), res.data());
-    if (rc) {
-      cleanup();
-      *err = "dbscan failed";
-      return rc;
-    }
-    size_t k = 0;
-    for (; k < eps.size(); ++k) {
-      warn(eps[k]);
-      sets.push_back(res[k]);
-      if (res[k].n_clusters == 1) {
-        stop = (int)sets.size() - 1;
-        break;
-      }
-    }
-    for (size_t j = k + 1; j < eps.size(); ++j) free_split_set_and_associated_clusters(res[j]);
-    if (stop < 0 && terminal) {
-      cleanup();
-      *err = "the sweep can never reach one cluster";
-      return SWE_ERR_SWEEP;
+  if (phase_ != SWEEP) return;
+  size_t k = 0;
+  for (; k < count; ++k) {
+    warn(req_[k]);
+    sets_.push_back(res[k]);
+    ++steps_;
+    if (res[k].n_clusters == 1) {
+      stop_ = (int)sets_.size() - 1;
+      break;
     }
   }
+  for (size_t j = k + 1; j < count; ++j) free_split_set_and_associated_clusters(res[j]);
+  if (stop_ >= 0) {
+    req_.clear();
+    phase_ = DONE;
+    return;
+  }
+  if (max_steps_ > 0 && (steps_ >= max_steps_ || terminal_)) {
+    // the step budget ends the sweep: the layers found so far are kept
+    truncated_ = true;
+    stop_ = (int)sets_.size() - 1;
+    req_.clear();
+    phase_ = DONE;
+    return;
+  }
+  if (terminal_) {
+    fail(SWE_ERR_SWEEP, "the sweep can never reach one cluster");
+    return;
+  }
+  next_sweep_batch();
+}
 
+void SweepMachine::abort(int status, const char* why) { fail(status, why); }
+
+void SweepMachine::finish(const char* prefix, std::vector<split_set>* kept) {
+  kept->clear();
+  if (status_ || stop_ < 0) return;
   std::vector<split_set> keep;
   std::vector<cluster_connections*> conns;
-  keep.push_back(sets[0]);
-  for (int i = 1; i <= stop; ++i) {
-    split_set ns = sets[i];
+  keep.push_back(sets_[0]);
+  for (int i = 1; i <= stop_; ++i) {
+    split_set ns = sets_[i];
     if (ns.n_clusters < keep.back().n_clusters) {
       const int count = (int)keep.size();
-      fprintf(log, "Layer %i has %i clusters\n", count, ns.n_clusters);
-      fprintf(log, "  Coverage at layer %i: %f\n", count, coverage(not_covered_count(ns, n), n));
-      fprintf(log, "  Epsilon at layer %i: %f\n", count, layer_eps(eps_start, i, eps_inc));
+      say("Layer %i has %i clusters\n", count, ns.n_clusters);
+      say("  Coverage at layer %i: %f\n", count, coverage(not_covered_count(ns, n_), n_));
+      say("  Epsilon at layer %i: %f\n", count, layer_eps(eps_start_, i, eps_inc_));
       conns.push_back(generate_split_set_relation(keep.back(), ns));
       keep.push_back(ns);
     } else {
       free_split_set_and_associated_clusters(ns);
     }
   }
-  sets.clear();
-  fprintf(log, "Connections found: \n");
+  for (size_t i = (size_t)stop_ + 1; i < sets_.size(); ++i) free_split_set_and_associated_clusters(sets_[i]);
+  sets_.clear();
+  say("Connections found: \n");
   if (prefix) {
     for (size_t i = 0; i < keep.size(); ++i) {
       std::string name = std::string(prefix);
@@ -188,11 +228,11 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
     }
   }
   for (int i = (int)keep.size() - 1; i > 0; --i) {
-    fprintf(log, "Layer %i:\n", i);
+    say("Layer %i:\n", i);
     for (int j = 0; j < keep[i].n_clusters; ++j) {
-      fprintf(log, "  Cluster %i connected to: \n  ", j);
-      for (int k = 0; k < conns[i - 1][j].n_connections; ++k) fprintf(log, "%i ", conns[i - 1][j].connections[k]);
-      fprintf(log, "\n");
+      say("  Cluster %i connected to: \n  ", j);
+      for (int k = 0; k < conns[i - 1][j].n_connections; ++k) say("%i ", conns[i - 1][j].connections[k]);
+      say("\n");
     }
   }
   for (int i = (int)keep.size() - 1; i > 0; --i) {
@@ -200,6 +240,41 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
     free(conns[i - 1]);
   }
   *kept = std::move(keep);
+}
+
+std::string SweepMachine::take_log() {
+  std::string out;
+  out.swap(log_);
+  return out;
+}
+
+int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
+                   const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
+                   std::vector<split_set>* kept, std::string* err, int max_steps) {
+  SweepMachine m(n, eps_start, eps_inc, minpts, max_steps, prov.batch, dbscan_sw_warnings, fixed_point);
+  auto flush = [&]() {
+    const std::string t = m.take_log();
+    if (!t.empty()) fwrite(t.data(), 1, t.size(), log);
+  };
+  while (!m.done()) {
+    flush();
+    const std::vector<float>& eps = m.request();
+    std::vector<split_set> res(eps.size(), split_set{0, nullptr});
+    const int rc = prov.run(eps.data(), (int)eps.size(), res.data());
+    if (rc) {
+      for (auto& s : res) free_split_set_and_associated_clusters(s);
+      m.abort(rc, "dbscan failed");
+      break;
+    }
+    m.consume(res.data());
+  }
+  if (m.status()) {
+    flush();
+    *err = m.error();
+    return m.status();
+  }
+  m.finish(prefix, kept);
+  flush();
   return 0;
 }
 

@@ -7,6 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <memory>
 #include <climits>
 #include <cmath>
 #include <cstdlib>
@@ -147,6 +150,10 @@ struct swe_ctx {
   HostPinned<int> h_counts;
   long long bits_T = LLONG_MIN;
   int bits_set = -1;
+  // threshold launches: groups, their row prefix and thresholds
+  DevBuf<ThrGroup> d_groups;
+  DevBuf<long long> d_rowpre;
+  DevBuf<unsigned> d_thr;
   // batched sweeps: one bitmap slot per distinct threshold
   DevBuf<uint64_t> d_bbits;
   DevBuf<int> d_bcounts;
@@ -583,9 +590,9 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   CK(fast_set_smem_limit(ctx->smem));
   const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
   ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
-  size_t bm_smem = 0;
-  for (int k = 0; k < n_sets; ++k) bm_smem = std::max(bm_smem, bitmap_smem_bytes(set_n[k], ctx->dist_bytes));
-  if (bm_smem) CK(bitmap_set_smem_limit(bm_smem));
+  size_t th_smem = 0;
+  for (int k = 0; k < n_sets; ++k) th_smem = std::max(th_smem, threshold_stage_bytes(set_n[k], ctx->dist_bytes));
+  if (th_smem) CK(threshold_set_smem_limit(th_smem));
   CK(cudaStreamSynchronize(st));
   return SWE_OK;
 }
@@ -748,6 +755,65 @@ swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out) {
 
 }  // extern "C"
 
+// Groups of one set against thresholds T[0..count) (all >= 0), THR_MAX per
+// group; threshold j's bitmap starts at word *bits_words + j * n_s * wpr and its
+// counts at *count_ints + j * n_s.  Advances both offsets past the set.
+static void add_set_groups(const swe_ctx* ctx, int s, const long long* T, int count, std::vector<ThrGroup>* groups,
+                           std::vector<unsigned>* thr, long long* bits_words, long long* count_ints) {
+  const int first = ctx->set_first[s], ns = ctx->set_first[s + 1] - first;
+  const int wpr = (ns + 63) / 64;
+  for (int j0 = 0; j0 < count; j0 += THR_MAX) {
+    ThrGroup g;
+    g.dist_base = ctx->set_base[s];
+    g.bits_base = *bits_words + (long long)j0 * ns * wpr;
+    g.counts_base = *count_ints + (long long)j0 * ns;
+    g.pos_first = first;
+    g.n_s = ns;
+    g.wpr = wpr;
+    g.thr_first = (int)thr->size();
+    g.nthr = std::min(THR_MAX, count - j0);
+    for (int j = j0; j < j0 + g.nthr; ++j) thr->push_back((unsigned)std::min<long long>(T[j], 0xFFFFFFFFLL));
+    if (ns > 0) groups->push_back(g);
+  }
+  *bits_words += (long long)count * ns * wpr;
+  *count_ints += (long long)count * ns;
+}
+
+// One threshold launch over `groups`, bracketed by ev[2] / ev[3].
+static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& groups, const std::vector<unsigned>& thr,
+                                uint64_t* d_bits, int* d_counts) {
+  std::vector<long long> pre(groups.size() + 1, 0);
+  int maxn = 0;
+  for (size_t g = 0; g < groups.size(); ++g) {
+    pre[g + 1] = pre[g] + groups[g].n_s;
+    maxn = std::max(maxn, groups[g].n_s);
+  }
+  CK(cudaEventRecord(ctx->ev[2], ctx->st));
+  if (pre.back() > 0) {
+    CK(ctx->d_groups.alloc(groups.size()));
+    CK(ctx->d_rowpre.alloc(pre.size()));
+    CK(ctx->d_thr.alloc(std::max<size_t>(thr.size(), 1)));
+    CK(cpy(ctx, ctx->d_groups.p, groups.data(), sizeof(ThrGroup) * groups.size(), cudaMemcpyHostToDevice, ctx->st));
+    CK(cpy(ctx, ctx->d_rowpre.p, pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice, ctx->st));
+    CK(cpy(ctx, ctx->d_thr.p, thr.data(), sizeof(unsigned) * thr.size(), cudaMemcpyHostToDevice, ctx->st));
+    ThrParams p{};
+    p.D16 = ctx->d_D16.p;
+    p.D32 = ctx->d_D32.p;
+    p.pos = ctx->d_pos.p;
+    p.groups = ctx->d_groups.p;
+    p.ngroups = (int)groups.size();
+    p.row_pre = ctx->d_rowpre.p;
+    p.thr = ctx->d_thr.p;
+    p.bits = d_bits;
+    p.counts = d_counts;
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    ctx->stats.kernel_launches += 1;
+    CK(launch_threshold(p, pre.back(), threshold_stage_bytes(maxn, ctx->dist_bytes), ctx->st));
+  }
+  CK(cudaEventRecord(ctx->ev[3], ctx->st));
+  return SWE_OK;
+}
+
 // Neighbour bitmap of set s for threshold T on the host (pinned), cached per
 // (set, T).  Rows and columns are in the set's original index order.
 static swe_status ensure_bitmap(swe_ctx* ctx, int s, long long T) {
@@ -766,11 +832,11 @@ static swe_status ensure_bitmap(swe_ctx* ctx, int s, long long T) {
   }
   CK(ctx->d_bits.alloc(words));
   CK(ctx->d_counts.alloc(n));
-  CK(cudaEventRecord(ctx->ev[2], ctx->st));
-  ctx->stats.kernel_launches += 1;
-  CK(launch_bitmap_set(set_D16(ctx, s), set_D32(ctx, s), ctx->d_pos.p + first, n, T, ctx->d_bits.p, ctx->wpr,
-                       ctx->d_counts.p, ctx->st));
-  CK(cudaEventRecord(ctx->ev[3], ctx->st));
+  std::vector<ThrGroup> groups;
+  std::vector<unsigned> thr;
+  long long bw = 0, ci = 0;
+  add_set_groups(ctx, s, &T, 1, &groups, &thr, &bw, &ci);
+  if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bits.p, ctx->d_counts.p)) return st;
   CK(cpy(ctx, ctx->h_bits.p, ctx->d_bits.p, words * 8, cudaMemcpyDeviceToHost, ctx->st));
   CK(cpy(ctx, ctx->h_counts.p, ctx->d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
@@ -904,6 +970,217 @@ swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts
   if (!ctx) return SWE_ERR_INVALID;
   if (swe_status s = need_one_set(ctx)) return s;
   return swe_adaptive_set(ctx, 0, eps_start, eps_inc, minpts, prefix, log, out_sets, out_n_sets);
+}
+
+}  // extern "C"
+
+namespace {
+
+// f(i) for i in [0, n) on up to hardware_concurrency threads, dynamic order.
+template <class F>
+void parallel_for(int n, F&& f) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int T = std::min(hw, n);
+  if (T <= 1) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  th.reserve(T);
+  for (int t = 0; t < T; ++t)
+    th.emplace_back([&]() {
+      for (;;) {
+        const int i = next.fetch_add(1);
+        if (i >= n) break;
+        f(i);
+      }
+    });
+  for (auto& t : th) t.join();
+}
+
+// One distinct threshold of one set in a round.
+struct SweepJob {
+  int set;
+  long long T;
+  long long bits_off;   // words into the round's bitmap buffer (-1: no launch, empty neighbourhoods)
+  long long count_off;  // ints into the round's count buffer
+  split_set res;
+  int rc;
+};
+
+}  // namespace
+
+extern "C" {
+
+swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, int max_steps,
+                             const char* prefix, swe_sweep_result* results) {
+  if (!ctx || !results || max_steps < 0) return SWE_ERR_INVALID;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  const auto t0 = std::chrono::steady_clock::now();
+  const int S = ctx->n_sets;
+  for (int k = 0; k < S; ++k) results[k] = swe_sweep_result{};
+  const long long fixed = 4LL * ctx->max_len;  // every distance is <= 4*max_len
+  const int mp = minpts == -1 ? 5 : minpts;    // dbscan.c:985-989
+  const int batch = max_steps > 0 ? std::min(8, max_steps) : 8;
+  std::vector<std::unique_ptr<SweepMachine>> m(S);
+  std::vector<std::string> logs(S);
+  for (int k = 0; k < S; ++k)
+    m[k].reset(new SweepMachine(ctx->set_first[k + 1] - ctx->set_first[k], eps_start, eps_inc, minpts, max_steps,
+                                batch, true, fixed));
+  auto finish_set = [&](int k) {
+    std::vector<split_set> kept;
+    std::string pre;
+    if (prefix) pre = std::string(prefix) + std::to_string(k) + "_";
+    m[k]->finish(prefix ? pre.c_str() : nullptr, &kept);
+    logs[k] += m[k]->take_log();
+    swe_sweep_result& r = results[k];
+    r.status = m[k]->status();
+    r.truncated = m[k]->truncated() ? 1 : 0;
+    r.steps = m[k]->steps();
+    r.n_layers = (int)kept.size();
+    r.layers = (split_set*)malloc(sizeof(split_set) * std::max<size_t>(kept.size(), 1));
+    r.log = (char*)malloc(logs[k].size() + 1);
+    if (r.layers) {
+      for (size_t i = 0; i < kept.size(); ++i) r.layers[i] = kept[i];
+    } else {
+      for (auto& x : kept) free_split_set_and_associated_clusters(x);
+      r.n_layers = 0;
+      r.status = SWE_ERR_OOM;
+    }
+    if (r.log) memcpy(r.log, logs[k].c_str(), logs[k].size() + 1);
+    r.done_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  };
+  std::vector<int> active;
+  for (int k = 0; k < S; ++k) {
+    logs[k] += m[k]->take_log();
+    if (m[k]->done()) finish_set(k);
+    else active.push_back(k);
+  }
+  const long long budget_words = (1LL << 30) / 8;  // bitmaps of one launch: 1 GiB
+  double kernel_ms = 0;
+  int launches = 0;
+  while (!active.empty()) {
+    size_t a = 0;
+    while (a < active.size()) {
+      // sets [a, b) of the active list share one launch
+      std::vector<ThrGroup> groups;
+      std::vector<unsigned> thr;
+      std::vector<SweepJob> jobs;
+      std::vector<size_t> job_first;
+      long long bw = 0, ci = 0;
+      size_t b = a;
+      for (; b < active.size(); ++b) {
+        const int k = active[b];
+        const int ns = ctx->set_first[k + 1] - ctx->set_first[k], wpr = (ns + 63) / 64;
+        std::vector<long long> launchT;
+        std::vector<long long> uniq;
+        for (float e : m[k]->request()) {
+          const long long T = eps_threshold(e == -1 ? 0.015f : e);  // dbscan.c:980-984
+          if (std::find(uniq.begin(), uniq.end(), T) == uniq.end()) uniq.push_back(T);
+        }
+        for (long long T : uniq)
+          if (T >= 0 && ns > 0) launchT.push_back(T);
+        const long long words = (long long)launchT.size() * ns * wpr;
+        if (b > a && bw + words > budget_words) break;
+        job_first.push_back(jobs.size());
+        long long off = bw, coff = ci;
+        for (long long T : uniq) {
+          SweepJob j{k, T, -1, -1, split_set{0, nullptr}, 0};
+          if (T >= 0 && ns > 0) {
+            j.bits_off = off;
+            j.count_off = coff;
+            off += (long long)ns * wpr;
+            coff += ns;
+          }
+          jobs.push_back(j);
+        }
+        add_set_groups(ctx, k, launchT.data(), (int)launchT.size(), &groups, &thr, &bw, &ci);
+      }
+      job_first.push_back(jobs.size());
+      if (bw > 0) {
+        CK(ctx->d_bbits.alloc((size_t)bw));
+        CK(ctx->d_bcounts.alloc((size_t)ci));
+        CK(ctx->h_bbits.alloc((size_t)bw));
+        CK(ctx->h_bcounts.alloc((size_t)ci));
+        if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bbits.p, ctx->d_bcounts.p)) return st;
+        CK(cpy(ctx, ctx->h_bbits.p, ctx->d_bbits.p, sizeof(uint64_t) * bw, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cpy(ctx, ctx->h_bcounts.p, ctx->d_bcounts.p, sizeof(int) * ci, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        kernel_ms += ms;
+        ++launches;
+      }
+      // order-faithful replays, one per (set, distinct threshold), largest sets first
+      std::vector<int> order(jobs.size());
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return ctx->set_first[jobs[x].set + 1] - ctx->set_first[jobs[x].set] >
+               ctx->set_first[jobs[y].set + 1] - ctx->set_first[jobs[y].set];
+      });
+      parallel_for((int)jobs.size(), [&](int q) {
+        SweepJob& j = jobs[order[q]];
+        const int ns = ctx->set_first[j.set + 1] - ctx->set_first[j.set], wpr = (ns + 63) / 64;
+        if (j.bits_off >= 0) {
+          j.rc = dbscan_replay_bitmap(ns, ctx->h_bbits.p + j.bits_off, wpr, ctx->h_bcounts.p + j.count_off, mp,
+                                      &j.res);
+        } else {  // no neighbour at all, not even the point itself
+          std::vector<uint64_t> zb((size_t)ns * wpr + 1, 0);
+          std::vector<int> zc((size_t)ns + 1, 0);
+          j.rc = dbscan_replay_bitmap(ns, zb.data(), wpr, zc.data(), mp, &j.res);
+        }
+      });
+      // advance every set of the launch
+      parallel_for((int)(b - a), [&](int x) {
+        const int k = active[a + x];
+        const std::vector<float>& req = m[k]->request();
+        std::vector<split_set> out(req.size(), split_set{0, nullptr});
+        std::vector<bool> used(job_first[x + 1] - job_first[x], false);
+        int rc = 0;
+        for (size_t q = job_first[x]; q < job_first[x + 1]; ++q) rc = rc ? rc : jobs[q].rc;
+        if (rc) {
+          for (size_t q = job_first[x]; q < job_first[x + 1]; ++q) free_split_set_and_associated_clusters(jobs[q].res);
+          m[k]->abort(rc, "dbscan replay failed");
+        } else {
+          for (size_t e = 0; e < req.size(); ++e) {
+            const long long T = eps_threshold(req[e] == -1 ? 0.015f : req[e]);
+            size_t q = job_first[x];
+            while (jobs[q].T != T) ++q;
+            const size_t u = q - job_first[x];
+            out[e] = used[u] ? copy_split_set(jobs[q].res) : jobs[q].res;
+            used[u] = true;
+          }
+          for (size_t q = job_first[x]; q < job_first[x + 1]; ++q)
+            if (!used[q - job_first[x]]) free_split_set_and_associated_clusters(jobs[q].res);
+          m[k]->consume(out.data());
+        }
+        logs[k] += m[k]->take_log();
+        if (m[k]->done()) finish_set(k);
+      });
+      a = b;
+    }
+    std::vector<int> still;
+    for (int k : active)
+      if (!m[k]->done()) still.push_back(k);
+    active.swap(still);
+  }
+  ctx->stats.ms_last_neighbors = kernel_ms;
+  ctx->stats.last_neighbor_launches = launches;
+  return SWE_OK;
+}
+
+void swe_free_sweep_results(swe_sweep_result* results, int n) {
+  if (!results) return;
+  for (int k = 0; k < n; ++k) {
+    for (int i = 0; i < results[k].n_layers; ++i) free_split_set_and_associated_clusters(results[k].layers[i]);
+    free(results[k].layers);
+    free(results[k].log);
+    results[k].layers = nullptr;
+    results[k].log = nullptr;
+    results[k].n_layers = 0;
+  }
 }
 
 swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsigned* out) {
@@ -1062,39 +1339,43 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
   const int U = (int)uniq.size();
   CK(ctx->h_bbits.alloc(std::max<size_t>(words * U, 1)));
   CK(ctx->h_bcounts.alloc(std::max<size_t>((size_t)n * U, 1)));
-  bool any_gpu = false;
-  for (int u = 0; u < U; ++u) any_gpu |= (uniq[u] >= 0 && n > 0);
-  if (any_gpu) {
-    CK(ctx->d_bbits.alloc(words * U));
-    CK(ctx->d_bcounts.alloc((size_t)n * U));
-  }
-  // the threshold kernels back to back (timed), then the copies
-  int launched = 0;
-  CK(cudaEventRecord(ctx->ev[2], ctx->st));
+  // thresholds >= 0 first (one launch reads the matrix once for all of them)
+  std::vector<int> launch_idx, none_idx;
+  std::vector<long long> launchT;
   for (int u = 0; u < U; ++u) {
-    if (uniq[u] < 0 || n == 0) continue;
-    ctx->stats.kernel_launches += 1;
-    ++launched;
-    CK(launch_bitmap_set(set_D16(ctx, set), set_D32(ctx, set), ctx->d_pos.p + first, n, uniq[u],
-                         ctx->d_bbits.p + words * u, wpr, ctx->d_bcounts.p + (size_t)n * u, ctx->st));
-  }
-  CK(cudaEventRecord(ctx->ev[3], ctx->st));
-  for (int u = 0; u < U; ++u) {
-    uint64_t* hb = ctx->h_bbits.p + words * u;
-    int* hc = ctx->h_bcounts.p + (size_t)n * u;
-    if (uniq[u] < 0 || n == 0) {  // no neighbour at all, not even the point itself
-      if (words) memset(hb, 0, words * 8);
-      if (n) memset(hc, 0, sizeof(int) * n);
-      continue;
+    if (uniq[u] >= 0 && n > 0) {
+      launch_idx.push_back(u);
+      launchT.push_back(uniq[u]);
+    } else {
+      none_idx.push_back(u);
     }
-    CK(cpy(ctx, hb, ctx->d_bbits.p + words * u, words * 8, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cpy(ctx, hc, ctx->d_bcounts.p + (size_t)n * u, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
   }
-  CK(cudaStreamSynchronize(ctx->st));
+  for (int u : none_idx) {  // no neighbour at all, not even the point itself
+    if (words) memset(ctx->h_bbits.p + words * u, 0, words * 8);
+    if (n) memset(ctx->h_bcounts.p + (size_t)n * u, 0, sizeof(int) * n);
+  }
+  const int UL = (int)launch_idx.size();
   float ms = 0;
-  CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+  if (UL > 0) {
+    CK(ctx->d_bbits.alloc(words * UL));
+    CK(ctx->d_bcounts.alloc((size_t)n * UL));
+    std::vector<ThrGroup> groups;
+    std::vector<unsigned> thr;
+    long long bw = 0, ci = 0;
+    add_set_groups(ctx, set, launchT.data(), UL, &groups, &thr, &bw, &ci);
+    if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bbits.p, ctx->d_bcounts.p)) return st;
+    for (int j = 0; j < UL; ++j) {
+      const int u = launch_idx[j];
+      CK(cpy(ctx, ctx->h_bbits.p + words * u, ctx->d_bbits.p + words * j, words * 8, cudaMemcpyDeviceToHost,
+             ctx->st));
+      CK(cpy(ctx, ctx->h_bcounts.p + (size_t)n * u, ctx->d_bcounts.p + (size_t)n * j, sizeof(int) * n,
+             cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+  }
   ctx->stats.ms_last_neighbors = ms;
-  ctx->stats.last_neighbor_launches = launched;
+  ctx->stats.last_neighbor_launches = UL > 0 ? 1 : 0;
   // one order-faithful replay per distinct threshold, in parallel
   std::vector<split_set> res(U, split_set{0, nullptr});
   std::vector<int> rc(U, 0);

@@ -33,17 +33,69 @@ struct DbscanProvider {
   int batch = 1;
 };
 
-// Adaptive sweep of dbscan.c:1117-1380 over a DBSCAN provider.  With
-// `dbscan_sw_warnings` the warnings dbscan_SW prints for eps == -1 or
-// minpts == -1 (dbscan.c:980-989) are printed for every DBSCAN result the
+// Adaptive sweep of dbscan.c:1117-1380 as a state machine: request() holds
+// the eps values to evaluate next, consume() takes their DBSCAN results
+// (ownership passes in), and once done() finish() selects the layers, writes
+// the split-set files and the rest of the log.  Log text accumulates in the
+// machine (take_log()).  Driving many machines at once lets one threshold
+// launch serve the pending requests of many independent sets.
+//
+// With `dbscan_sw_warnings` the warnings dbscan_SW prints for eps == -1 or
+// minpts == -1 (dbscan.c:980-989) are logged for every DBSCAN result the
 // sweep consumes, where the reference's dbscanner calls would print them.
 // `fixed_point` (when >= 0) is a threshold at or above which every eps gives
 // the same result, used to stop sweeps that could never reach one cluster
-// (the reference loops forever there).  Kept layers are returned in `kept`
-// (ownership passes to the caller).
+// (the reference loops forever there).  max_steps > 0 bounds the DBSCAN runs
+// of the sweep phase (after the starting eps); a sweep that reaches the bound
+// before a one-cluster result keeps the layers found so far (truncated()).
+// max_steps == 0 is the reference's unbounded sweep.
+class SweepMachine {
+ public:
+  SweepMachine(int n, float eps_start, float eps_inc, int minpts, int max_steps, int batch, bool dbscan_sw_warnings,
+               long long fixed_point);
+  ~SweepMachine();
+  SweepMachine(const SweepMachine&) = delete;
+  SweepMachine& operator=(const SweepMachine&) = delete;
+  bool done() const { return phase_ == DONE; }
+  const std::vector<float>& request() const { return req_; }
+  void consume(split_set* res);
+  void abort(int status, const char* why);
+  void finish(const char* prefix, std::vector<split_set>* kept);
+  std::string take_log();
+  int status() const { return status_; }
+  const std::string& error() const { return err_; }
+  bool truncated() const { return truncated_; }
+  int steps() const { return steps_; }
+
+ private:
+  enum Phase { FIRST, HALVING, SWEEP, DONE };
+  void say(const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+  void warn(float eps);
+  void fail(int status, const char* why);
+  void next_sweep_batch();
+  int n_;
+  float eps_start_, eps_inc_;
+  int minpts_, max_steps_, batch_;
+  bool warnings_;
+  long long fixed_;
+  Phase phase_ = FIRST;
+  std::vector<float> req_;
+  std::vector<split_set> sets_;
+  float eps_now_ = 0;
+  int counter_ = 0, steps_ = 0, stop_ = -1, status_ = 0;
+  bool terminal_ = false, truncated_ = false;
+  std::string log_, err_;
+};
+
+// One sweep driven to the end over a DBSCAN provider, log lines written to
+// `log` as they are produced.  Kept layers are returned in `kept` (ownership
+// passes to the caller).
 int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char* prefix, FILE* log,
                    const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
-                   std::vector<split_set>* kept, std::string* err);
+                   std::vector<split_set>* kept, std::string* err, int max_steps = 0);
+
+int not_covered_count(const split_set& s, int n);
+float coverage(int not_covered, int n);
 
 // The engine's batched DBSCAN over its scored matrix: the GPU builds one
 // neighbour bitmap per distinct threshold and host threads replay them in

@@ -12,8 +12,10 @@
 //                          persistent over a cost-ordered tile list;
 //   generic_kernel         32-bit warp wavefront, one pair per warp, any
 //                          length (512-column chunks) and any symbol;
-//   bitmap_kernel          eps threshold of the distance matrix into a
-//                          neighbour bitmap plus per-row counts;
+//   threshold_kernel       eps thresholds of the distance matrices of many
+//                          sets at once into neighbour bitmaps plus per-row
+//                          counts (each row read once for all thresholds);
+//   unpermute_kernel       a set's matrix back in original index order;
 //   csr_fill_kernel        bitmap -> ascending CSR column lists.
 #include "sw_device.cuh"
 #include "sw_kernels.cuh"
@@ -422,74 +424,96 @@ cudaError_t launch_diag(const DistLayout& L, int n, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// Neighbour bitmap of one set.  One CTA per row i (original order): the row
-// pos[i] of the set's sorted matrix is staged in shared memory when it fits,
-// then each warp builds 64-bit words of the row's bits in original column
-// order by gathering through pos[].
-// ---------------------------------------------------------------------------
-constexpr int BITMAP_STAGE_MAX = 200 * 1024;
+// Rows of up to this many bytes are staged in shared memory by the threshold pass.
+constexpr int THRESHOLD_STAGE_MAX = 200 * 1024;
 
-size_t bitmap_smem_bytes(int n_s, int dist_bytes) {
-  const size_t b = (size_t)n_s * (size_t)dist_bytes;
-  return b <= (size_t)BITMAP_STAGE_MAX ? ((b + 15) & ~(size_t)15) : 0;
+// ---------------------------------------------------------------------------
+// Threshold pass over groups (set x up to 32 thresholds).  One CTA per row
+// (global row list over all groups): the row is staged in shared memory once,
+// then each warp gathers two columns per lane through pos[] and produces one
+// 64-bit word per threshold with two ballots; lane u keeps threshold u's word
+// and count, so a row's distances are read once for all its thresholds.
+// ---------------------------------------------------------------------------
+size_t threshold_stage_bytes(int max_n_s, int dist_bytes) {
+  const size_t b = (size_t)max_n_s * (size_t)dist_bytes;
+  return b <= (size_t)THRESHOLD_STAGE_MAX ? ((b + 15) & ~(size_t)15) : 0;
 }
 
 template <typename DT, bool STAGE>
-__global__ void __launch_bounds__(256) bitmap_kernel(const DT* __restrict__ Dset, const int* __restrict__ pos,
-                                                     int ns, long long T, uint64_t* __restrict__ bits, int wpr,
-                                                     int* __restrict__ counts) {
-  extern __shared__ __align__(16) uint8_t bm_smem[];
-  DT* srow = reinterpret_cast<DT*>(bm_smem);
-  __shared__ int s_cnt[8];
+__global__ void __launch_bounds__(256) threshold_kernel(ThrParams p, const DT* __restrict__ D, long long total) {
+  extern __shared__ __align__(16) uint8_t th_smem[];
+  DT* srow = reinterpret_cast<DT*>(th_smem);
+  __shared__ unsigned s_thr[THR_MAX];
+  __shared__ int s_cnt[8][THR_MAX];
+  __shared__ int s_group;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int i = blockIdx.x; i < ns; i += gridDim.x) {
-    const DT* row = Dset + (long long)pos[i] * ns;
-    if (STAGE) {
-      for (int k = threadIdx.x; k < ns; k += blockDim.x) srow[k] = row[k];
-      __syncthreads();
+  for (long long r = blockIdx.x; r < total; r += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = p.ngroups - 1;  // last group with row_pre[g] <= r
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.row_pre[mid] <= r) lo = mid;
+        else hi = mid - 1;
+      }
+      s_group = lo;
     }
+    __syncthreads();
+    const ThrGroup G = p.groups[s_group];
+    const int i = (int)(r - p.row_pre[s_group]);
+    const int ns = G.n_s, nthr = G.nthr;
+    const int* pos = p.pos + G.pos_first;
+    const DT* row = D + G.dist_base + (long long)pos[i] * ns;
+    if (threadIdx.x < nthr) s_thr[threadIdx.x] = p.thr[G.thr_first + threadIdx.x];
+    if (STAGE)
+      for (int k = threadIdx.x; k < ns; k += blockDim.x) srow[k] = row[k];
+    __syncthreads();
     const DT* src = STAGE ? srow : row;
     int cnt = 0;
-    for (int w = warp; w < wpr; w += nwarps) {
+    for (int w = warp; w < G.wpr; w += nwarps) {
       const int c0 = w * 64 + lane, c1 = c0 + 32;
-      const bool v0 = c0 < ns && (long long)src[pos[c0]] <= T;
-      const bool v1 = c1 < ns && (long long)src[pos[c1]] <= T;
-      const uint32_t lo = __ballot_sync(0xFFFFFFFFu, v0), hi = __ballot_sync(0xFFFFFFFFu, v1);
-      if (lane == 0) bits[(size_t)i * wpr + w] = (uint64_t)lo | ((uint64_t)hi << 32);
-      cnt += __popc(lo) + __popc(hi);
+      const unsigned d0 = c0 < ns ? (unsigned)src[pos[c0]] : 0xFFFFFFFFu;
+      const unsigned d1 = c1 < ns ? (unsigned)src[pos[c1]] : 0xFFFFFFFFu;
+      uint64_t mine = 0;
+      for (int u = 0; u < nthr; ++u) {
+        const unsigned t = s_thr[u];
+        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, c0 < ns && d0 <= t);
+        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, c1 < ns && d1 <= t);
+        if (lane == u) mine = (uint64_t)lo | ((uint64_t)hi << 32);
+      }
+      if (lane < nthr) {
+        p.bits[G.bits_base + ((long long)lane * ns + i) * G.wpr + w] = mine;
+        cnt += __popcll(mine);
+      }
     }
-    if (lane == 0) s_cnt[warp] = cnt;
+    if (lane < nthr) s_cnt[warp][lane] = cnt;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < nthr) {
       int c = 0;
-      for (int k = 0; k < nwarps; ++k) c += s_cnt[k];
-      counts[i] = c;
+      for (int k = 0; k < nwarps; ++k) c += s_cnt[k][threadIdx.x];
+      p.counts[G.counts_base + (long long)threadIdx.x * ns + i] = c;
     }
-    __syncthreads();  // srow and s_cnt are reused by the next row
+    __syncthreads();  // srow, s_thr, s_cnt and s_group are reused by the next row
   }
 }
 
-cudaError_t bitmap_set_smem_limit(size_t bytes) {
-  cudaError_t e = cudaFuncSetAttribute(bitmap_kernel<uint16_t, true>,
+cudaError_t threshold_set_smem_limit(size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(threshold_kernel<uint16_t, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(bitmap_kernel<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(threshold_kernel<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes);
   return e;
 }
 
-cudaError_t launch_bitmap_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s,
-                              long long T, uint64_t* bits, int words_per_row, int* counts, cudaStream_t st) {
-  if (n_s <= 0) return cudaSuccess;
-  const int grid = min(n_s, 148 * 8);
-  const size_t smem = bitmap_smem_bytes(n_s, D16set ? 2 : 4);
-  if (D16set) {
-    if (smem) bitmap_kernel<uint16_t, true><<<grid, 256, smem, st>>>(D16set, pos, n_s, T, bits, words_per_row, counts);
-    else bitmap_kernel<uint16_t, false><<<grid, 256, 0, st>>>(D16set, pos, n_s, T, bits, words_per_row, counts);
+cudaError_t launch_threshold(const ThrParams& p, long long total_rows, size_t stage_bytes, cudaStream_t st) {
+  if (total_rows <= 0 || p.ngroups <= 0) return cudaSuccess;
+  const int grid = total_rows < 148 * 8 ? (int)total_rows : 148 * 8;
+  if (p.D16) {
+    if (stage_bytes) threshold_kernel<uint16_t, true><<<grid, 256, stage_bytes, st>>>(p, p.D16, total_rows);
+    else threshold_kernel<uint16_t, false><<<grid, 256, 0, st>>>(p, p.D16, total_rows);
   } else {
-    if (smem) bitmap_kernel<uint32_t, true><<<grid, 256, smem, st>>>(D32set, pos, n_s, T, bits, words_per_row, counts);
-    else bitmap_kernel<uint32_t, false><<<grid, 256, 0, st>>>(D32set, pos, n_s, T, bits, words_per_row, counts);
+    if (stage_bytes) threshold_kernel<uint32_t, true><<<grid, 256, stage_bytes, st>>>(p, p.D32, total_rows);
+    else threshold_kernel<uint32_t, false><<<grid, 256, 0, st>>>(p, p.D32, total_rows);
   }
   return cudaGetLastError();
 }

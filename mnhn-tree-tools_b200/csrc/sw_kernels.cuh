@@ -109,18 +109,41 @@ int fast_occupancy(int block, size_t smem);
 cudaError_t launch_generic(const GenParams& p, int grid, cudaStream_t st);
 // Zero self-distances of every sequence.
 cudaError_t launch_diag(const DistLayout& L, int n, cudaStream_t st);
-// Neighbour bitmap of one set for threshold T, rows and columns in the set's
-// original index order: bit k of row i is set iff D_s[pos i][pos k] <= T;
-// counts[i] is row i's popcount.  D16set / D32set point at the set's matrix
-// (one is null) and pos at the set's slice of the position table.
-cudaError_t launch_bitmap_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s,
-                              long long T, uint64_t* bits, int words_per_row, int* counts, cudaStream_t st);
-size_t bitmap_smem_bytes(int n_s, int dist_bytes);
-cudaError_t bitmap_set_smem_limit(size_t bytes);
 // Rows [r0, r1) of one set's matrix in original index order, widened to 32
 // bits (out holds (r1 - r0) x n_s entries).
 cudaError_t launch_unpermute_set(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s, int r0,
                                  int r1, uint32_t* out, cudaStream_t st);
+// Threshold pass over several sets and several thresholds at once.  A group
+// is one set against up to THR_MAX thresholds; each row of the set's matrix is
+// read once and yields one bitmap row per threshold.  Bits of group g,
+// threshold u, row i (original order inside the set), word w are at
+// bits[bits_base + (u * n_s + i) * wpr + w]; its popcount at
+// counts[counts_base + u * n_s + i].  A threshold t keeps d <= t.
+constexpr int THR_MAX = 32;
+struct ThrGroup {
+  long long dist_base;    // offset of the set's matrix in D (elements)
+  long long bits_base;    // words
+  long long counts_base;  // ints
+  int pos_first;          // the set's slice of the position table
+  int n_s, wpr;
+  int thr_first, nthr;    // thresholds thr[thr_first .. thr_first + nthr), nthr <= THR_MAX
+};
+struct ThrParams {
+  const uint16_t* D16;      // one of D16 / D32 is non-null
+  const uint32_t* D32;
+  const int* pos;
+  const ThrGroup* groups;
+  int ngroups;
+  const long long* row_pre;  // [ngroups + 1] prefix sums of the groups' n_s
+  const unsigned* thr;
+  uint64_t* bits;
+  int* counts;
+};
+// stage_bytes: the largest set row in bytes when every row is staged in
+// shared memory, 0 to read rows from global memory.
+cudaError_t launch_threshold(const ThrParams& p, long long total_rows, size_t stage_bytes, cudaStream_t st);
+size_t threshold_stage_bytes(int max_n_s, int dist_bytes);
+cudaError_t threshold_set_smem_limit(size_t bytes);
 // CSR from a bitmap: ascending column indices per row at row_ptr[i].
 cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, const long long* row_ptr,
                             int* cols, cudaStream_t st);

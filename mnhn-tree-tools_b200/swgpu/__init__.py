@@ -73,6 +73,11 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SweepResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("truncated", C.c_int), ("steps", C.c_int), ("n_layers", C.c_int),
+                ("layers", C.POINTER(SplitSet)), ("log", C.c_void_p), ("done_ms", C.c_double)]
+
+
 DBSCANNER = C.CFUNCTYPE(SplitSet, Dataset, C.c_float, C.c_int)
 
 # Every symbol the public headers declare (checked by the CPU test suite).
@@ -83,7 +88,7 @@ EXPORTS = [
     "swe_score_one_to_many", "swe_score_pairs", "swe_get_stats", "swe_free", "swe_dbscan_bitmap",
     "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop", "swe_score_pairs_noalloc",
     "swe_upload_sets", "swe_set_count", "swe_copy_set_distances", "swe_neighbors_set", "swe_dbscan_set",
-    "swe_adaptive_set",
+    "swe_adaptive_set", "swe_adaptive_sets", "swe_free_sweep_results",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -135,6 +140,10 @@ def lib():
         L.swe_adaptive_set.restype = C.c_int
         L.swe_adaptive_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_int, C.c_char_p,
                                        C.c_void_p, C.POINTER(C.POINTER(SplitSet)), C.POINTER(C.c_int)]
+        L.swe_adaptive_sets.restype = C.c_int
+        L.swe_adaptive_sets.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_int, C.c_char_p,
+                                        C.POINTER(SweepResult)]
+        L.swe_free_sweep_results.argtypes = [C.POINTER(SweepResult), C.c_int]
         L.swe_score_one_to_many.restype = C.c_int
         L.swe_score_one_to_many.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p]
         L.swe_score_pairs.restype = C.c_int
@@ -312,6 +321,24 @@ class Engine:
             lib().free_split_set_and_associated_clusters(sets[k])
         lib().swe_free(sets)
         return text, kept
+
+    def adaptive_sets(self, eps_start: float, eps_inc: float, minpts: int, max_steps: int = 0,
+                      prefix: str | None = None):
+        """Sweeps of every uploaded set at once; one dict per set with its
+        status, truncated flag, steps, log text, kept layers and done_ms."""
+        S = self.set_count()
+        res = (SweepResult * max(S, 1))()
+        _check(lib().swe_adaptive_sets(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts, max_steps,
+                                       prefix.encode() if prefix else None, res), self.ctx)
+        out = []
+        for k in range(S):
+            r = res[k]
+            out.append({"status": r.status, "truncated": bool(r.truncated), "steps": r.steps,
+                        "log": C.string_at(r.log).decode("latin-1") if r.log else "",
+                        "layers": [split_set_to_lists(r.layers[i]) for i in range(r.n_layers)],
+                        "done_ms": r.done_ms})
+        lib().swe_free_sweep_results(res, S)
+        return out
 
     def one_to_many(self, q: bytes, qlen: int | None = None) -> np.ndarray:
         qlen = len(q) if qlen is None else qlen

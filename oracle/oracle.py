@@ -324,13 +324,18 @@ def cluster_fasta_text(members, seqs) -> str:
     return "".join(out)
 
 
-def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_steps: int = 100000):
+def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_steps: int = 100000,
+             truncate: bool = False):
     """adaptive_dbscan, dbscan.c:1117-1380, single thread, over a distance matrix.
 
     Returns (stdout text, kept split sets).  Float semantics follow the
     reference: eps_{k+1} = eps_k + inc in float (dbscan.c:1079-1080, 1267),
     halving eps_start while the first result has one cluster (dbscan.c:1211-1231),
     and the logged eps is eps_start + (i+1)*inc (dbscan.c:1323-1324).
+
+    The reference's sweep is unbounded.  With truncate=True a sweep that has
+    not reached one cluster after max_steps DBSCAN runs keeps the layers found
+    so far (the engine's bounded sweep for many sets); otherwise it raises.
     """
     n = D.shape[0]
     out = []
@@ -371,7 +376,9 @@ def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_s
             stop = len(sets) - 1
             break
     if stop is None:
-        raise RuntimeError("sweep did not reach one cluster")
+        if not truncate:
+            raise RuntimeError("sweep did not reach one cluster")
+        stop = len(sets) - 1
     kept = [first]
     conns = []
     for i in range(1, stop + 1):

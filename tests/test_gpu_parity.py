@@ -207,6 +207,62 @@ def test_adaptive_per_set_matches_single_set_runs(tmp_path):
     e1.close()
 
 
+def _sweep_sets():
+    sets, _ = W.config5(seed=15, n_sets=10, lo=30, hi=300)
+    pool, _ = W.config1()
+    rng = np.random.default_rng(8)
+    sets.append(_mixed_set(rng)[:60])          # 32-bit-path sequences inside a set
+    sets.append([pool[7]] * 12)                 # one cluster at every eps: the start search fails
+    sets.append(pool[:3])                       # fewer points than minpts: never one cluster
+    sets.append([pool[0]])
+    return sets
+
+
+@pytest.mark.parametrize("eps_start,eps_inc,minpts,max_steps", [(150.0, 50.0, 5, 0), (100.0, 60.0, 5, 12),
+                                                                 (150.0, 50.0, 3, 2), (20.0, 35.0, 4, 5)])
+def test_adaptive_sets_match_oracle(tmp_path, eps_start, eps_inc, minpts, max_steps):
+    """All sets' sweeps advanced together (one threshold launch per round):
+    each set's log text, kept layers and split-set files equal the oracle's
+    sweep of that set alone; max_steps bounds the sweep (layers found so far
+    are kept)."""
+    sets = _sweep_sets()
+    e = swgpu.Engine()
+    e.upload_sets(sets)
+    e.score_all_pairs()
+    res = e.adaptive_sets(eps_start, eps_inc, minpts, max_steps=max_steps, prefix=str(tmp_path / "L"))
+    st = e.stats()
+    assert st["last_neighbor_launches"] >= 1
+    singles = {}
+    if max_steps == 0:  # the single-set call on the same upload
+        for k in range(len(sets)):
+            try:
+                singles[k] = e.adaptive(eps_start, eps_inc, minpts, set=k)
+            except swgpu.SwgpuError as err:
+                singles[k] = err.status
+    e.close()
+    for k, st in enumerate(sets):
+        r = res[k]
+        D = O.all_pairs(st)
+        if len(set(st)) == 1 and len(st) >= minpts:
+            assert r["status"] == 9 and r["layers"] == [], k  # SWE_ERR_SWEEP
+            assert r["log"].endswith("Error did not find a sufficient starting position in 20 tries \n")
+            continue
+        if len(st) < minpts and max_steps == 0:
+            assert r["status"] == 9, k
+            continue
+        text, kept = O.adaptive(D, eps_start, eps_inc, minpts, max_steps=max_steps or 100000,
+                                truncate=max_steps > 0)
+        assert r["status"] == 0, (k, r["log"][-300:])
+        assert r["log"] == text, k
+        assert r["layers"] == kept, k
+        for i, layer in enumerate(kept):
+            assert (tmp_path / f"L{k}_{i:04d}").read_bytes() == O.split_set_bytes(layer), (k, i)
+        if max_steps == 0:
+            assert singles[k] == (text, kept), k
+        else:
+            assert r["steps"] <= max_steps
+
+
 # ---------------------------------------------------------------------------
 # neighbourhoods, DBSCAN, adaptive sweep
 # ---------------------------------------------------------------------------

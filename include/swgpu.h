@@ -48,6 +48,10 @@ typedef struct {
   int inject_timeout;  /* test hook: 1 = the score pass's first tile waits on a
                           copy that is never issued, so its bounded wait runs
                           out and the pass returns SWE_ERR_TIMEOUT */
+  int threshold_path;  /* test hook for the eps threshold pass: 0 = automatic,
+                          1 = rows read from global memory, 2 = bulk-copied rows
+                          with positions read from global memory, 3 = one
+                          bulk-copy row buffer (no double buffering) */
 } swe_opts;
 
 typedef struct {

@@ -31,7 +31,7 @@ int main(int argc, char** argv) {
   swe_status s;
   unsigned* dist;
   const char* dev = getenv("SWGPU_DEVICE");
-  swe_opts o = {0, 0, 0, 0};
+  swe_opts o = {0};
 
   if (argc < 6) {
     printf("Arguments are: \n"

@@ -86,6 +86,7 @@ struct swe_ctx {
   int packs_per_block = 32;
   int threads = 256;
   int inject_timeout = 0;
+  int threshold_path = 0;
   int graph_kernels = 0;
   std::string err;
 
@@ -153,7 +154,8 @@ struct swe_ctx {
   // threshold launches: groups, their row prefix and thresholds
   DevBuf<ThrGroup> d_groups;
   DevBuf<long long> d_rowpre;
-  DevBuf<unsigned> d_thr;
+  DevBuf<unsigned> d_thr, d_thr_status;
+  HostPinned<unsigned> h_thr_status;
   // batched sweeps: one bitmap slot per distinct threshold
   DevBuf<uint64_t> d_bbits;
   DevBuf<int> d_bcounts;
@@ -296,6 +298,7 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
     ctx->threads = opts->threads;
   }
   if (opts && opts->inject_timeout) ctx->inject_timeout = 1;
+  if (opts && opts->threshold_path >= 0 && opts->threshold_path <= 3) ctx->threshold_path = opts->threshold_path;
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
   for (auto& ev : ctx->ev)
@@ -565,8 +568,10 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   const size_t nn = (size_t)ctx->set_base[n_sets];
   ctx->d_D16.release();
   ctx->d_D32.release();
-  if (ctx->dist_bytes == 2) CK(ctx->d_D16.alloc(std::max<size_t>(nn, 1)));
-  else CK(ctx->d_D32.alloc(std::max<size_t>(nn, 1)));
+  // 16 bytes of slack after the last row: the threshold pass copies 16-byte
+  // aligned windows around each row
+  if (ctx->dist_bytes == 2) CK(ctx->d_D16.alloc(nn + 8));
+  else CK(ctx->d_D32.alloc(nn + 4));
 
   // 32-bit path resources: rerun queue (only when the guard can fire) and
   // per-warp boundary columns for sequences longer than one 512-column chunk
@@ -590,9 +595,6 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   CK(fast_set_smem_limit(ctx->smem));
   const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
   ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
-  size_t th_smem = 0;
-  for (int k = 0; k < n_sets; ++k) th_smem = std::max(th_smem, threshold_stage_bytes(set_n[k], ctx->dist_bytes));
-  if (th_smem) CK(threshold_set_smem_limit(th_smem));
   CK(cudaStreamSynchronize(st));
   return SWE_OK;
 }
@@ -806,13 +808,35 @@ static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& group
     p.thr = ctx->d_thr.p;
     p.bits = d_bits;
     p.counts = d_counts;
+    CK(ctx->d_thr_status.alloc(1));
+    CK(ctx->h_thr_status.alloc(1));
+    CK(cudaMemsetAsync(ctx->d_thr_status.p, 0, sizeof(unsigned), ctx->st));
+    p.status = ctx->d_thr_status.p;
+    p.wait_limit = 1u << 22;
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     ctx->stats.kernel_launches += 1;
-    CK(launch_threshold(p, pre.back(), threshold_stage_bytes(maxn, ctx->dist_bytes), ctx->st));
+    ThrPlan plan = threshold_plan(maxn, ctx->dist_bytes);
+    if (ctx->threshold_path == 1) {
+      plan.staged = 0, plan.nbuf = 0, plan.stage_pos = 0, plan.block = 256, plan.smem = 0;
+    } else if (ctx->threshold_path >= 2 && plan.staged) {
+      plan.stage_pos = 0;
+      if (ctx->threshold_path == 3) plan.nbuf = 1;
+      plan.smem = plan.nbuf * plan.rowbuf;
+    }
+    CK(launch_threshold(p, pre.back(), plan, ctx->st));
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(cpy(ctx, ctx->h_thr_status.p, ctx->d_thr_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+  } else {
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(ctx->h_thr_status.alloc(1));
+    ctx->h_thr_status.p[0] = 0;
   }
-  CK(cudaEventRecord(ctx->ev[3], ctx->st));
   return SWE_OK;
 }
+
+// Status word of the last threshold launch; valid once the stream has been
+// synchronised after launch_groups.
+static swe_status thr_status(swe_ctx* ctx) { return check_kernel_status(ctx, ctx->h_thr_status.p[0]); }
 
 // Neighbour bitmap of set s for threshold T on the host (pinned), cached per
 // (set, T).  Rows and columns are in the set's original index order.
@@ -840,6 +864,7 @@ static swe_status ensure_bitmap(swe_ctx* ctx, int s, long long T) {
   CK(cpy(ctx, ctx->h_bits.p, ctx->d_bits.p, words * 8, cudaMemcpyDeviceToHost, ctx->st));
   CK(cpy(ctx, ctx->h_counts.p, ctx->d_counts.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
+  if (swe_status st = thr_status(ctx)) return st;
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
   ctx->stats.ms_last_neighbors = ms;
@@ -1108,6 +1133,7 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
         CK(cpy(ctx, ctx->h_bbits.p, ctx->d_bbits.p, sizeof(uint64_t) * bw, cudaMemcpyDeviceToHost, ctx->st));
         CK(cpy(ctx, ctx->h_bcounts.p, ctx->d_bcounts.p, sizeof(int) * ci, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
+        if (swe_status st = thr_status(ctx)) return st;
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
         kernel_ms += ms;
@@ -1372,6 +1398,7 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
              cudaMemcpyDeviceToHost, ctx->st));
     }
     CK(cudaStreamSynchronize(ctx->st));
+    if (swe_status st = thr_status(ctx)) return st;
     CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
   }
   ctx->stats.ms_last_neighbors = ms;

@@ -17,6 +17,8 @@
 //                          counts (each row read once for all thresholds);
 //   unpermute_kernel       a set's matrix back in original index order;
 //   csr_fill_kernel        bitmap -> ascending CSR column lists.
+#include <algorithm>
+
 #include "sw_device.cuh"
 #include "sw_kernels.cuh"
 #include "sw_wavefront32.cuh"  // sw32_warp
@@ -424,98 +426,226 @@ cudaError_t launch_diag(const DistLayout& L, int n, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// Rows of up to this many bytes are staged in shared memory by the threshold pass.
-constexpr int THRESHOLD_STAGE_MAX = 200 * 1024;
+// ---------------------------------------------------------------------------
+// Threshold pass over groups (set x up to 32 thresholds), persistent over the
+// global row list of all groups.  Each CTA walks rows blockIdx.x + k*grid:
+// one thread brings the row's bytes into shared memory with a bulk copy (TMA
+// engine) completed on an mbarrier, the next row's copy in flight while the
+// current one is processed.  Each warp then gathers two columns per lane
+// through the set's position table (staged in shared memory when it fits)
+// and produces one 64-bit word per threshold with two ballots; lane u keeps
+// threshold u's word and count, so a row is read once for all thresholds.
+// ---------------------------------------------------------------------------
+constexpr size_t THRESHOLD_SMEM_MAX = 220 * 1024;
+constexpr int THR_BLOCK = 512;
 
-// ---------------------------------------------------------------------------
-// Threshold pass over groups (set x up to 32 thresholds).  One CTA per row
-// (global row list over all groups): the row is staged in shared memory once,
-// then each warp gathers two columns per lane through pos[] and produces one
-// 64-bit word per threshold with two ballots; lane u keeps threshold u's word
-// and count, so a row's distances are read once for all its thresholds.
-// ---------------------------------------------------------------------------
-size_t threshold_stage_bytes(int max_n_s, int dist_bytes) {
-  const size_t b = (size_t)max_n_s * (size_t)dist_bytes;
-  return b <= (size_t)THRESHOLD_STAGE_MAX ? ((b + 15) & ~(size_t)15) : 0;
+ThrPlan threshold_plan(int max_n_s, int dist_bytes) {
+  ThrPlan pl{};
+  pl.rowbuf = ((size_t)max_n_s * (size_t)dist_bytes + 32 + 15) & ~(size_t)15;
+  const size_t posb = (size_t)max_n_s * 4;
+  pl.block = THR_BLOCK;
+  if (2 * pl.rowbuf + posb <= THRESHOLD_SMEM_MAX) {
+    pl.staged = 1, pl.nbuf = 2, pl.stage_pos = 1;
+  } else if (2 * pl.rowbuf <= THRESHOLD_SMEM_MAX) {
+    pl.staged = 1, pl.nbuf = 2, pl.stage_pos = 0;
+  } else if (pl.rowbuf <= THRESHOLD_SMEM_MAX) {
+    pl.staged = 1, pl.nbuf = 1, pl.stage_pos = 0;
+  } else {
+    pl.staged = 0, pl.nbuf = 0, pl.stage_pos = 0, pl.block = 256;
+  }
+  pl.smem = pl.staged ? pl.nbuf * pl.rowbuf + (pl.stage_pos ? posb : 0) : 0;
+  return pl;
 }
 
-template <typename DT, bool STAGE>
-__global__ void __launch_bounds__(256) threshold_kernel(ThrParams p, const DT* __restrict__ D, long long total) {
+__device__ __forceinline__ int thr_find_group(const ThrParams& p, long long r) {
+  int lo = 0, hi = p.ngroups - 1;  // last group with row_pre[g] <= r
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (p.row_pre[mid] <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One row: words of threshold `lane` for every 64-column word this warp owns,
+// two words per iteration so that four gathers are in flight per lane.
+template <typename DT>
+__device__ __forceinline__ int thr_row(const ThrParams& p, const ThrGroup& G, int i, const DT* src, const int* ps,
+                                       const unsigned* s_thr, int lane, int warp, int nwarps) {
+  const int ns = G.n_s, nthr = G.nthr;
+  uint64_t* brow = p.bits + G.bits_base + (long long)i * G.wpr;
+  const long long plane = (long long)ns * G.wpr;  // words between thresholds
+  int cnt = 0;
+  for (int w = warp; w < G.wpr; w += 2 * nwarps) {
+    const int wb = w + nwarps;  // second word (warp-uniform validity)
+    const int c0 = w * 64 + lane, c1 = c0 + 32, c2 = wb * 64 + lane, c3 = c2 + 32;
+    const unsigned d0 = c0 < ns ? (unsigned)src[ps[c0]] : 0xFFFFFFFFu;
+    const unsigned d1 = c1 < ns ? (unsigned)src[ps[c1]] : 0xFFFFFFFFu;
+    const unsigned d2 = c2 < ns ? (unsigned)src[ps[c2]] : 0xFFFFFFFFu;
+    const unsigned d3 = c3 < ns ? (unsigned)src[ps[c3]] : 0xFFFFFFFFu;
+    uint64_t ma = 0, mb = 0;
+    for (int u = 0; u < nthr; ++u) {
+      const unsigned t = s_thr[u];
+      const uint32_t a0 = __ballot_sync(0xFFFFFFFFu, c0 < ns && d0 <= t);
+      const uint32_t a1 = __ballot_sync(0xFFFFFFFFu, c1 < ns && d1 <= t);
+      const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c2 < ns && d2 <= t);
+      const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c3 < ns && d3 <= t);
+      if (lane == u) {
+        ma = (uint64_t)a0 | ((uint64_t)a1 << 32);
+        mb = (uint64_t)b0 | ((uint64_t)b1 << 32);
+      }
+    }
+    if (lane < nthr) {
+      brow[lane * plane + w] = ma;
+      cnt += __popcll(ma);
+      if (wb < G.wpr) {
+        brow[lane * plane + wb] = mb;
+        cnt += __popcll(mb);
+      }
+    }
+  }
+  return cnt;
+}
+
+template <typename DT, bool STAGE_POS>
+__global__ void __launch_bounds__(THR_BLOCK) threshold_bulk_kernel(ThrParams p, const DT* __restrict__ D,
+                                                                   long long total, int nbuf, unsigned rowbuf) {
   extern __shared__ __align__(16) uint8_t th_smem[];
-  DT* srow = reinterpret_cast<DT*>(th_smem);
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int s_group[2], s_off[2];
+  __shared__ unsigned s_thr[THR_MAX];
+  __shared__ int s_cnt[THR_BLOCK / 32][THR_MAX];
+  __shared__ int s_ok, s_cur;
+  int* pos_s = reinterpret_cast<int*>(th_smem + (size_t)nbuf * rowbuf);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+
+  // thread 0: bulk copy of row r into buffer b (16-byte aligned window around the row)
+  auto issue = [&](int b, long long r) {
+    const int g = thr_find_group(p, r);
+    const ThrGroup& G = p.groups[g];
+    const int i = (int)(r - p.row_pre[g]);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(D + G.dist_base + (long long)p.pos[G.pos_first + i] * G.n_s);
+    const uintptr_t a16 = a & ~(uintptr_t)15;
+    const unsigned off = (unsigned)(a - a16);
+    const unsigned bytes = (off + (unsigned)G.n_s * (unsigned)sizeof(DT) + 15u) & ~15u;
+    s_group[b] = g;
+    s_off[b] = (int)(off / sizeof(DT));
+    mbar_arrive_expect_tx(&bar[b], bytes);
+    bulk_g2s(th_smem + (size_t)b * rowbuf, reinterpret_cast<const void*>(a16), bytes, &bar[b]);
+  };
+
+  if (tid == 0) {
+    for (int b = 0; b < nbuf; ++b) mbar_init(&bar[b], 1);
+    s_cur = -1;
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int b = 0; b < nbuf; ++b) {
+      const long long r = blockIdx.x + (long long)b * gridDim.x;
+      if (r < total) issue(b, r);
+    }
+  for (long long it = 0;; ++it) {
+    const long long r = blockIdx.x + it * gridDim.x;
+    if (r >= total) break;
+    const int b = (int)(it % nbuf);
+    const unsigned parity = (unsigned)((it / nbuf) & 1);
+    if (tid == 0) s_ok = mbar_wait_bounded(&bar[b], parity, p.wait_limit) ? 1 : 0;
+    __syncthreads();
+    if (!s_ok) {  // CTA-uniform
+      if (tid == 0) {
+        atomicOr(p.status, KST_TIMEOUT);
+        // let every copy this CTA issued land before it leaves
+        for (int k = 0; k < nbuf; ++k) {
+          const long long it2 = it + k;
+          if (blockIdx.x + it2 * gridDim.x < total)
+            mbar_wait_bounded(&bar[it2 % nbuf], (unsigned)((it2 / nbuf) & 1), p.wait_limit);
+        }
+      }
+      break;
+    }
+    const int g = s_group[b];
+    const ThrGroup G = p.groups[g];
+    const int i = (int)(r - p.row_pre[g]);
+    if (g != s_cur) {  // CTA-uniform: thresholds (and positions) of a new group
+      if (tid < G.nthr) s_thr[tid] = p.thr[G.thr_first + tid];
+      if (STAGE_POS)
+        for (int k = tid; k < G.n_s; k += blockDim.x) pos_s[k] = p.pos[G.pos_first + k];
+      __syncthreads();
+      if (tid == 0) s_cur = g;
+    }
+    const DT* src = reinterpret_cast<const DT*>(th_smem + (size_t)b * rowbuf) + s_off[b];
+    const int* ps = STAGE_POS ? pos_s : p.pos + G.pos_first;
+    const int cnt = thr_row<DT>(p, G, i, src, ps, s_thr, lane, warp, nwarps);
+    if (lane < G.nthr) s_cnt[warp][lane] = cnt;
+    __syncthreads();  // buffer b, s_cnt and s_cur are complete
+    if (tid < G.nthr) {
+      int c = 0;
+      for (int k = 0; k < nwarps; ++k) c += s_cnt[k][tid];
+      p.counts[G.counts_base + (long long)tid * G.n_s + i] = c;
+    }
+    if (tid == 0) {
+      const long long rn = r + (long long)nbuf * gridDim.x;
+      if (rn < total) issue(b, rn);
+    }
+  }
+}
+
+// Rows longer than shared memory: gathered straight from global memory.
+template <typename DT>
+__global__ void __launch_bounds__(256) threshold_global_kernel(ThrParams p, const DT* __restrict__ D,
+                                                               long long total) {
   __shared__ unsigned s_thr[THR_MAX];
   __shared__ int s_cnt[8][THR_MAX];
   __shared__ int s_group;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (long long r = blockIdx.x; r < total; r += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = p.ngroups - 1;  // last group with row_pre[g] <= r
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (p.row_pre[mid] <= r) lo = mid;
-        else hi = mid - 1;
-      }
-      s_group = lo;
-    }
+    if (threadIdx.x == 0) s_group = thr_find_group(p, r);
     __syncthreads();
     const ThrGroup G = p.groups[s_group];
     const int i = (int)(r - p.row_pre[s_group]);
-    const int ns = G.n_s, nthr = G.nthr;
-    const int* pos = p.pos + G.pos_first;
-    const DT* row = D + G.dist_base + (long long)pos[i] * ns;
-    if (threadIdx.x < nthr) s_thr[threadIdx.x] = p.thr[G.thr_first + threadIdx.x];
-    if (STAGE)
-      for (int k = threadIdx.x; k < ns; k += blockDim.x) srow[k] = row[k];
+    if (threadIdx.x < G.nthr) s_thr[threadIdx.x] = p.thr[G.thr_first + threadIdx.x];
     __syncthreads();
-    const DT* src = STAGE ? srow : row;
-    int cnt = 0;
-    for (int w = warp; w < G.wpr; w += nwarps) {
-      const int c0 = w * 64 + lane, c1 = c0 + 32;
-      const unsigned d0 = c0 < ns ? (unsigned)src[pos[c0]] : 0xFFFFFFFFu;
-      const unsigned d1 = c1 < ns ? (unsigned)src[pos[c1]] : 0xFFFFFFFFu;
-      uint64_t mine = 0;
-      for (int u = 0; u < nthr; ++u) {
-        const unsigned t = s_thr[u];
-        const uint32_t lo = __ballot_sync(0xFFFFFFFFu, c0 < ns && d0 <= t);
-        const uint32_t hi = __ballot_sync(0xFFFFFFFFu, c1 < ns && d1 <= t);
-        if (lane == u) mine = (uint64_t)lo | ((uint64_t)hi << 32);
-      }
-      if (lane < nthr) {
-        p.bits[G.bits_base + ((long long)lane * ns + i) * G.wpr + w] = mine;
-        cnt += __popcll(mine);
-      }
-    }
-    if (lane < nthr) s_cnt[warp][lane] = cnt;
+    const int* ps = p.pos + G.pos_first;
+    const DT* row = D + G.dist_base + (long long)ps[i] * G.n_s;
+    const int cnt = thr_row<DT>(p, G, i, row, ps, s_thr, lane, warp, nwarps);
+    if (lane < G.nthr) s_cnt[warp][lane] = cnt;
     __syncthreads();
-    if (threadIdx.x < nthr) {
+    if (threadIdx.x < G.nthr) {
       int c = 0;
       for (int k = 0; k < nwarps; ++k) c += s_cnt[k][threadIdx.x];
-      p.counts[G.counts_base + (long long)threadIdx.x * ns + i] = c;
+      p.counts[G.counts_base + (long long)threadIdx.x * G.n_s + i] = c;
     }
-    __syncthreads();  // srow, s_thr, s_cnt and s_group are reused by the next row
+    __syncthreads();  // s_group, s_thr and s_cnt are reused by the next row
   }
 }
 
-cudaError_t threshold_set_smem_limit(size_t bytes) {
-  cudaError_t e = cudaFuncSetAttribute(threshold_kernel<uint16_t, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(threshold_kernel<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bytes);
-  return e;
-}
-
-cudaError_t launch_threshold(const ThrParams& p, long long total_rows, size_t stage_bytes, cudaStream_t st) {
-  if (total_rows <= 0 || p.ngroups <= 0) return cudaSuccess;
-  const int grid = total_rows < 148 * 8 ? (int)total_rows : 148 * 8;
-  if (p.D16) {
-    if (stage_bytes) threshold_kernel<uint16_t, true><<<grid, 256, stage_bytes, st>>>(p, p.D16, total_rows);
-    else threshold_kernel<uint16_t, false><<<grid, 256, 0, st>>>(p, p.D16, total_rows);
-  } else {
-    if (stage_bytes) threshold_kernel<uint32_t, true><<<grid, 256, stage_bytes, st>>>(p, p.D32, total_rows);
-    else threshold_kernel<uint32_t, false><<<grid, 256, 0, st>>>(p, p.D32, total_rows);
+template <typename DT>
+static cudaError_t launch_threshold_t(const ThrParams& p, const DT* D, long long total, const ThrPlan& pl,
+                                      cudaStream_t st) {
+  int dev = 0, sms = 148, occ = 1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (!pl.staged) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, threshold_global_kernel<DT>, 256, 0);
+    if (e != cudaSuccess) return e;
+    const long long grid = std::min<long long>(total, (long long)sms * std::max(occ, 1));
+    threshold_global_kernel<DT><<<(int)grid, 256, 0, st>>>(p, D, total);
+    return cudaGetLastError();
   }
+  auto kern = pl.stage_pos ? threshold_bulk_kernel<DT, true> : threshold_bulk_kernel<DT, false>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, pl.block, pl.smem);
+  if (e != cudaSuccess) return e;
+  const long long grid = std::min<long long>(total, (long long)sms * std::max(occ, 1));
+  kern<<<(int)grid, pl.block, pl.smem, st>>>(p, D, total, pl.nbuf, (unsigned)pl.rowbuf);
   return cudaGetLastError();
+}
+
+cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const ThrPlan& plan, cudaStream_t st) {
+  if (total_rows <= 0 || p.ngroups <= 0) return cudaSuccess;
+  if (p.D16) return launch_threshold_t<uint16_t>(p, p.D16, total_rows, plan, st);
+  return launch_threshold_t<uint32_t>(p, p.D32, total_rows, plan, st);
 }
 
 // Set matrix in original index order, widened to 32 bits.

@@ -138,12 +138,19 @@ struct ThrParams {
   const unsigned* thr;
   uint64_t* bits;
   int* counts;
+  unsigned* status;          // KST_TIMEOUT when a bounded wait gave up
+  unsigned wait_limit;       // attempts of the bounded mbarrier wait
 };
-// stage_bytes: the largest set row in bytes when every row is staged in
-// shared memory, 0 to read rows from global memory.
-cudaError_t launch_threshold(const ThrParams& p, long long total_rows, size_t stage_bytes, cudaStream_t st);
-size_t threshold_stage_bytes(int max_n_s, int dist_bytes);
-cudaError_t threshold_set_smem_limit(size_t bytes);
+// Shared-memory plan of a threshold launch whose largest set has max_n_s
+// sequences: rows arrive by bulk copy into nbuf row buffers (double-buffered
+// when two fit), the set's position table is staged too when it fits, and
+// rows too long for shared memory are read from global memory (staged == 0).
+struct ThrPlan {
+  int staged, nbuf, stage_pos, block;
+  size_t rowbuf, smem;
+};
+ThrPlan threshold_plan(int max_n_s, int dist_bytes);
+cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const ThrPlan& plan, cudaStream_t st);
 // CSR from a bitmap: ascending column indices per row at row_ptr[i].
 cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, const long long* row_ptr,
                             int* cols, cudaStream_t st);

@@ -57,7 +57,8 @@ class SplitSet(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("sat_limit", C.c_int), ("packs_per_block", C.c_int),
-                ("threads", C.c_int), ("inject_timeout", C.c_int)]
+                ("threads", C.c_int), ("inject_timeout", C.c_int),
+                ("threshold_path", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -207,9 +208,9 @@ class Engine:
     """One engine context (one CUDA stream on one device)."""
 
     def __init__(self, device: int = 0, sat_limit: int = 0, packs_per_block: int = 0, threads: int = 0,
-                 inject_timeout: int = 0):
+                 inject_timeout: int = 0, threshold_path: int = 0):
         self.ctx = C.c_void_p()
-        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout)
+        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path)
         _check(lib().swe_create(C.byref(self.ctx), C.byref(opts)))
         self.n = 0
         self._buf = None

@@ -151,26 +151,34 @@ def test_long_sequences_need_uint32_matrix():
     seqs = [W.BASES[rng.integers(0, 4, size=17000)].tobytes()]
     seqs.append(W._mutate(rng, np.frombuffer(seqs[0], dtype=np.uint8).copy(), 0.02, 0.0).tobytes())
     seqs.append(W.BASES[rng.integers(0, 4, size=300)].tobytes())
+    seqs += [W.BASES[rng.integers(0, 4, size=int(rng.integers(50, 300)))].tobytes() for _ in range(70)]
     e = swgpu.Engine()
     D = _matrix(e, seqs)
     assert e.stats()["dist_bytes"] == 4
-    e.close()
     for i in range(3):
         for k in range(3):
             assert D[i, k] == O.score(seqs[k], seqs[i]), (i, k)
+    ref = O.all_pairs(seqs)
+    assert np.array_equal(D, ref)
+    for eps in [500.0, 1200.0, 70000.0]:
+        assert e.dbscan(eps, 2) == O.dbscan(ref, eps, 2), eps
+    e.close()
 
 
-def test_many_sets_in_one_upload_match_one_by_one():
+@pytest.mark.parametrize("threshold_path", [0, 1, 2, 3])
+def test_many_sets_in_one_upload_match_one_by_one(threshold_path):
     """Independent sets scored in one pass: each set's matrix equals the oracle's
     for that set alone (no pair across sets), and per-set neighbourhoods and
     DBSCAN equal the single-set results.  Sizes include empty and one-sequence
-    sets and sets with 32-bit-path sequences only."""
+    sets and sets with 32-bit-path sequences only.  Every path of the threshold
+    pass (global gather, bulk-copied rows with and without staged positions,
+    one or two row buffers) gives the same bits."""
     rng = np.random.default_rng(31)
     mixed = _mixed_set(rng)
     pool, _ = W.config1()
     sets = [pool[:150], [], [pool[200]], mixed[:20], [b"", b"N" * 3, b"ACGT" * 300], pool[300:301] * 5,
             mixed, pool[400:1000], [pool[1100], pool[1101]]]
-    e = swgpu.Engine()
+    e = swgpu.Engine(threshold_path=threshold_path)
     e.upload_sets(sets)
     assert e.set_count() == len(sets)
     e.score_all_pairs()
@@ -189,6 +197,13 @@ def test_many_sets_in_one_upload_match_one_by_one():
         for i in range(len(st)):
             want = np.nonzero(ref[i].astype(np.float32) <= np.float32(90.0))[0]
             assert np.array_equal(cols[rp[i]:rp[i + 1]], want), (k, i)
+    # many thresholds of many sets in one launch
+    res = e.adaptive_sets(100.0, 37.0, 3, max_steps=12)
+    for k, st in enumerate(sets):
+        if len(st) >= 3 and len(set(st)) > 1:
+            D = O.all_pairs(st)
+            text, kept = O.adaptive(D, 100.0, 37.0, 3, max_steps=12, truncate=True)
+            assert res[k]["log"] == text and res[k]["layers"] == kept, k
     e.close()
 
 

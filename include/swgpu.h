@@ -48,10 +48,10 @@ typedef struct {
   int inject_timeout;  /* test hook: 1 = the score pass's first tile waits on a
                           copy that is never issued, so its bounded wait runs
                           out and the pass returns SWE_ERR_TIMEOUT */
-  int threshold_path;  /* test hook for the eps threshold pass: 0 = automatic,
-                          1 = rows read from global memory, 2 = bulk-copied rows
-                          with positions read from global memory, 3 = one
-                          bulk-copy row buffer (no double buffering) */
+  int threshold_path;  /* test hook for the eps threshold pass: 0 = automatic
+                          (bulk-copied rows, double-buffered), 1 = rows read
+                          from global memory, 2 = positions staged in shared
+                          memory too, 3 = one bulk-copy row buffer */
 } swe_opts;
 
 typedef struct {
@@ -220,6 +220,45 @@ swe_status swe_timer_stop(swe_ctx* ctx, double* ms);
 #define SWE_NOALLOC_MAX_LEN 65535
 swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* off, const int* len, const int* pairs,
                                    int64_t npairs, unsigned* out, int max_len, void* stream);
+
+/* ------------------------------------------------------------------------
+   Learned prefilter (no counterpart in the reference).  Features are the
+   5-mer counts of kmers.c (windows 0 .. len-6, A0 C1 G2 T3, windows with other
+   symbols count nothing), L1-normalised; an MLP 1024 -> 512 -> 256 -> 128 with
+   exact GELU after the first two layers, bf16 weights and fp32 accumulation,
+   maps them to embeddings whose L2 distance is trained (MSE) to predict
+   d / (4 * max(len_a, len_b)) of the exact distance d.  The exact engine
+   stays the default; the prefilter only decides which pairs to score.
+   ------------------------------------------------------------------------ */
+
+/* k-mer features (k = 1..6) of the uploaded sequences: out holds n * 4^k
+   floats (row i = sequence i), or NULL to only compute them. */
+swe_status swe_kmer_features(swe_ctx* ctx, int k, float* out);
+
+/* Random initial weights (uniform +-1/sqrt(fan_in), seeded). */
+swe_status swe_prefilter_init(swe_ctx* ctx, uint64_t seed);
+/* Number of parameters: W1 [512x1024], b1, W2 [256x512], b2, W3 [128x256], b3,
+   in that order, row-major, in one flat fp32 vector. */
+int64_t swe_prefilter_param_count(void);
+/* Copies the fp32 master parameters out (get != NULL) and/or in (set != NULL). */
+swe_status swe_prefilter_params(swe_ctx* ctx, float* get, const float* set);
+/* Mean loss over the pairs (a[k], b[k]) with exact distances dist[k], and
+   the gradient of every parameter (same layout as the parameters). */
+swe_status swe_prefilter_loss_grad(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int npairs,
+                                   float* loss, float* grad);
+/* Adam training over the pairs for `epochs` passes in shuffled batches of
+   batch_pairs pairs (full batches only); epoch_loss[e] = mean batch loss. */
+swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int64_t npairs,
+                               int epochs, int batch_pairs, float lr, uint64_t seed, float* epoch_loss);
+/* Embeddings of the uploaded sequences (out: n x 128, or NULL). */
+swe_status swe_prefilter_embed(swe_ctx* ctx, float* out);
+/* Embedding distances of explicit pairs. */
+swe_status swe_prefilter_pair_dist(swe_ctx* ctx, const int* a, const int* b, int64_t np, float* out);
+/* The tensor-core GEMM alone, for tests: C[M x N] = A[M x K] * B[N x K]^T
+   (+ bias, GELU when act = 1) with A, B bf16 and C fp32 DEVICE pointers;
+   M and N multiples of 128, K a multiple of 64. */
+swe_status swe_gemm_bf16(int device, const void* A, const void* B, int M, int N, int K, const float* bias, int act,
+                         float* C);
 
 void swe_free(void* p);
 

@@ -20,172 +20,11 @@
 #include <thread>
 #include <vector>
 
-#include "host_internal.h"
-#include "sw_device.cuh"
-#include "sw_kernels.cuh"
+#include "engine_ctx.cuh"
 
 using namespace swgpu;
 
-namespace {
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  cudaError_t alloc(size_t count) {
-    if (p && count <= n) return cudaSuccess;
-    release();
-    if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
-    if (e == cudaSuccess) n = count;
-    else p = nullptr;
-    return e;
-  }
-};
-
-template <typename T>
-struct HostPinned {
-  T* p = nullptr;
-  size_t n = 0;
-  HostPinned() = default;
-  HostPinned(const HostPinned&) = delete;
-  HostPinned& operator=(const HostPinned&) = delete;
-  ~HostPinned() { release(); }
-  void release() {
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    n = 0;
-  }
-  cudaError_t alloc(size_t count) {
-    if (p && count <= n) return cudaSuccess;
-    release();
-    if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), count * sizeof(T));
-    if (e == cudaSuccess) n = count;
-    else p = nullptr;
-    return e;
-  }
-};
-
-}  // namespace
-
-struct swe_ctx {
-  int device = 0;
-  cudaStream_t st = nullptr;
-  int num_sms = 148;
-  int sat_limit = 32000;
-  int packs_per_block = 32;
-  int threads = 256;
-  int inject_timeout = 0;
-  int threshold_path = 0;
-  int graph_kernels = 0;
-  std::string err;
-
-  // dataset (host)
-  int n = 0;
-  int max_len = 0;
-  int max_fast_len = 0;
-  int nfast = 0;
-  std::vector<int> len;
-  std::vector<int64_t> off;
-  std::vector<uint8_t> codes;
-  int code_of[256];
-  std::vector<int> order, exc;
-  std::vector<uint8_t> is_exc;
-  int npacks = 0;
-  int max_block_rows = 0;
-  int max_cols = 0;
-  size_t smem = 0;
-  int fast_grid = 0;
-  std::vector<FastTile> tiles;
-
-  // sets (independent datasets in one upload) and the sorted layout
-  int n_sets = 0;
-  std::vector<int> set_first, set_nfast;  // set_first has n_sets + 1 entries
-  std::vector<long long> set_base;        // n_sets + 1 entries
-  std::vector<int> pos, set_of;           // per original index
-  std::vector<long long> exc_pre;
-
-  // dataset (device)
-  DevBuf<uint8_t> d_codes;
-  DevBuf<int64_t> d_off;
-  DevBuf<int> d_len, d_order, d_exc, d_pack_off, d_pack_rows;
-  DevBuf<uint8_t> d_isexc;
-  DevBuf<int> d_pos, d_setof, d_set_first, d_set_n, d_set_nfast, d_pack_first, d_block_first, d_block_npacks;
-  DevBuf<long long> d_set_base, d_exc_pre;
-  DevBuf<uint8_t> d_pack_pair;
-  int nblocks = 0;
-  DevBuf<uint16_t> d_sel;
-  DevBuf<FastTile> d_tiles;
-  DevBuf<unsigned> d_ctr;  // [0] tile counter, [1] status, [2] rerun count
-  DevBuf<int2> d_rerun;
-  unsigned rerun_cap = 0;
-  bool rerun_possible = false;
-  DevBuf<int> d_scratch;
-  long long scratch_stride = 0;
-  int gen_grid = 0;
-
-  // distances
-  DevBuf<uint16_t> d_D16;
-  DevBuf<uint32_t> d_D32;
-  int dist_bytes = 2;
-  bool scored = false;
-  cudaGraphExec_t graph = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t tev[2] = {nullptr, nullptr};
-
-  // neighbour bitmaps
-  int wpr = 0;
-  DevBuf<uint64_t> d_bits;
-  DevBuf<int> d_counts;
-  HostPinned<uint64_t> h_bits;
-  HostPinned<int> h_counts;
-  long long bits_T = LLONG_MIN;
-  int bits_set = -1;
-  // threshold launches: groups, their row prefix and thresholds
-  DevBuf<ThrGroup> d_groups;
-  DevBuf<long long> d_rowpre;
-  DevBuf<unsigned> d_thr, d_thr_status;
-  HostPinned<unsigned> h_thr_status;
-  // batched sweeps: one bitmap slot per distinct threshold
-  DevBuf<uint64_t> d_bbits;
-  DevBuf<int> d_bcounts;
-  HostPinned<uint64_t> h_bbits;
-  HostPinned<int> h_bcounts;
-
-  // small transfers
-  DevBuf<uint8_t> d_q;
-  DevBuf<unsigned> d_out;
-  DevBuf<int2> d_pairs;
-  DevBuf<int64_t> d_small_off;
-  DevBuf<int> d_small_len;
-  DevBuf<int> d_small_scratch;
-  DevBuf<long long> d_row_ptr;
-  DevBuf<int> d_cols;
-
-  swe_stats stats{};
-
-  ~swe_ctx() {
-    cudaSetDevice(device);
-    if (graph) cudaGraphExecDestroy(graph);
-    for (auto& e : ev)
-      if (e) cudaEventDestroy(e);
-    for (auto& e : tev)
-      if (e) cudaEventDestroy(e);
-    if (st) cudaStreamDestroy(st);
-  }
-};
-
-namespace {
+namespace swgpu {
 
 swe_status fail(swe_ctx* ctx, swe_status s, const std::string& msg) {
   if (ctx) ctx->err = msg;
@@ -197,18 +36,16 @@ swe_status cuda_fail(swe_ctx* ctx, cudaError_t e, const char* what) {
   return fail(ctx, s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define CK(call)                                          \
-  do {                                                    \
-    cudaError_t e_ = (call);                              \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
-  } while (0)
-
 swe_status check_kernel_status(swe_ctx* ctx, unsigned status) {
   if (status & KST_TIMEOUT) return fail(ctx, SWE_ERR_TIMEOUT, "device-side wait timed out");
   if (status & KST_RERUN_OVERFLOW) return fail(ctx, SWE_ERR_RERUN, "32-bit rerun queue overflowed");
   if (status & KST_BAD_TILE) return fail(ctx, SWE_ERR_STATE, "invalid tile descriptor");
   return SWE_OK;
 }
+
+}  // namespace swgpu
+
+namespace {
 
 void drop_graph(swe_ctx* ctx) {
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
@@ -236,7 +73,10 @@ void build_code_table(const uint64_t* freq, int* code_of) {
     if (code_of[c] < 0) code_of[c] = next++;
 }
 
-// Stream-ordered copy that also counts the bytes crossing PCIe.
+}  // namespace
+
+namespace swgpu {
+
 cudaError_t cpy(swe_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
   if (kind == cudaMemcpyHostToDevice) ctx->stats.h2d_bytes += (int64_t)bytes;
   else if (kind == cudaMemcpyDeviceToHost) ctx->stats.d2h_bytes += (int64_t)bytes;
@@ -248,7 +88,7 @@ swe_status select_device(swe_ctx* ctx) {
   return SWE_OK;
 }
 
-}  // namespace
+}  // namespace swgpu
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -374,6 +214,9 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   }
   ctx->max_len = max_len;
   build_code_table(freq, ctx->code_of);
+  ctx->upload_gen++;
+  ctx->first_code.assign(std::max(n, 1), 0);
+  for (int i = 0; i < n; ++i) ctx->first_code[i] = (uint8_t)ctx->code_of[(unsigned char)(seqs[i] ? seqs[i][0] : 0)];
   ctx->codes.assign((size_t)std::max<int64_t>(total, 16), 0);
   int max_fast = 0;
   for (int i = 0; i < n; ++i) {
@@ -537,6 +380,7 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
     return e;
   };
   CK(up(ctx->d_codes, ctx->codes));
+  CK(up(ctx->d_first, ctx->first_code));
   CK(up(ctx->d_off, ctx->off));
   CK(up(ctx->d_len, ctx->len));
   CK(up(ctx->d_order, ctx->order));
@@ -818,10 +662,13 @@ static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& group
     ThrPlan plan = threshold_plan(maxn, ctx->dist_bytes);
     if (ctx->threshold_path == 1) {
       plan.staged = 0, plan.nbuf = 0, plan.stage_pos = 0, plan.block = 256, plan.smem = 0;
-    } else if (ctx->threshold_path >= 2 && plan.staged) {
-      plan.stage_pos = 0;
-      if (ctx->threshold_path == 3) plan.nbuf = 1;
-      plan.smem = plan.nbuf * plan.rowbuf;
+    } else if (ctx->threshold_path == 2 && plan.staged) {
+      plan.stage_pos = 1;
+      plan.smem = plan.nbuf * plan.rowbuf + (size_t)maxn * 4;
+      if (plan.smem > 220 * 1024) plan.stage_pos = 0, plan.smem = plan.nbuf * plan.rowbuf;
+    } else if (ctx->threshold_path == 3 && plan.staged) {
+      plan.nbuf = 1;
+      plan.smem = plan.rowbuf;
     }
     CK(launch_threshold(p, pre.back(), plan, ctx->st));
     CK(cudaEventRecord(ctx->ev[3], ctx->st));

@@ -1,0 +1,198 @@
+// Engine context shared by the engine's translation units (no public ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "host_internal.h"
+#include "sw_device.cuh"
+#include "sw_kernels.cuh"
+
+namespace swgpu {
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (p && count <= n) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+template <typename T>
+struct HostPinned {
+  T* p = nullptr;
+  size_t n = 0;
+  HostPinned() = default;
+  HostPinned(const HostPinned&) = delete;
+  HostPinned& operator=(const HostPinned&) = delete;
+  ~HostPinned() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (p && count <= n) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+};
+
+struct PrefilterState;
+void prefilter_destroy(PrefilterState* pf);
+
+}  // namespace swgpu
+
+struct swe_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int num_sms = 148;
+  int sat_limit = 32000;
+  int packs_per_block = 32;
+  int threads = 256;
+  int inject_timeout = 0;
+  int threshold_path = 0;
+  int graph_kernels = 0;
+  std::string err;
+
+  // dataset (host)
+  int n = 0;
+  int max_len = 0;
+  int max_fast_len = 0;
+  int nfast = 0;
+  std::vector<int> len;
+  std::vector<int64_t> off;
+  std::vector<uint8_t> codes;
+  int code_of[256];
+  std::vector<int> order, exc;
+  std::vector<uint8_t> is_exc;
+  int npacks = 0;
+  int max_block_rows = 0;
+  int max_cols = 0;
+  size_t smem = 0;
+  int fast_grid = 0;
+  std::vector<swgpu::FastTile> tiles;
+
+  // sets (independent datasets in one upload) and the sorted layout
+  int n_sets = 0;
+  std::vector<int> set_first, set_nfast;  // set_first has n_sets + 1 entries
+  std::vector<long long> set_base;        // n_sets + 1 entries
+  std::vector<int> pos, set_of;           // per original index
+  std::vector<long long> exc_pre;
+
+  int upload_gen = 0;               // bumped by every upload
+  std::vector<uint8_t> first_code;  // code of s[0] per sequence (k-mer features)
+
+  // dataset (device)
+  swgpu::DevBuf<uint8_t> d_codes, d_first;
+  swgpu::DevBuf<int64_t> d_off;
+  swgpu::DevBuf<int> d_len, d_order, d_exc, d_pack_off, d_pack_rows;
+  swgpu::DevBuf<uint8_t> d_isexc;
+  swgpu::DevBuf<int> d_pos, d_setof, d_set_first, d_set_n, d_set_nfast, d_pack_first, d_block_first, d_block_npacks;
+  swgpu::DevBuf<long long> d_set_base, d_exc_pre;
+  swgpu::DevBuf<uint8_t> d_pack_pair;
+  int nblocks = 0;
+  swgpu::DevBuf<uint16_t> d_sel;
+  swgpu::DevBuf<swgpu::FastTile> d_tiles;
+  swgpu::DevBuf<unsigned> d_ctr;  // [0] tile counter, [1] status, [2] rerun count
+  swgpu::DevBuf<int2> d_rerun;
+  unsigned rerun_cap = 0;
+  bool rerun_possible = false;
+  swgpu::DevBuf<int> d_scratch;
+  long long scratch_stride = 0;
+  int gen_grid = 0;
+
+  // distances
+  swgpu::DevBuf<uint16_t> d_D16;
+  swgpu::DevBuf<uint32_t> d_D32;
+  int dist_bytes = 2;
+  bool scored = false;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t tev[2] = {nullptr, nullptr};
+
+  // neighbour bitmaps
+  int wpr = 0;
+  swgpu::DevBuf<uint64_t> d_bits;
+  swgpu::DevBuf<int> d_counts;
+  swgpu::HostPinned<uint64_t> h_bits;
+  swgpu::HostPinned<int> h_counts;
+  long long bits_T = LLONG_MIN;
+  int bits_set = -1;
+  // threshold launches: groups, their row prefix and thresholds
+  swgpu::DevBuf<swgpu::ThrGroup> d_groups;
+  swgpu::DevBuf<long long> d_rowpre;
+  swgpu::DevBuf<unsigned> d_thr, d_thr_status;
+  swgpu::HostPinned<unsigned> h_thr_status;
+  // batched sweeps: one bitmap slot per distinct threshold
+  swgpu::DevBuf<uint64_t> d_bbits;
+  swgpu::DevBuf<int> d_bcounts;
+  swgpu::HostPinned<uint64_t> h_bbits;
+  swgpu::HostPinned<int> h_bcounts;
+
+  // small transfers
+  swgpu::DevBuf<uint8_t> d_q;
+  swgpu::DevBuf<unsigned> d_out;
+  swgpu::DevBuf<int2> d_pairs;
+  swgpu::DevBuf<int64_t> d_small_off;
+  swgpu::DevBuf<int> d_small_len;
+  swgpu::DevBuf<int> d_small_scratch;
+  swgpu::DevBuf<long long> d_row_ptr;
+  swgpu::DevBuf<int> d_cols;
+
+  swe_stats stats{};
+
+  // learned prefilter (null until first used)
+  swgpu::PrefilterState* pf = nullptr;
+
+  ~swe_ctx() {
+    cudaSetDevice(device);
+    swgpu::prefilter_destroy(pf);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : tev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+namespace swgpu {
+
+swe_status fail(swe_ctx* ctx, swe_status s, const std::string& msg);
+swe_status cuda_fail(swe_ctx* ctx, cudaError_t e, const char* what);
+swe_status check_kernel_status(swe_ctx* ctx, unsigned status);
+// Stream-ordered copy that also counts the bytes crossing PCIe.
+cudaError_t cpy(swe_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st);
+swe_status select_device(swe_ctx* ctx);
+
+}  // namespace swgpu
+
+#define CK(call)                                                      \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) return swgpu::cuda_fail(ctx, e_, #call);   \
+  } while (0)

@@ -90,6 +90,9 @@ EXPORTS = [
     "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop", "swe_score_pairs_noalloc",
     "swe_upload_sets", "swe_set_count", "swe_copy_set_distances", "swe_neighbors_set", "swe_dbscan_set",
     "swe_adaptive_set", "swe_adaptive_sets", "swe_free_sweep_results",
+    "swe_kmer_features", "swe_prefilter_init", "swe_prefilter_param_count", "swe_prefilter_params",
+    "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
+    "swe_gemm_bf16",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -145,6 +148,27 @@ def lib():
         L.swe_adaptive_sets.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_int, C.c_char_p,
                                         C.POINTER(SweepResult)]
         L.swe_free_sweep_results.argtypes = [C.POINTER(SweepResult), C.c_int]
+        L.swe_kmer_features.restype = C.c_int
+        L.swe_kmer_features.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.swe_prefilter_init.restype = C.c_int
+        L.swe_prefilter_init.argtypes = [C.c_void_p, C.c_uint64]
+        L.swe_prefilter_param_count.restype = C.c_int64
+        L.swe_prefilter_param_count.argtypes = []
+        L.swe_prefilter_params.restype = C.c_int
+        L.swe_prefilter_params.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.swe_prefilter_loss_grad.restype = C.c_int
+        L.swe_prefilter_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                              C.POINTER(C.c_float), C.c_void_p]
+        L.swe_prefilter_train.restype = C.c_int
+        L.swe_prefilter_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
+                                          C.c_int, C.c_float, C.c_uint64, C.c_void_p]
+        L.swe_prefilter_embed.restype = C.c_int
+        L.swe_prefilter_embed.argtypes = [C.c_void_p, C.c_void_p]
+        L.swe_prefilter_pair_dist.restype = C.c_int
+        L.swe_prefilter_pair_dist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.swe_gemm_bf16.restype = C.c_int
+        L.swe_gemm_bf16.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                    C.c_int, C.c_void_p]
         L.swe_score_one_to_many.restype = C.c_int
         L.swe_score_one_to_many.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, C.c_void_p]
         L.swe_score_pairs.restype = C.c_int
@@ -339,6 +363,60 @@ class Engine:
                         "layers": [split_set_to_lists(r.layers[i]) for i in range(r.n_layers)],
                         "done_ms": r.done_ms})
         lib().swe_free_sweep_results(res, S)
+        return out
+
+    # ---------------------------------------------------------------- prefilter
+    def kmer_features(self, k: int = 5) -> np.ndarray:
+        out = np.zeros((self.n, 4 ** k), dtype=np.float32)
+        _check(lib().swe_kmer_features(self.ctx, k, out.ctypes.data), self.ctx)
+        return out
+
+    def prefilter_init(self, seed: int = 0):
+        _check(lib().swe_prefilter_init(self.ctx, seed), self.ctx)
+
+    def prefilter_params(self, set_to: np.ndarray | None = None) -> np.ndarray:
+        n = lib().swe_prefilter_param_count()
+        out = np.zeros(n, dtype=np.float32)
+        src = None
+        if set_to is not None:
+            src = np.ascontiguousarray(set_to, dtype=np.float32)
+            assert src.size == n
+        _check(lib().swe_prefilter_params(self.ctx, out.ctypes.data, src.ctypes.data if src is not None else None),
+               self.ctx)
+        return out if set_to is None else src.copy()
+
+    @staticmethod
+    def _pairs(a, b, d=None):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.int32)
+        d = None if d is None else np.ascontiguousarray(d, dtype=np.uint32)
+        return a, b, d
+
+    def prefilter_loss_grad(self, a, b, dist):
+        a, b, d = self._pairs(a, b, dist)
+        loss = C.c_float()
+        grad = np.zeros(lib().swe_prefilter_param_count(), dtype=np.float32)
+        _check(lib().swe_prefilter_loss_grad(self.ctx, a.ctypes.data, b.ctypes.data, d.ctypes.data, len(a),
+                                             C.byref(loss), grad.ctypes.data), self.ctx)
+        return loss.value, grad
+
+    def prefilter_train(self, a, b, dist, epochs: int, batch_pairs: int = 4096, lr: float = 1e-3, seed: int = 0):
+        a, b, d = self._pairs(a, b, dist)
+        losses = np.zeros(max(epochs, 1), dtype=np.float32)
+        _check(lib().swe_prefilter_train(self.ctx, a.ctypes.data, b.ctypes.data, d.ctypes.data, len(a), epochs,
+                                         batch_pairs, C.c_float(lr), seed, losses.ctypes.data), self.ctx)
+        return losses[:epochs]
+
+    def prefilter_embed(self) -> np.ndarray:
+        out = np.zeros((self.n, 128), dtype=np.float32)
+        _check(lib().swe_prefilter_embed(self.ctx, out.ctypes.data), self.ctx)
+        return out
+
+    def prefilter_pair_dist(self, a, b) -> np.ndarray:
+        a, b, _ = self._pairs(a, b)
+        out = np.zeros(len(a), dtype=np.float32)
+        _check(lib().swe_prefilter_pair_dist(self.ctx, a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data),
+               self.ctx)
         return out
 
     def one_to_many(self, q: bytes, qlen: int | None = None) -> np.ndarray:

@@ -273,10 +273,41 @@ def subset_goldens():
     matrix_golden("config3_head1500_golden", s3[:1500])
 
 
+def kmer_golden():
+    """5-mer counts from the reference's own frequence_of_kmer_in_sequence()
+    (kmers.c:157-229) over the k-mer strings of gen_dna_kmers() (kmers.c:87-107),
+    so index b of the table is the reference's own k-mer order."""
+    import ctypes as C
+    R = O.ref_lib()
+    R.gen_dna_kmers.restype = C.POINTER(C.c_char_p)
+    R.gen_dna_kmers.argtypes = [C.c_size_t]
+    R.frequence_of_kmer_in_sequence.restype = C.c_short
+    R.frequence_of_kmer_in_sequence.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
+    rng = np.random.default_rng(77)
+    seqs = [b"", b"A", b"ACGT", b"ACGTA", b"ACGTAC", b"AAAAAA", b"AAAAAAAAAAAAAAAAAAAA", b"ACGTN" * 6,
+            b"acgtacgtacgt", b"ACGTRYACGTACGTAAA"]
+    for L in [15, 16, 17, 20, 21, 22, 63, 100, 250, 600]:
+        seqs.append(rand_seq(rng, L))
+    for L in [40, 120, 300]:
+        seqs.append(with_n_runs(rng, rand_seq(rng, L), 0.08))
+    cases = []
+    for k in (5, 3):
+        km = R.gen_dna_kmers(k)
+        for sq in seqs:
+            counts = {}
+            for b in range(4 ** k):
+                c = R.frequence_of_kmer_in_sequence(km[b], sq, k)
+                if c:
+                    counts[str(b)] = int(c)
+            cases.append({"k": k, "seq": sq.decode("latin-1"), "counts": counts})
+    (OUT / "kmer_counts.json").write_text(json.dumps(cases))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         O.build()
-    which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets"]
+    which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
+                             "kmer"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -293,3 +324,5 @@ if __name__ == "__main__":
         config1_golden()
     if "subsets" in which:
         subset_goldens()
+    if "kmer" in which:
+        kmer_golden()

@@ -1,0 +1,164 @@
+"""Learned prefilter: k-mer features against the reference's own k-mer
+counter (golden vectors), the tcgen05 GEMM against a float64 product, and the
+network's loss and gradients against the float64 oracle (oracle/mlp_oracle.py)."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import mlp_oracle as MO
+import oracle as O
+import swgpu
+from conftest import load_golden
+from swgpu import workloads as W
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle pinned to the reference
+# ---------------------------------------------------------------------------
+def test_kmer_oracle_matches_reference_counts():
+    for case in load_golden("kmer_counts.json"):
+        k, seq = case["k"], case["seq"].encode("latin-1")
+        got = O.kmer_counts(seq, k)
+        want = np.zeros(4 ** k, dtype=np.int64)
+        for b, c in case["counts"].items():
+            want[int(b)] = c
+        assert np.array_equal(got.astype(np.int64), want), (k, seq[:30])
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.00390625, 1.01171875, -3.0e-5, 65504.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8])
+    got = MO.bf16(x)
+    # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: even mantissa (1.0) wins; 1 + 3*2^-8 rounds up to 1 + 2^-6
+    assert got[5] == 1.0 and got[6] == 1.0 + 2 ** -6
+    assert np.all(np.abs(got - x) <= np.abs(x) * 2 ** -8)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    n = 12
+    X = MO.features(rng.integers(0, 5, size=(n, 1024)))
+    params = np.concatenate([rng.normal(0, 0.05, size=MO.NPARAM)])
+    a = rng.integers(0, n, size=10)
+    b = (a + 1 + rng.integers(0, n - 1, size=10)) % n
+    d = rng.integers(0, 400, size=10)
+    lens = rng.integers(50, 300, size=n)
+    loss, g = MO.loss_grad(X, a, b, d, lens, params, emulate_bf16=False)
+    for idx in [0, 1234, MO.NPARAM - 200, 512 * 1024 + 3, 512 * 1024 + 512 + 77]:
+        h = 1e-6
+        p1 = params.copy()
+        p1[idx] += h
+        p0 = params.copy()
+        p0[idx] -= h
+        fd = (MO.loss_grad(X, a, b, d, lens, p1, False)[0] - MO.loss_grad(X, a, b, d, lens, p0, False)[0]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-5 * max(1.0, abs(fd)), (idx, fd, g[idx])
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+@pytest.mark.gpu
+def test_kmer_features_match_reference():
+    cases = load_golden("kmer_counts.json")
+    for k in (5, 3):
+        sub = [c for c in cases if c["k"] == k]
+        seqs = [c["seq"].encode("latin-1") for c in sub]
+        e = swgpu.Engine()
+        e.upload(seqs)
+        F = e.kmer_features(k)
+        e.close()
+        for i, c in enumerate(sub):
+            want = np.zeros(4 ** k)
+            for b, v in c["counts"].items():
+                want[int(b)] = v
+            tot = want.sum()
+            want = want / tot if tot else want
+            np.testing.assert_allclose(F[i], want, rtol=1e-6, atol=0, err_msg=str((k, c["seq"][:30])))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,N,K,bias,act", [(128, 128, 64, False, 0), (256, 256, 128, True, 0),
+                                            (384, 512, 1024, True, 1), (128, 256, 8192, False, 0),
+                                            (512, 1024, 256, False, 1)])
+def test_tcgen05_gemm_matches_float64(M, N, K, bias, act):
+    import torch
+    g = torch.Generator().manual_seed(M * 7 + N + K)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16)
+    bv = torch.randn(N, generator=g).float() if bias else None
+    ref = A.double() @ B.double().T
+    if bias:
+        ref = ref + bv.double()
+    if act:
+        ref = 0.5 * ref * (1 + torch.erf(ref / math.sqrt(2)))
+    Ad, Bd = A.cuda(), B.cuda()
+    bd = bv.cuda() if bias else None
+    Cd = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    st = swgpu.lib().swe_gemm_bf16(0, Ad.data_ptr(), Bd.data_ptr(), M, N, K, bd.data_ptr() if bias else None, act,
+                                   Cd.data_ptr())
+    assert st == 0
+    got = Cd.cpu().double()
+    err = (got - ref).abs().max().item()
+    assert err <= 2e-5 * math.sqrt(K) * 4 + 1e-4, err
+
+
+@pytest.fixture(scope="module")
+def small_set():
+    seqs, _ = W.config2(n=600)
+    rng = np.random.default_rng(4)
+    a = rng.integers(0, len(seqs), size=512)
+    b = (a + 1 + rng.integers(0, len(seqs) - 1, size=512)) % len(seqs)
+    return seqs, a.astype(np.int32), b.astype(np.int32)
+
+
+@pytest.mark.gpu
+def test_prefilter_gradients_match_float64_oracle(small_set):
+    """Loss and every parameter gradient of one batch, on the tensor-core path,
+    against the float64 oracle with the same bf16 roundings: relative L2 error
+    per tensor <= 1e-2 (loss <= 1e-3); against the pure float64 network <= 5e-2."""
+    seqs, a, b = small_set
+    e = swgpu.Engine()
+    e.upload(seqs)
+    d = e.score_pairs(a, b)
+    e.prefilter_init(seed=11)
+    params = e.prefilter_params()
+    loss, grad = e.prefilter_loss_grad(a, b, d)
+    e.close()
+    X = MO.features(np.stack([O.kmer_counts(s, 5) for s in seqs]))
+    lens = [len(s) for s in seqs]
+    for emulate, tol in [(True, 1e-2), (False, 5e-2)]:
+        lo, go = MO.loss_grad(X, a, b, d, lens, params.astype(np.float64), emulate_bf16=emulate)
+        assert abs(loss - lo) <= (tol / 10) * abs(lo), (emulate, loss, lo)
+        o = 0
+        for name, shape in MO.SIZES:
+            k = int(np.prod(shape))
+            gg, oo = grad[o:o + k].astype(np.float64), go[o:o + k]
+            o += k
+            if name == "b3":
+                assert np.abs(gg).max() <= 1e-6 and np.abs(oo).max() <= 1e-9
+                continue
+            rel = np.linalg.norm(gg - oo) / max(np.linalg.norm(oo), 1e-30)
+            assert rel <= tol, (emulate, name, rel)
+
+
+@pytest.mark.gpu
+def test_prefilter_training_reduces_loss(small_set):
+    seqs, _, _ = small_set
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, len(seqs), size=40000).astype(np.int32)
+    b = ((a + 1 + rng.integers(0, len(seqs) - 1, size=40000)) % len(seqs)).astype(np.int32)
+    e = swgpu.Engine()
+    e.upload(seqs)
+    d = e.score_pairs(a, b)
+    e.prefilter_init(seed=1)
+    losses = e.prefilter_train(a, b, d, epochs=6, batch_pairs=2048, lr=2e-3, seed=5)
+    emb = e.prefilter_embed()
+    pd = e.prefilter_pair_dist(a[:1000], b[:1000])
+    e.close()
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.5 * losses[0], losses
+    np.testing.assert_allclose(pd, np.linalg.norm(emb[a[:1000]] - emb[b[:1000]], axis=1), rtol=1e-4, atol=1e-5)

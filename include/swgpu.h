@@ -254,6 +254,43 @@ swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const u
 swe_status swe_prefilter_embed(swe_ctx* ctx, float* out);
 /* Embedding distances of explicit pairs. */
 swe_status swe_prefilter_pair_dist(swe_ctx* ctx, const int* a, const int* b, int64_t np, float* out);
+/* Replaces the embeddings of the uploaded sequences (n x 128) by the
+   caller's, e.g. an embedding without the network for comparison; the next
+   swe_prefilter_embed recomputes them from the network. */
+swe_status swe_prefilter_set_embeddings(swe_ctx* ctx, const float* emb);
+
+typedef struct {
+  int64_t candidates;   /* pairs passing the length bound and the embedding margin */
+  int64_t tiles_kept;   /* tiles of the 16x2 kernel that hold a candidate */
+  int64_t tiles_all;    /* tiles of the full layout */
+  double tile_cells;    /* DP cells the 16x2 kernel processed */
+  double ms_embed, ms_candidates, ms_layout, ms_score, ms_total;  /* host wall times */
+  int fallback_full;    /* 1 when there were too many candidates and every pair was scored */
+} swe_prefilter_stats;
+
+/* Margins of the prefilter by the pair's longer length L: bucket b < n-1
+   holds L < upper[b], the last bucket every longer pair (upper[n-1] unused). */
+#define SWE_MARGIN_BUCKETS 8
+typedef struct {
+  int n;
+  int upper[SWE_MARGIN_BUCKETS];
+  float margin[SWE_MARGIN_BUCKETS];
+} swe_margins;
+
+/* Prefiltered score pass for neighbourhoods up to eps: a pair is scored
+   exactly when 4*|len_a - len_b| <= floor(eps) (every distance is at least
+   that) and, with use_emb, its embedding distance is at most
+   floor(eps) / (4*max(len_a, len_b)) + margin(max(len_a, len_b)).
+   Sequences joined by candidate pairs that pass without margin are grouped
+   (connected components), each group laid out contiguously, and only the
+   tiles of the 16x2 kernel that hold a candidate pair are run; every other pair reads as the largest
+   distance (never an eps-neighbour).  Scores that are computed are exact, so
+   neighbourhoods at any eps' <= eps are a subset of the exact ones, missing
+   only pairs the prefilter skipped.  swe_score_all_pairs returns to the exact
+   pass. */
+swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* margins, int use_emb,
+                                 swe_prefilter_stats* out);
+
 /* The tensor-core GEMM alone, for tests: C[M x N] = A[M x K] * B[N x K]^T
    (+ bias, GELU when act = 1) with A, B bf16 and C fp32 DEVICE pointers;
    M and N multiples of 128, K a multiple of 64. */

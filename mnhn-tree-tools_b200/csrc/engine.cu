@@ -176,6 +176,281 @@ static DistLayout layout(const swe_ctx* ctx) {
   return L;
 }
 
+// Sorted order, packs, row blocks, tiles and every device array that depends
+// on them.  key (optional, per original index): packed-path sequences of a set
+// are ordered by (key, longer first) instead of longer first.  cand
+// (optional): only tiles holding one of these pairs (original indices) are
+// kept, and the distance matrix starts out at the largest value (no pair
+// scored means no neighbour).
+static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand) {
+  // per set: packed-path sequences in the chosen order (longest first by
+  // default), then the 32-bit-path ones
+  const int n = ctx->n, n_sets = ctx->n_sets;
+  drop_graph(ctx);
+  ctx->scored = false;
+  ctx->bits_T = LLONG_MIN;
+  ctx->bits_set = -1;
+  ctx->masked = cand != nullptr;
+  ctx->set_nfast.assign(n_sets, 0);
+  ctx->set_base.assign(n_sets + 1, 0);
+  ctx->order.assign(n, 0);
+  ctx->pos.assign(n, 0);
+  ctx->set_of.assign(n, 0);
+  ctx->exc.clear();
+  ctx->exc_pre.assign(1, 0);
+  int nfast_total = 0;
+  for (int k = 0; k < n_sets; ++k) {
+    const int f = ctx->set_first[k], nk = ctx->set_first[k + 1] - f;
+    std::vector<int> fast, slow;
+    for (int i = f; i < f + nk; ++i) (ctx->is_exc[i] ? slow : fast).push_back(i);
+    if (key)
+      std::stable_sort(fast.begin(), fast.end(), [&](int a, int b) {
+        return (*key)[a] != (*key)[b] ? (*key)[a] < (*key)[b] : ctx->len[a] > ctx->len[b];
+      });
+    else
+      std::stable_sort(fast.begin(), fast.end(), [&](int a, int b) { return ctx->len[a] > ctx->len[b]; });
+    int p = 0;
+    for (int i : fast) ctx->order[f + p++] = i;
+    for (int i : slow) ctx->order[f + p++] = i;
+    for (int q = 0; q < nk; ++q) {
+      ctx->pos[ctx->order[f + q]] = q;
+      ctx->set_of[ctx->order[f + q]] = k;
+    }
+    ctx->set_nfast[k] = (int)fast.size();
+    nfast_total += (int)fast.size();
+    ctx->set_base[k + 1] = ctx->set_base[k] + (long long)nk * nk;
+    for (int q = (int)fast.size(); q < nk; ++q) {
+      ctx->exc.push_back(f + q);
+      ctx->exc_pre.push_back(ctx->exc_pre.back() + nk);
+    }
+  }
+  ctx->nfast = nfast_total;
+
+  // packs of two neighbouring sorted sequences of one set; blocks of up to PB
+  // packs of one set, each starting on an 8-row (16-byte) boundary so a block
+  // is one bulk copy
+  const int PB = cand ? std::min(ctx->pf_packs_per_block, ctx->packs_per_block) : ctx->packs_per_block;
+  ctx->layout_pb = PB;
+  std::vector<int> pack_first, pack_off, pack_rows, block_first, block_npacks, block_rows, block_set;
+  std::vector<uint8_t> pack_pair;
+  int64_t row = 0;
+  int max_block_rows = 8;
+  for (int k = 0; k < n_sets; ++k) {
+    const int f = ctx->set_first[k], nf = ctx->set_nfast[k];
+    const int npk = (nf + 1) / 2;
+    for (int b = 0; b < npk; b += PB) {
+      row = (row + 7) & ~int64_t(7);
+      const int64_t start = row;
+      block_first.push_back((int)pack_first.size());
+      block_npacks.push_back(std::min(PB, npk - b));
+      block_set.push_back(k);
+      for (int pl = b; pl < std::min(npk, b + PB); ++pl) {
+        const int g = f + 2 * pl;
+        const bool pair = 2 * pl + 1 < nf;
+        // an even row count: the 16x2 kernel processes two rows per step
+        const int R = (std::max(ctx->len[ctx->order[g]], pair ? ctx->len[ctx->order[g + 1]] : 0) + 1) & ~1;
+        pack_first.push_back(g);
+        pack_pair.push_back(pair ? 1 : 0);
+        pack_off.push_back((int)row);
+        pack_rows.push_back(R);
+        row += R;
+      }
+      block_rows.push_back((int)(row - start));
+      max_block_rows = std::max(max_block_rows, (int)((row - start + 7) & ~int64_t(7)));
+      if (row > INT_MAX / 2) return fail(ctx, SWE_ERR_INVALID, "dataset too large for one upload");
+    }
+  }
+  row = (row + 7) & ~int64_t(7);
+  const int npacks = (int)pack_first.size();
+  ctx->npacks = npacks;
+  ctx->nblocks = (int)block_first.size();
+  ctx->max_block_rows = max_block_rows;
+
+  // tiles: blocks of column sequences against the row blocks of the same set
+  // that hold a later sequence.  A column block's lane split follows its
+  // longest sequence.  With candidate pairs, only the tiles holding one are kept.
+  const int cta_warps = ctx->threads / 32;
+  ctx->tiles.clear();
+  std::vector<double> cost;
+  double tile_cells = 0;
+  long long tiles_all = 0;
+  for (int q0 = 0, k = 0; k < n_sets; ++k) {
+    const int f = ctx->set_first[k], nf = ctx->set_nfast[k];
+    int q1 = q0;
+    while (q1 < ctx->nblocks && block_set[q1] == k) ++q1;
+    std::vector<int> cb_of(nf, 0);  // position -> column block index (within the set)
+    struct ColBlock {
+      int b0, nb, W, lpb;
+    };
+    std::vector<ColBlock> cbs;
+    for (int b0 = 0; b0 < nf;) {
+      int lpb = 8, nb = 0, L = 0;
+      for (int it = 0; it < 3; ++it) {  // the split depends on the block's longest sequence
+        nb = std::min(nf - b0, cta_warps * (32 / lpb));
+        L = 0;
+        for (int x = b0; x < b0 + nb; ++x) L = std::max(L, ctx->len[ctx->order[f + x]]);
+        const int need = L <= 8 * FAST_MAX_W ? 8 : (L <= 16 * FAST_MAX_W ? 16 : 32);
+        if (need <= lpb) break;
+        lpb = need;
+      }
+      for (int x = b0; x < b0 + nb; ++x) cb_of[x] = (int)cbs.size();
+      cbs.push_back(ColBlock{b0, nb, (L + lpb - 1) / lpb, lpb});
+      b0 += nb;
+    }
+    std::vector<uint8_t> mark;
+    if (cand) {
+      mark.assign(cbs.size() * (size_t)std::max(q1 - q0, 1), 0);
+      const int lo = f, hi = ctx->set_first[k + 1], nq = q1 - q0;
+      auto mark_range = [&](std::vector<uint8_t>* mk, size_t c0, size_t c1) {
+        for (size_t c = c0; c < c1; ++c) {
+          const int2 pr = (*cand)[c];
+          if (pr.x < lo || pr.x >= hi || pr.y < lo || pr.y >= hi) continue;
+          int px = ctx->pos[pr.x], py = ctx->pos[pr.y];
+          if (px >= nf || py >= nf || px == py) continue;  // 32-bit-path pairs are all scored anyway
+          if (px > py) std::swap(px, py);
+          const int q = (py / 2) / PB;  // row block of the later sequence, within the set
+          (*mk)[(size_t)cb_of[px] * nq + q] = 1;
+        }
+      };
+      // threads mark private copies over slices of the candidates, then OR them
+      const size_t C = cand->size();
+      const int T = (int)std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 1 + C / 200000);
+      std::vector<std::vector<uint8_t>> priv(T - 1, std::vector<uint8_t>(mark.size(), 0));
+      std::vector<std::thread> th;
+      for (int t = 1; t < T; ++t) th.emplace_back(mark_range, &priv[t - 1], C * t / T, C * (t + 1) / T);
+      mark_range(&mark, 0, C / T);
+      for (auto& x : th) x.join();
+      for (const auto& pm : priv)
+        for (size_t i = 0; i < mark.size(); ++i) mark[i] |= pm[i];
+    }
+    for (size_t c = 0; c < cbs.size(); ++c) {
+      const ColBlock& cb = cbs[c];
+      for (int q = q0; q < q1; ++q) {
+        const int lastpk = block_first[q] + block_npacks[q] - 1;
+        const int maxA = pack_first[lastpk] - f + (pack_pair[lastpk] ? 1 : 0);
+        if (maxA > cb.b0) {
+          ++tiles_all;
+          if (cand && !mark[c * (q1 - q0) + (q - q0)]) continue;
+          ctx->tiles.push_back(FastTile{f + cb.b0, cb.nb, q, cb.W | (cb.lpb << 8), k});
+          const double cc = (double)cb.nb * cb.lpb * cb.W * block_rows[q];
+          cost.push_back(cc);
+          tile_cells += 2.0 * cc;
+        }
+      }
+    }
+    q0 = q1;
+  }
+  ctx->tiles_all = tiles_all;
+  {
+    std::vector<int> idx(ctx->tiles.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<FastTile> sorted(ctx->tiles.size());
+    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]];
+    ctx->tiles.swap(sorted);
+  }
+  ctx->max_cols = cta_warps * 4;
+  ctx->smem = fast_smem_bytes(ctx->max_block_rows, ctx->max_cols, PB);
+
+  // statistics
+  {
+    double cells = 0;
+    int64_t pairs = 0;
+    for (int k = 0; k < n_sets; ++k) {
+      double sum = 0, sq = 0;
+      for (int i = ctx->set_first[k]; i < ctx->set_first[k + 1]; ++i) {
+        sum += ctx->len[i];
+        sq += (double)ctx->len[i] * ctx->len[i];
+      }
+      cells += (sum * sum - sq) / 2.0;
+      const int64_t nk = ctx->set_first[k + 1] - ctx->set_first[k];
+      pairs += nk * (nk - 1) / 2;
+    }
+    ctx->stats.cells = cells;
+    ctx->stats.tile_cells = tile_cells;
+    ctx->stats.n_sequences = n;
+    ctx->stats.n_fast = nfast_total;
+    ctx->stats.n_exceptional = (int64_t)ctx->exc.size();
+    ctx->stats.unique_pairs = pairs;
+    ctx->stats.n_tiles = (int64_t)ctx->tiles.size();
+  }
+
+  // device copies
+  std::vector<int> set_n(n_sets);
+  for (int k = 0; k < n_sets; ++k) set_n[k] = ctx->set_first[k + 1] - ctx->set_first[k];
+  cudaStream_t st = ctx->st;
+  auto up = [&](auto& buf, const auto& vec) -> cudaError_t {
+    cudaError_t e = buf.alloc(std::max<size_t>(vec.size(), 1));
+    if (e == cudaSuccess && !vec.empty())
+      e = cpy(ctx, buf.p, vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice, st);
+    return e;
+  };
+  CK(up(ctx->d_order, ctx->order));
+  CK(up(ctx->d_pos, ctx->pos));
+  CK(up(ctx->d_setof, ctx->set_of));
+  CK(up(ctx->d_set_first, ctx->set_first));
+  CK(up(ctx->d_set_n, set_n));
+  CK(up(ctx->d_set_nfast, ctx->set_nfast));
+  CK(up(ctx->d_set_base, ctx->set_base));
+  CK(up(ctx->d_exc, ctx->exc));
+  CK(up(ctx->d_exc_pre, ctx->exc_pre));
+  CK(up(ctx->d_pack_first, pack_first));
+  CK(up(ctx->d_pack_pair, pack_pair));
+  CK(up(ctx->d_pack_off, pack_off));
+  CK(up(ctx->d_pack_rows, pack_rows));
+  CK(up(ctx->d_block_first, block_first));
+  CK(up(ctx->d_block_npacks, block_npacks));
+  CK(up(ctx->d_tiles, ctx->tiles));
+  CK(ctx->d_sel.alloc(std::max<int64_t>(row, 8)));
+  // rows outside the packs (block alignment) hold the pad selector 0xF7F7
+  CK(cudaMemsetAsync(ctx->d_sel.p, 0xF7, sizeof(uint16_t) * std::max<int64_t>(row, 8), st));
+  ctx->stats.kernel_launches += 1;
+  CK(launch_build_sel(ctx->d_codes.p, ctx->d_off.p, ctx->d_len.p, ctx->d_order.p, ctx->d_pack_first.p,
+                      ctx->d_pack_pair.p, ctx->d_pack_off.p, ctx->d_pack_rows.p, npacks, ctx->d_sel.p, st));
+
+  // distance storage: one sorted n_s x n_s matrix per set
+  ctx->dist_bytes = ctx->max_len <= 16383 ? 2 : 4;
+  ctx->stats.dist_bytes = ctx->dist_bytes;
+  const size_t nn = (size_t)ctx->set_base[n_sets];
+  // 16 bytes of slack after the last row: the threshold pass copies 16-byte
+  // aligned windows around each row
+  if (ctx->dist_bytes == 2) {
+    ctx->d_D32.release();
+    if (ctx->d_D16.n < nn + 8 || ctx->d_D16.n > 2 * (nn + 8)) ctx->d_D16.release();
+    CK(ctx->d_D16.alloc(nn + 8));
+  } else {
+    ctx->d_D16.release();
+    if (ctx->d_D32.n < nn + 4 || ctx->d_D32.n > 2 * (nn + 4)) ctx->d_D32.release();
+    CK(ctx->d_D32.alloc(nn + 4));
+  }
+
+  // 32-bit path resources: rerun queue (only when the guard can fire) and
+  // per-warp boundary columns for sequences longer than one 512-column chunk
+  ctx->rerun_possible = (long long)ctx->sat_limit <= 4LL * ctx->max_fast_len + 8;
+  double tile_pairs = 0;
+  for (const auto& t : ctx->tiles) tile_pairs += 2.0 * t.nb * PB;
+  ctx->rerun_cap = ctx->rerun_possible ? (unsigned)std::min(tile_pairs, (double)(1u << 26)) : 1024u;
+  CK(ctx->d_rerun.alloc(std::max(ctx->rerun_cap, 1u)));
+  ctx->gen_grid = ctx->num_sms * 4;
+  ctx->scratch_stride = 0;
+  if (ctx->max_len > GEN_CHUNK) {
+    ctx->scratch_stride = (long long)ctx->max_len + 1;
+    const long long warps = (long long)ctx->gen_grid * 8;
+    const long long budget = 1LL << 31;  // bytes
+    if (warps * ctx->scratch_stride * 4 > budget)
+      ctx->gen_grid = (int)std::max<long long>(ctx->num_sms, budget / (ctx->scratch_stride * 4 * 8));
+    CK(ctx->d_scratch.alloc((size_t)ctx->gen_grid * 8 * ctx->scratch_stride));
+  }
+
+  // launch shapes
+  CK(fast_set_smem_limit(ctx->smem));
+  const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
+  ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
+  CK(cudaStreamSynchronize(st));
+  return SWE_OK;
+}
+
+
 // Uploads n sequences forming n_sets independent sets: set k is the original
 // indices [set_first[k], set_first[k+1]).  Pairs are scored only inside a set.
 static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n,
@@ -234,144 +509,8 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   }
   ctx->max_fast_len = max_fast;
 
-  // per set: packed-path sequences longest first, then the 32-bit-path ones
   ctx->n_sets = n_sets;
   ctx->set_first.assign(set_first_in, set_first_in + n_sets + 1);
-  ctx->set_nfast.assign(n_sets, 0);
-  ctx->set_base.assign(n_sets + 1, 0);
-  ctx->order.assign(n, 0);
-  ctx->pos.assign(n, 0);
-  ctx->set_of.assign(n, 0);
-  ctx->exc.clear();
-  ctx->exc_pre.assign(1, 0);
-  int nfast_total = 0;
-  for (int k = 0; k < n_sets; ++k) {
-    const int f = ctx->set_first[k], nk = ctx->set_first[k + 1] - f;
-    std::vector<int> fast, slow;
-    for (int i = f; i < f + nk; ++i) (ctx->is_exc[i] ? slow : fast).push_back(i);
-    std::stable_sort(fast.begin(), fast.end(), [&](int a, int b) { return ctx->len[a] > ctx->len[b]; });
-    int p = 0;
-    for (int i : fast) ctx->order[f + p++] = i;
-    for (int i : slow) ctx->order[f + p++] = i;
-    for (int q = 0; q < nk; ++q) {
-      ctx->pos[ctx->order[f + q]] = q;
-      ctx->set_of[ctx->order[f + q]] = k;
-    }
-    ctx->set_nfast[k] = (int)fast.size();
-    nfast_total += (int)fast.size();
-    ctx->set_base[k + 1] = ctx->set_base[k] + (long long)nk * nk;
-    for (int q = (int)fast.size(); q < nk; ++q) {
-      ctx->exc.push_back(f + q);
-      ctx->exc_pre.push_back(ctx->exc_pre.back() + nk);
-    }
-  }
-  ctx->nfast = nfast_total;
-
-  // packs of two neighbouring sorted sequences of one set; blocks of up to PB
-  // packs of one set, each starting on an 8-row (16-byte) boundary so a block
-  // is one bulk copy
-  const int PB = ctx->packs_per_block;
-  std::vector<int> pack_first, pack_off, pack_rows, block_first, block_npacks, block_rows, block_set;
-  std::vector<uint8_t> pack_pair;
-  int64_t row = 0;
-  int max_block_rows = 8;
-  for (int k = 0; k < n_sets; ++k) {
-    const int f = ctx->set_first[k], nf = ctx->set_nfast[k];
-    const int npk = (nf + 1) / 2;
-    for (int b = 0; b < npk; b += PB) {
-      row = (row + 7) & ~int64_t(7);
-      const int64_t start = row;
-      block_first.push_back((int)pack_first.size());
-      block_npacks.push_back(std::min(PB, npk - b));
-      block_set.push_back(k);
-      for (int pl = b; pl < std::min(npk, b + PB); ++pl) {
-        const int g = f + 2 * pl;
-        const bool pair = 2 * pl + 1 < nf;
-        // an even row count: the 16x2 kernel processes two rows per step
-        const int R = (std::max(ctx->len[ctx->order[g]], pair ? ctx->len[ctx->order[g + 1]] : 0) + 1) & ~1;
-        pack_first.push_back(g);
-        pack_pair.push_back(pair ? 1 : 0);
-        pack_off.push_back((int)row);
-        pack_rows.push_back(R);
-        row += R;
-      }
-      block_rows.push_back((int)(row - start));
-      max_block_rows = std::max(max_block_rows, (int)((row - start + 7) & ~int64_t(7)));
-      if (row > INT_MAX / 2) return fail(ctx, SWE_ERR_INVALID, "dataset too large for one upload");
-    }
-  }
-  row = (row + 7) & ~int64_t(7);
-  const int npacks = (int)pack_first.size();
-  ctx->npacks = npacks;
-  ctx->nblocks = (int)block_first.size();
-  ctx->max_block_rows = max_block_rows;
-
-  // tiles: blocks of column sequences (longest first) against the row blocks
-  // of the same set that hold a later sequence
-  const int cta_warps = ctx->threads / 32;
-  ctx->tiles.clear();
-  std::vector<double> cost;
-  double tile_cells = 0;
-  for (int q0 = 0, k = 0; k < n_sets; ++k) {
-    const int f = ctx->set_first[k], nf = ctx->set_nfast[k];
-    int q1 = q0;
-    while (q1 < ctx->nblocks && block_set[q1] == k) ++q1;
-    for (int b0 = 0; b0 < nf;) {
-      const int L = ctx->len[ctx->order[f + b0]];
-      const int lpb = L <= 8 * FAST_MAX_W ? 8 : (L <= 16 * FAST_MAX_W ? 16 : 32);
-      const int W = (L + lpb - 1) / lpb;
-      const int nb = std::min(nf - b0, cta_warps * (32 / lpb));
-      for (int q = q0; q < q1; ++q) {
-        const int lastpk = block_first[q] + block_npacks[q] - 1;
-        const int maxA = pack_first[lastpk] - f + (pack_pair[lastpk] ? 1 : 0);
-        if (maxA > b0) {
-          ctx->tiles.push_back(FastTile{f + b0, nb, q, W | (lpb << 8), k});
-          const double c = (double)nb * lpb * W * block_rows[q];
-          cost.push_back(c);
-          tile_cells += 2.0 * c;
-        }
-      }
-      b0 += nb;
-    }
-    q0 = q1;
-  }
-  {
-    std::vector<int> idx(ctx->tiles.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    std::vector<FastTile> sorted(ctx->tiles.size());
-    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]];
-    ctx->tiles.swap(sorted);
-  }
-  ctx->max_cols = cta_warps * 4;
-  ctx->smem = fast_smem_bytes(ctx->max_block_rows, ctx->max_cols, PB);
-
-  // statistics
-  {
-    double cells = 0;
-    int64_t pairs = 0;
-    for (int k = 0; k < n_sets; ++k) {
-      double sum = 0, sq = 0;
-      for (int i = ctx->set_first[k]; i < ctx->set_first[k + 1]; ++i) {
-        sum += ctx->len[i];
-        sq += (double)ctx->len[i] * ctx->len[i];
-      }
-      cells += (sum * sum - sq) / 2.0;
-      const int64_t nk = ctx->set_first[k + 1] - ctx->set_first[k];
-      pairs += nk * (nk - 1) / 2;
-    }
-    ctx->stats.cells = cells;
-    ctx->stats.tile_cells = tile_cells;
-    ctx->stats.n_sequences = n;
-    ctx->stats.n_fast = nfast_total;
-    ctx->stats.n_exceptional = (int64_t)ctx->exc.size();
-    ctx->stats.unique_pairs = pairs;
-    ctx->stats.n_tiles = (int64_t)ctx->tiles.size();
-  }
-
-  // device copies
-  std::vector<int> set_n(n_sets);
-  for (int k = 0; k < n_sets; ++k) set_n[k] = ctx->set_first[k + 1] - ctx->set_first[k];
   cudaStream_t st = ctx->st;
   auto up = [&](auto& buf, const auto& vec) -> cudaError_t {
     cudaError_t e = buf.alloc(std::max<size_t>(vec.size(), 1));
@@ -383,64 +522,7 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   CK(up(ctx->d_first, ctx->first_code));
   CK(up(ctx->d_off, ctx->off));
   CK(up(ctx->d_len, ctx->len));
-  CK(up(ctx->d_order, ctx->order));
-  CK(up(ctx->d_pos, ctx->pos));
-  CK(up(ctx->d_setof, ctx->set_of));
-  CK(up(ctx->d_set_first, ctx->set_first));
-  CK(up(ctx->d_set_n, set_n));
-  CK(up(ctx->d_set_nfast, ctx->set_nfast));
-  CK(up(ctx->d_set_base, ctx->set_base));
-  CK(up(ctx->d_exc, ctx->exc));
-  CK(up(ctx->d_exc_pre, ctx->exc_pre));
-  CK(up(ctx->d_pack_first, pack_first));
-  CK(up(ctx->d_pack_pair, pack_pair));
-  CK(up(ctx->d_pack_off, pack_off));
-  CK(up(ctx->d_pack_rows, pack_rows));
-  CK(up(ctx->d_block_first, block_first));
-  CK(up(ctx->d_block_npacks, block_npacks));
-  CK(up(ctx->d_tiles, ctx->tiles));
-  CK(ctx->d_sel.alloc(std::max<int64_t>(row, 8)));
-  // rows outside the packs (block alignment) hold the pad selector 0xF7F7
-  CK(cudaMemsetAsync(ctx->d_sel.p, 0xF7, sizeof(uint16_t) * std::max<int64_t>(row, 8), st));
-  ctx->stats.kernel_launches += 1;
-  CK(launch_build_sel(ctx->d_codes.p, ctx->d_off.p, ctx->d_len.p, ctx->d_order.p, ctx->d_pack_first.p,
-                      ctx->d_pack_pair.p, ctx->d_pack_off.p, ctx->d_pack_rows.p, npacks, ctx->d_sel.p, st));
-
-  // distance storage: one sorted n_s x n_s matrix per set
-  ctx->dist_bytes = max_len <= 16383 ? 2 : 4;
-  ctx->stats.dist_bytes = ctx->dist_bytes;
-  const size_t nn = (size_t)ctx->set_base[n_sets];
-  ctx->d_D16.release();
-  ctx->d_D32.release();
-  // 16 bytes of slack after the last row: the threshold pass copies 16-byte
-  // aligned windows around each row
-  if (ctx->dist_bytes == 2) CK(ctx->d_D16.alloc(nn + 8));
-  else CK(ctx->d_D32.alloc(nn + 4));
-
-  // 32-bit path resources: rerun queue (only when the guard can fire) and
-  // per-warp boundary columns for sequences longer than one 512-column chunk
-  ctx->rerun_possible = (long long)ctx->sat_limit <= 4LL * max_fast + 8;
-  double tile_pairs = 0;
-  for (const auto& t : ctx->tiles) tile_pairs += 2.0 * t.nb * PB;
-  ctx->rerun_cap = ctx->rerun_possible ? (unsigned)std::min(tile_pairs, (double)(1u << 26)) : 1024u;
-  CK(ctx->d_rerun.alloc(std::max(ctx->rerun_cap, 1u)));
-  ctx->gen_grid = ctx->num_sms * 4;
-  ctx->scratch_stride = 0;
-  if (max_len > GEN_CHUNK) {
-    ctx->scratch_stride = (long long)max_len + 1;
-    const long long warps = (long long)ctx->gen_grid * 8;
-    const long long budget = 1LL << 31;  // bytes
-    if (warps * ctx->scratch_stride * 4 > budget)
-      ctx->gen_grid = (int)std::max<long long>(ctx->num_sms, budget / (ctx->scratch_stride * 4 * 8));
-    CK(ctx->d_scratch.alloc((size_t)ctx->gen_grid * 8 * ctx->scratch_stride));
-  }
-
-  // launch shapes
-  CK(fast_set_smem_limit(ctx->smem));
-  const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
-  ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
-  CK(cudaStreamSynchronize(st));
-  return SWE_OK;
+  return build_layout(ctx, nullptr, nullptr);
 }
 
 swe_status swe_upload(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n) {
@@ -460,6 +542,11 @@ static swe_status build_score_graph(swe_ctx* ctx) {
   const DistLayout L = layout(ctx);
   CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemsetAsync(ctx->d_ctr.p, 0, 4 * sizeof(unsigned), st);
+  if (e == cudaSuccess && ctx->masked) {  // pairs outside the candidate tiles read as the largest value
+    const size_t nn = (size_t)ctx->set_base[ctx->n_sets];
+    e = ctx->d_D16.p ? cudaMemsetAsync(ctx->d_D16.p, 0xFF, nn * sizeof(uint16_t), st)
+                     : cudaMemsetAsync(ctx->d_D32.p, 0xFF, nn * sizeof(uint32_t), st);
+  }
   ctx->graph_kernels = 1;
   if (e == cudaSuccess) e = launch_diag(L, ctx->n, st);
   // inside a capture only an external record becomes a real event node
@@ -477,7 +564,7 @@ static swe_status build_score_graph(swe_ctx* ctx) {
     p.pack_rows = ctx->d_pack_rows.p;
     p.block_first = ctx->d_block_first.p;
     p.block_npacks = ctx->d_block_npacks.p;
-    p.max_packs_per_block = ctx->packs_per_block;
+    p.max_packs_per_block = ctx->layout_pb;
     p.tiles = ctx->d_tiles.p;
     p.ntiles = (int)ctx->tiles.size();
     p.tile_counter = ctx->d_ctr.p;
@@ -536,6 +623,20 @@ static swe_status build_score_graph(swe_ctx* ctx) {
 swe_status swe_score_all_pairs(swe_ctx* ctx) {
   if (!ctx) return SWE_ERR_INVALID;
   if (swe_status s = select_device(ctx)) return s;
+  if (ctx->masked)  // back from a prefiltered pass: every tile again, longest first
+    if (swe_status s = build_layout(ctx, nullptr, nullptr)) return s;
+  return score_pass(ctx);
+}
+
+}  // extern "C"
+
+namespace swgpu {
+
+swe_status engine_relayout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand) {
+  return build_layout(ctx, key, cand);
+}
+
+swe_status score_pass(swe_ctx* ctx) {
   ctx->bits_T = LLONG_MIN;
   ctx->bits_set = -1;
   if (ctx->n == 0) {
@@ -561,6 +662,10 @@ swe_status swe_score_all_pairs(swe_ctx* ctx) {
   ctx->scored = true;
   return SWE_OK;
 }
+
+}  // namespace swgpu
+
+extern "C" {
 
 static const uint16_t* set_D16(const swe_ctx* ctx, int s) {
   return ctx->d_D16.p ? ctx->d_D16.p + ctx->set_base[s] : nullptr;

@@ -71,7 +71,9 @@ struct swe_ctx {
   cudaStream_t st = nullptr;
   int num_sms = 148;
   int sat_limit = 32000;
-  int packs_per_block = 32;
+  int packs_per_block = 32;     // row-sequence pairs per tile of the full layout
+  int pf_packs_per_block = 8;   // the same for candidate-tile layouts (sparser work, finer tiles)
+  int layout_pb = 32;           // the value the current layout was built with
   int threads = 256;
   int inject_timeout = 0;
   int threshold_path = 0;
@@ -95,6 +97,8 @@ struct swe_ctx {
   size_t smem = 0;
   int fast_grid = 0;
   std::vector<swgpu::FastTile> tiles;
+  long long tiles_all = 0;  // tiles of the full layout (before a candidate mask)
+  bool masked = false;      // only candidate tiles are scored; other pairs read as the largest value
 
   // sets (independent datasets in one upload) and the sorted layout
   int n_sets = 0;
@@ -188,6 +192,11 @@ swe_status check_kernel_status(swe_ctx* ctx, unsigned status);
 // Stream-ordered copy that also counts the bytes crossing PCIe.
 cudaError_t cpy(swe_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st);
 swe_status select_device(swe_ctx* ctx);
+// Rebuilds the sorted layout (see build_layout in engine.cu) and runs one
+// score pass over the current layout.
+swe_status engine_relayout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand);
+swe_status score_pass(swe_ctx* ctx);
+long long eps_threshold(float eps);
 
 }  // namespace swgpu
 

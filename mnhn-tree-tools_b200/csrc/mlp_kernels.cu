@@ -451,7 +451,7 @@ constexpr int C_T = 64;
 template <int D>
 __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict__ emb, const int* __restrict__ orig,
                                                          const int* __restrict__ len, int first, int n, long long T,
-                                                         float margin, int use_emb, int2* __restrict__ pairs,
+                                                         MarginTable margins, int use_emb, int2* __restrict__ pairs,
                                                          unsigned long long cap, unsigned long long* count) {
   extern __shared__ float c_smem[];
   float (*ei)[D + 1] = reinterpret_cast<float (*)[D + 1]>(c_smem);
@@ -514,13 +514,22 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
         const int xi = ty * 4 + q, xj = tx * 4 + r;
         const int pi = i0 + xi, pj = j0 + xj;
         bool cand = pi < n && pj < n && pi < pj;
+        bool strong = false;
         if (cand) {
           const int la = li[xi], lb = lj[xj];
           const int mx = la > lb ? la : lb, mn = la > lb ? lb : la;
           cand = 4LL * (mx - mn) <= T;
           if (cand && use_emb) {
-            const float thr = (float)T / (4.0f * (float)(mx > 0 ? mx : 1)) + margin;
+            float m = margins.m[margins.n - 1];
+            for (int b = 0; b < margins.n - 1; ++b)
+              if (mx < margins.upper[b]) {
+                m = margins.m[b];
+                break;
+              }
+            const float thr0 = (float)T / (4.0f * (float)(mx > 0 ? mx : 1));
+            const float thr = thr0 + m;
             cand = thr >= 0.f && acc[q][r] <= thr * thr;
+            strong = cand && acc[q][r] <= thr0 * thr0;
           }
         }
         const unsigned bal = __ballot_sync(0xFFFFFFFFu, cand);
@@ -530,7 +539,7 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
           base = __shfl_sync(0xFFFFFFFFu, base, 0);
           if (cand) {
             const unsigned long long at = base + __popc(bal & ((1u << lane) - 1u));
-            if (at < cap) pairs[at] = make_int2(oi[xi], oj[xj]);
+            if (at < cap) pairs[at] = make_int2(oi[xi] | (strong ? (int)0x80000000u : 0), oj[xj]);
           }
         }
       }
@@ -538,8 +547,9 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
 }
 
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
-                              long long T, float margin, int use_emb, int2* pairs, unsigned long long cap,
-                              unsigned long long* count, cudaStream_t st) {
+                              long long T, const MarginTable& margins, int use_emb, int2* pairs,
+                              unsigned long long cap, unsigned long long* count, cudaStream_t st) {
+  if (margins.n < 1 || margins.n > MARGIN_BUCKETS) return cudaErrorInvalidValue;
   if (n <= 1) return cudaSuccess;
   if (D != 128) return cudaErrorInvalidValue;
   const long long nt = (n + C_T - 1) / C_T;
@@ -550,7 +560,8 @@ cudaError_t launch_candidates(const float* emb, int D, const int* orig, const in
     cudaError_t e = cudaFuncSetAttribute(candidates_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  candidates_kernel<128><<<grid, 256, smem, st>>>(emb, orig, len, first, n, T, margin, use_emb, pairs, cap, count);
+  candidates_kernel<128><<<grid, 256, smem, st>>>(emb, orig, len, first, n, T, margins, use_emb, pairs, cap,
+                                                  count);
   return cudaGetLastError();
 }
 

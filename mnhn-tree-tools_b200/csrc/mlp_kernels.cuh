@@ -71,14 +71,25 @@ cudaError_t launch_publish(const float* W, int R, int C, __nv_bfloat16* Wb, __nv
 // ---------------------------------------------------------------------------
 // candidates
 // ---------------------------------------------------------------------------
+// Margins by the pair's longer length: bucket b (b < n-1) holds max lengths
+// below upper[b], the last bucket everything else.
+constexpr int MARGIN_BUCKETS = 8;
+struct MarginTable {
+  int n;
+  int upper[MARGIN_BUCKETS];
+  float m[MARGIN_BUCKETS];
+};
+
 // For every pair i < j of one set (global sorted range [first, first+n)):
 // candidate when 4*|len_i - len_j| <= T (a bound every exact distance obeys:
-// d >= 4*(max - min)) and emb_dist(i, j) <= T / (4*max(len_i, len_j)) + margin.
-// Candidates go to pairs[] (original indices, up to cap; count in *count).
-// Embeddings are per original index, D floats each.
+// d >= 4*(max - min)) and emb_dist(i, j) <= T / (4*max(len_i, len_j)) +
+// margin(max).  Candidates go to pairs[] (original indices, up to cap; count in
+// *count); bit 31 of .x flags a "strong" pair, one whose embedding distance is
+// within the threshold without any margin.  Embeddings are per original
+// index, D floats each.  use_emb = 0: the length bound alone.
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
-                              long long T, float margin, int use_emb, int2* pairs, unsigned long long cap,
-                              unsigned long long* count, cudaStream_t st);
+                              long long T, const MarginTable& margins, int use_emb, int2* pairs,
+                              unsigned long long cap, unsigned long long* count, cudaStream_t st);
 // Embedding distances of explicit pairs (original indices).
 cudaError_t launch_pair_dist(const float* emb, int D, const int* a, const int* b, long long np, float* out,
                              cudaStream_t st);

@@ -8,6 +8,7 @@
 //
 // No counterpart in the reference; the features follow kmers.c:157-241.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -37,6 +38,11 @@ struct PrefilterState {
   // features and embeddings of the current upload
   DevBuf<float> X, emb;
   int feat_gen = -1, emb_gen = -1;
+  bool emb_external = false;  // embeddings given by the caller (swe_prefilter_set_embeddings)
+
+  // candidate pairs of the last prefiltered pass
+  DevBuf<int2> cand;
+  DevBuf<unsigned long long> cand_count;
 
   // batch buffers (M rows)
   int M = 0;
@@ -362,7 +368,7 @@ swe_status swe_prefilter_embed(swe_ctx* ctx, float* out) {
   if (swe_status s = pf_need(ctx, true)) return s;
   PS* pf = ctx->pf;
   const int n = ctx->n;
-  if (pf->emb_gen != ctx->upload_gen && n > 0) {
+  if ((pf->emb_gen != ctx->upload_gen || pf->emb_external) && n > 0) {
     if (swe_status s = ensure_features(ctx)) return s;
     const int chunk = std::min(16384, (n + 127) / 128 * 128);
     if (swe_status s = ensure_batch(ctx, chunk)) return s;
@@ -381,6 +387,7 @@ swe_status swe_prefilter_embed(swe_ctx* ctx, float* out) {
     }
     if (swe_status s = check_status(ctx)) return s;
     pf->emb_gen = ctx->upload_gen;
+    pf->emb_external = false;
   }
   if (out && n > 0) CK(cpy(ctx, out, pf->emb.p, sizeof(float) * (size_t)n * PS::D3, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
@@ -403,6 +410,132 @@ swe_status swe_prefilter_pair_dist(swe_ctx* ctx, const int* a, const int* b, int
   CK(launch_pair_dist(ctx->pf->emb.p, PS::D3, da.p, db.p, np, dout.p, ctx->st));
   CK(cpy(ctx, out, dout.p, sizeof(float) * np, cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
+  return SWE_OK;
+}
+
+swe_status swe_prefilter_set_embeddings(swe_ctx* ctx, const float* emb) {
+  if (!ctx || (!emb && ctx->n > 0)) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  if (swe_status s = pf_need(ctx, false)) return s;
+  PS* pf = ctx->pf;
+  CK(pf->emb.alloc((size_t)std::max(ctx->n, 1) * PS::D3));
+  if (ctx->n > 0)
+    CK(cpy(ctx, pf->emb.p, emb, sizeof(float) * (size_t)ctx->n * PS::D3, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  pf->emb_gen = ctx->upload_gen;
+  pf->emb_external = true;
+  return SWE_OK;
+}
+
+swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* margins, int use_emb,
+                                 swe_prefilter_stats* out) {
+  if (!ctx || (use_emb && !margins)) return SWE_ERR_INVALID;
+  MarginTable mt{};
+  mt.n = 1;
+  if (margins) {
+    if (margins->n < 1 || margins->n > SWE_MARGIN_BUCKETS) return fail(ctx, SWE_ERR_INVALID, "1..8 margin buckets");
+    mt.n = margins->n;
+    for (int b = 0; b < mt.n; ++b) {
+      mt.upper[b] = margins->upper[b];
+      mt.m[b] = margins->margin[b];
+      if (b > 0 && b < mt.n - 1 && mt.upper[b] <= mt.upper[b - 1])
+        return fail(ctx, SWE_ERR_INVALID, "margin bucket bounds must increase");
+    }
+  }
+  if (swe_status s = select_device(ctx)) return s;
+  if (swe_status s = pf_need(ctx, false)) return s;
+  PS* pf = ctx->pf;
+  swe_prefilter_stats st{};
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
+  const auto t0 = clk::now();
+  if (use_emb && !(pf->emb_external && pf->emb_gen == ctx->upload_gen)) {
+    if (!pf->init) return fail(ctx, SWE_ERR_STATE, "prefilter not initialised");
+    if (swe_status s = swe_prefilter_embed(ctx, nullptr)) return s;
+  }
+  st.ms_embed = ms_since(t0);
+  const long long T = eps_threshold(eps);
+  // candidate pairs of every set
+  const auto t1 = clk::now();
+  const unsigned long long cap = 1ull << 25;
+  CK(pf->cand.alloc(cap));
+  CK(pf->cand_count.alloc(1));
+  CK(cudaMemsetAsync(pf->cand_count.p, 0, sizeof(unsigned long long), ctx->st));
+  if (T >= 0 && ctx->n > 1) {
+    for (int k = 0; k < ctx->n_sets; ++k) {
+      const int f = ctx->set_first[k], nk = ctx->set_first[k + 1] - f;
+      if (nk < 2) continue;
+      ctx->stats.kernel_launches += 1;
+      CK(launch_candidates(use_emb ? pf->emb.p : nullptr, PS::D3, ctx->d_order.p, ctx->d_len.p, f, nk, T, mt,
+                           use_emb, pf->cand.p, cap, pf->cand_count.p, ctx->st));
+    }
+  }
+  unsigned long long count = 0;
+  CK(cpy(ctx, &count, pf->cand_count.p, sizeof(count), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  st.candidates = (int64_t)count;
+  std::vector<int2> cand;
+  if (count <= cap) {
+    cand.resize(count);
+    if (count) CK(cpy(ctx, cand.data(), pf->cand.p, sizeof(int2) * count, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
+  st.ms_candidates = ms_since(t1);
+  // layout: candidate components contiguous (longer first inside each), only candidate tiles
+  const auto t2 = clk::now();
+  if (count > cap) {
+    st.fallback_full = 1;
+    if (swe_status s = engine_relayout(ctx, nullptr, nullptr)) return s;
+  } else {
+    // groups: connected components of the strong candidate pairs (embedding
+    // distance within the threshold without margin), each laid out together,
+    // longer first, so that the candidate pairs of a group fall into few tiles
+    const int n = ctx->n;
+    std::vector<int> parent(n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) {
+      while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+      }
+      return x;
+    };
+    for (int2& pr : cand) {
+      const bool strong = pr.x < 0;
+      pr.x &= 0x7FFFFFFF;
+      if (!strong) continue;
+      const int x = find(pr.x), y = find(pr.y);
+      if (x != y) parent[std::max(x, y)] = std::min(x, y);  // the root is the group's smallest index
+    }
+    // groups in order of their mean length (longest first), so that the
+    // column blocks and packs that straddle two groups still hold sequences
+    // of similar lengths
+    std::vector<uint8_t> has(n, 0);
+    for (const int2& pr : cand) has[pr.x] = has[pr.y] = 1;
+    std::vector<int64_t> gsum(n, 0), gcnt(n, 0);
+    for (int i = 0; i < n; ++i) {
+      const int r = find(i);
+      gsum[r] += ctx->len[i];
+      gcnt[r] += 1;
+    }
+    std::vector<int64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+      const int r = find(i);
+      const int64_t mean = (gsum[r] + gcnt[r] / 2) / std::max<int64_t>(gcnt[r], 1);
+      // no candidate at all: after every group (any order works for them)
+      key[i] = has[i] ? (((int64_t)INT32_MAX - mean) << 32 | (int64_t)r) : INT64_MAX;
+    }
+    if (swe_status s = engine_relayout(ctx, &key, &cand)) return s;
+  }
+  st.tiles_kept = (int64_t)ctx->tiles.size();
+  st.tiles_all = ctx->tiles_all;
+  st.tile_cells = ctx->stats.tile_cells;
+  st.ms_layout = ms_since(t2);
+  const auto t3 = clk::now();
+  if (swe_status s = score_pass(ctx)) return s;
+  st.ms_score = ms_since(t3);
+  st.ms_total = ms_since(t0);
+  if (out) *out = st;
   return SWE_OK;
 }
 

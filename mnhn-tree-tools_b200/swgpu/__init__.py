@@ -74,6 +74,33 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PrefilterStats(C.Structure):
+    _fields_ = [("candidates", C.c_int64), ("tiles_kept", C.c_int64), ("tiles_all", C.c_int64),
+                ("tile_cells", C.c_double), ("ms_embed", C.c_double), ("ms_candidates", C.c_double),
+                ("ms_layout", C.c_double), ("ms_score", C.c_double), ("ms_total", C.c_double),
+                ("fallback_full", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Margins(C.Structure):
+    _fields_ = [("n", C.c_int), ("upper", C.c_int * 8), ("margin", C.c_float * 8)]
+
+    @staticmethod
+    def of(m):
+        """A float (one margin for every pair) or a list of (upper, margin)
+        buckets by the pair's longer length (the last upper is ignored)."""
+        if isinstance(m, (int, float)):
+            m = [(0, float(m))]
+        t = Margins()
+        t.n = len(m)
+        for i, (u, v) in enumerate(m):
+            t.upper[i] = int(u)
+            t.margin[i] = float(v)
+        return t
+
+
 class SweepResult(C.Structure):
     _fields_ = [("status", C.c_int), ("truncated", C.c_int), ("steps", C.c_int), ("n_layers", C.c_int),
                 ("layers", C.POINTER(SplitSet)), ("log", C.c_void_p), ("done_ms", C.c_double)]
@@ -92,7 +119,7 @@ EXPORTS = [
     "swe_adaptive_set", "swe_adaptive_sets", "swe_free_sweep_results",
     "swe_kmer_features", "swe_prefilter_init", "swe_prefilter_param_count", "swe_prefilter_params",
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
-    "swe_gemm_bf16",
+    "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -166,6 +193,11 @@ def lib():
         L.swe_prefilter_embed.argtypes = [C.c_void_p, C.c_void_p]
         L.swe_prefilter_pair_dist.restype = C.c_int
         L.swe_prefilter_pair_dist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        L.swe_prefilter_set_embeddings.restype = C.c_int
+        L.swe_prefilter_set_embeddings.argtypes = [C.c_void_p, C.c_void_p]
+        L.swe_score_prefiltered.restype = C.c_int
+        L.swe_score_prefiltered.argtypes = [C.c_void_p, C.c_float, C.POINTER(Margins), C.c_int,
+                                            C.POINTER(PrefilterStats)]
         L.swe_gemm_bf16.restype = C.c_int
         L.swe_gemm_bf16.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                     C.c_int, C.c_void_p]
@@ -418,6 +450,19 @@ class Engine:
         _check(lib().swe_prefilter_pair_dist(self.ctx, a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data),
                self.ctx)
         return out
+
+    def prefilter_set_embeddings(self, emb: np.ndarray):
+        emb = np.ascontiguousarray(emb, dtype=np.float32)
+        assert emb.shape == (self.n, 128)
+        _check(lib().swe_prefilter_set_embeddings(self.ctx, emb.ctypes.data), self.ctx)
+
+    def score_prefiltered(self, eps: float, margins, use_emb: bool = True) -> dict:
+        """Prefiltered score pass; margins: a float or [(upper_len, margin), ...]."""
+        st = PrefilterStats()
+        mt = Margins.of(margins)
+        _check(lib().swe_score_prefiltered(self.ctx, C.c_float(eps), C.byref(mt), int(use_emb), C.byref(st)),
+               self.ctx)
+        return st.as_dict()
 
     def one_to_many(self, q: bytes, qlen: int | None = None) -> np.ndarray:
         qlen = len(q) if qlen is None else qlen

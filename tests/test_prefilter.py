@@ -162,3 +162,54 @@ def test_prefilter_training_reduces_loss(small_set):
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.5 * losses[0], losses
     np.testing.assert_allclose(pd, np.linalg.norm(emb[a[:1000]] - emb[b[:1000]], axis=1), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("emb_kind", ["random", "clustered"])
+def test_prefiltered_scores_are_exact_or_skipped(emb_kind):
+    """Every pair the prefiltered pass scores holds its exact distance; every
+    other pair reads as the largest value; no pair passing the candidate test
+    is skipped.  Embeddings are set directly so the candidate graph (and so
+    the component layout) is arbitrary: random embeddings mix lengths inside
+    tiles, clustered ones follow the families."""
+    rng = np.random.default_rng(12)
+    seqs, fam = W.config2(n=2500, seed=21)
+    seqs = list(seqs) + _odd_sequences(rng)
+    n = len(seqs)
+    e = swgpu.Engine()
+    e.upload(seqs)
+    e.score_all_pairs()
+    D = e.distances()
+    if emb_kind == "random":
+        emb = rng.normal(0, 0.1, size=(n, 128)).astype(np.float32)
+    else:
+        centers = rng.normal(0, 1, size=(fam.max() + 2, 128))
+        lab = np.concatenate([fam, np.full(n - len(fam), fam.max() + 1)])
+        emb = (centers[lab] + rng.normal(0, 0.05, size=(n, 128))).astype(np.float32)
+    e.prefilter_set_embeddings(emb)
+    eps, margins = 420.0, [(200, 0.05), (400, 0.03), (0, 0.06)]
+    st = e.score_prefiltered(eps, margins)
+    Dp = e.distances()
+    e.close()
+    assert st["fallback_full"] == 0 and 0 < st["tiles_kept"] < st["tiles_all"]
+    lens = np.array([len(s) for s in seqs])
+    mx = np.maximum(lens[:, None], lens[None, :])
+    ed = np.linalg.norm(emb[:, None, :].astype(np.float64) - emb[None, :, :], axis=2)
+    T = math.floor(eps)
+    margin = np.where(mx < 200, 0.05, np.where(mx < 400, 0.03, 0.06))
+    cand = (4 * np.abs(lens[:, None] - lens[None, :]) <= T) & (ed <= T / (4.0 * np.maximum(mx, 1)) + margin + 1e-4)
+    scored = Dp != 0xFFFF
+    assert np.array_equal(Dp[scored], D[scored])
+    assert not np.any(Dp[~scored] != 0xFFFF)
+    sure = cand & ~((ed > T / (4.0 * np.maximum(mx, 1)) + margin - 1e-4))  # away from float rounding
+    np.fill_diagonal(sure, False)
+    missing = np.argwhere(sure & ~scored)
+    assert len(missing) == 0, missing[:5]
+
+
+def _odd_sequences(rng):
+    """A few sequences off the packed path and of unusual lengths."""
+    out = [b"ACGT" * 200, b"N" * 50, b"ACGTRYACGT" * 10, b"A"]
+    for L in [100, 101, 599, 600, 37]:
+        out.append(W.BASES[rng.integers(0, 4, size=L)].tobytes())
+    return out

@@ -43,6 +43,11 @@ WORKLOADS = {
           "text": "config2: 20,000 DNA reads, lognormal lengths 100-600 bp (median 220), 200 families, "
                   "2-15% substitution, 1-3% indel, 2% N runs; one all-pairs score pass + adaptive DBSCAN "
                   "sweep over 8 eps values (eps_start 200, eps_inc 200, minpts 5)"},
+    "4": {"gen": "config2", "mode": "prefilter", "eps_list": [300.0, 200.0], "minpts": 5,
+          "text": "config4: learned prefilter on the config-2 distribution (20,000 reads); 5-mer features, MLP "
+                  "1024-512-256-128 GELU, bf16 weights / fp32 accumulation, trained on 2M exact-scored pairs of "
+                  "60 datasets of 6,000 reads (3,600 families), margins calibrated on 200k held-out pairs of "
+                  "another dataset; prefiltered score pass + DBSCAN (minpts 5) against the exact pass + DBSCAN"},
     "5": {"gen": "config5", "mode": "multi", "eps_start": 300.0, "eps_inc": 100.0, "minpts": 5, "max_steps": 12,
           "text": "config5: 500 independent split sets of 50-5,000 reads (log-uniform sizes, 521,216 reads), "
                   "config-1 generator with 2-20 families per set; one score pass over all sets + every set's "
@@ -535,6 +540,179 @@ def run_gpu_multi(args):
     return 0
 
 
+def run_gpu_prefilter(args):
+    """Learned prefilter (config 4): train on exact-scored pairs of other
+    datasets of the distribution, calibrate on a held-out one, then time the
+    prefiltered pass + DBSCAN against the exact pass + DBSCAN on the same GPU
+    and report eps-neighbour recall and adjusted Rand of the clusters."""
+    import numpy as np
+    import torch
+
+    import swgpu
+    from swgpu import prefilter as PF
+    from swgpu import workloads as W
+
+    rank, local, world = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.config]
+    t0 = time.perf_counter()
+    train_sets = [W.config2(seed=1000 + k, n=6000, n_fam=60)[0] for k in range(60)]
+    cal_seqs, _ = W.config2(seed=101)
+    test, _ = W.config2(seed=2 + rank)
+    if args.n:
+        test = test[:args.n]
+    gen_s = time.perf_counter() - t0
+    eng = swgpu.Engine(device=dev)
+    eps_list = wl["eps_list"]
+    trep = PF.train(eng, train_sets, max(eps_list), seed=0, weight_decay=args.weight_decay)
+    cal = {eps: PF.calibrate(eng, cal_seqs, eps, seed=0) for eps in eps_list}
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
+    n = len(test)
+    cells = W.cells(test)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            flush.fill_(1)
+            torch.cuda.synchronize(dev)
+            fn()
+        out, ms = None, []
+        barrier()
+        for _ in range(steps):
+            flush.fill_(1)
+            torch.cuda.synchronize(dev)
+            eng.timer_start()
+            out = fn()
+            ms.append(eng.timer_stop())
+        barrier()
+        return out, statistics.median(ms)
+
+    eng.upload(test)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    per_eps = {}
+    launches_pf = None
+    for eps in eps_list:
+        margins, crep = cal[eps]
+
+        def exact_step():
+            eng.score_all_pairs()
+            return eng.dbscan(eps, wl["minpts"])
+
+        def pf_step():
+            st = eng.score_prefiltered(eps, margins)
+            return eng.dbscan(eps, wl["minpts"]), st
+
+        lab_ex, ms_ex = timed(exact_step, args.steps, args.warmup)
+        rp, _ = eng.neighbors(eps)
+        exact_nbrs = int(rp[-1]) - n
+        s0 = eng.stats()["kernel_launches"]
+        (lab_pf, st), ms_pf = timed(pf_step, args.steps, args.warmup)
+        launches_pf = (eng.stats()["kernel_launches"] - s0) // max(args.steps + args.warmup, 1)
+        rp, _ = eng.neighbors(eps)
+        recall = (int(rp[-1]) - n) / exact_nbrs if exact_nbrs else 1.0
+        ari = PF.adjusted_rand(PF.labels_from_split(lab_ex, n), PF.labels_from_split(lab_pf, n))
+        per_eps[str(int(eps))] = {
+            "recall": round(recall, 6), "ari": round(ari, 6), "speedup": round(ms_ex / ms_pf, 3),
+            "ms_exact_step": round(ms_ex, 2), "ms_prefilter_step": round(ms_pf, 2),
+            "exact_neighbour_pairs": exact_nbrs // 2, "clusters_exact": len(lab_ex), "clusters_prefilter": len(lab_pf),
+            "candidates": int(st["candidates"]), "tiles_kept": int(st["tiles_kept"]), "tiles_all": int(st["tiles_all"]),
+            "tile_cells": st["tile_cells"], "ms_embed": round(st["ms_embed"], 2),
+            "ms_candidates": round(st["ms_candidates"], 2), "ms_layout": round(st["ms_layout"], 2),
+            "ms_score": round(st["ms_score"], 2), "margins": [[u, round(m, 5)] for u, m in margins],
+            "scale": crep.get("scale"), "cal_recall_trials": crep.get("scale_trials")}
+    clk = clocks.stop()
+    head = str(int(eps_list[0]))
+
+    # e2e through the C ABI with host buffers: upload, prefiltered pass, DBSCAN, clusters on the host
+    margins0 = cal[eps_list[0]][0]
+    e2e_ms = []
+    b0 = eng.stats()
+    for _ in range(max(1, args.steps)):
+        barrier()
+        t1 = time.perf_counter()
+        eng.upload(test)
+        eng.score_prefiltered(eps_list[0], margins0)
+        eng.dbscan(eps_list[0], wl["minpts"])
+        e2e_ms.append(1e3 * (time.perf_counter() - t1))
+    b1 = eng.stats()
+
+    # the same recipe without the network: a fixed random projection of the k-mer features
+    ablation = {}
+    if not args.no_ablation:
+        sub = train_sets[:5]
+        eng.upload_sets(sub)
+        Fsub = eng.kmer_features(5)
+        ta, tb, td, tl = trep["train_pairs"]
+        nsub = sum(len(x) for x in sub)
+        keep = (ta < nsub) & (tb < nsub)
+        scale = PF.projection_scale(Fsub, ta[keep], tb[keep], td[keep], tl)
+        proj = lambda en: (scale * PF.projection_embeddings(en.kmer_features(5))).astype(np.float32)
+        for eps in eps_list:
+            m2, r2 = PF.calibrate(eng, cal_seqs, eps, seed=0, embeddings=proj)
+            eng.upload(test)
+            eng.prefilter_set_embeddings(proj(eng))
+            eng.score_all_pairs()
+            rp, _ = eng.neighbors(eps)
+            exact_nbrs = int(rp[-1]) - n
+            eng.timer_start()
+            st2 = eng.score_prefiltered(eps, m2)
+            eng.dbscan(eps, wl["minpts"])
+            ms2 = eng.timer_stop()
+            rp, _ = eng.neighbors(eps)
+            ablation[str(int(eps))] = {
+                "recall": round((int(rp[-1]) - n) / exact_nbrs if exact_nbrs else 1.0, 6),
+                "speedup": round(per_eps[str(int(eps))]["ms_exact_step"] / ms2, 3),
+                "candidates": int(st2["candidates"]), "tiles_kept": int(st2["tiles_kept"]),
+                "fallback_full": int(st2["fallback_full"]), "scale": r2.get("scale"),
+                "margins": [[u, round(m, 5)] for u, m in m2]}
+
+    if rank == 0:
+        sp = per_eps[head]["speedup"]
+        line = {
+            "metric": METRIC, "value": sp, "unit": "x (prefiltered vs exact step, same GPU)", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_eps[head]["ms_prefilter_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "s16x2 + bf16",
+            "data": "synthetic",
+            "config": {"workload": wl["text"], "n_sequences": n, "cells_per_gpu": cells, "eps": eps_list,
+                       "headline_eps": eps_list[0], "minpts": wl["minpts"],
+                       "parallelism": f"{world} independent datasets (one per GPU)",
+                       "l2": "256 MB buffer written between timed steps (L2 flush)"},
+            "prefilter": per_eps,
+            "training": {"generation_s": round(gen_s, 2), "train_exact_pass_s": trep["train_exact_pass_s"],
+                         "train_pair_scoring_s": trep["train_pair_scoring_s"], "train_s": trep["train_s"],
+                         "epoch_loss": trep["epoch_loss"], "n_train": trep["n_train"],
+                         "n_cal": cal[eps_list[0]][1]["n_cal"], "train_pools": trep["train_pools"],
+                         "weight_decay": args.weight_decay},
+            "ablation_without_network": ablation,
+            "e2e": {"value": round(per_eps[head]["ms_exact_step"] / statistics.median(e2e_ms), 3),
+                    "unit": "x (exact device step / prefiltered host-to-host step)",
+                    "h2d_bytes_per_step": int(b1["h2d_bytes"]), "d2h_bytes_per_step": int(b1["d2h_bytes"])},
+            "gpu_launches": int(launches_pf) if launches_pf is not None else None,
+            "clocks": clk,
+            "prefilter_speedup": sp,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    del flush
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -547,11 +725,15 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="profile a smaller case: the first n reads of the workload "
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
+    ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
+    ap.add_argument("--weight-decay", type=float, default=0.0, help="config 4: decoupled weight decay of Adam")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if WORKLOADS[args.config]["mode"] == "multi":
         return run_gpu_multi(args)
+    if WORKLOADS[args.config]["mode"] == "prefilter":
+        return run_gpu_prefilter(args)
     return run_gpu(args)
 
 

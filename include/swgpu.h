@@ -246,10 +246,12 @@ swe_status swe_prefilter_params(swe_ctx* ctx, float* get, const float* set);
    the gradient of every parameter (same layout as the parameters). */
 swe_status swe_prefilter_loss_grad(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int npairs,
                                    float* loss, float* grad);
-/* Adam training over the pairs for `epochs` passes in shuffled batches of
-   batch_pairs pairs (full batches only); epoch_loss[e] = mean batch loss. */
+/* Adam training (decoupled weight decay weight_decay, 0 for none) over the
+   pairs for `epochs` passes in shuffled batches of batch_pairs pairs (full
+   batches only); epoch_loss[e] = mean batch loss. */
 swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int64_t npairs,
-                               int epochs, int batch_pairs, float lr, uint64_t seed, float* epoch_loss);
+                               int epochs, int batch_pairs, float lr, float weight_decay, uint64_t seed,
+                               float* epoch_loss);
 /* Embeddings of the uploaded sequences (out: n x 128, or NULL). */
 swe_status swe_prefilter_embed(swe_ctx* ctx, float* out);
 /* Embedding distances of explicit pairs. */

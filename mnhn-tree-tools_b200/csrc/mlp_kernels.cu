@@ -402,20 +402,20 @@ cudaError_t launch_pair_loss(const float* E, int D, const float* target, int P, 
 
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float bc1,
-                            float bc2) {
+                            float bc2, float wd) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const float gi = g[i];
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    w[i] -= lr * ((mi / bc1) / (sqrtf(vi / bc2) + eps) + wd * w[i]);
   }
 }
 
 cudaError_t launch_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
-                        float eps, float bc1, float bc2, cudaStream_t st) {
-  adam_kernel<<<148 * 4, 256, 0, st>>>(w, g, m, v, n, lr, b1, b2, eps, bc1, bc2);
+                        float eps, float bc1, float bc2, float wd, cudaStream_t st) {
+  adam_kernel<<<148 * 4, 256, 0, st>>>(w, g, m, v, n, lr, b1, b2, eps, bc1, bc2, wd);
   return cudaGetLastError();
 }
 

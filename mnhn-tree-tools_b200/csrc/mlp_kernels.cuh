@@ -62,9 +62,10 @@ cudaError_t launch_gather_rows(const float* X, int D, const int* idx, int rows, 
 // [D x M] and column sums.  Rows >= 2P get zero gradient.
 cudaError_t launch_pair_loss(const float* E, int D, const float* target, int P, int M, float* loss,
                              __nv_bfloat16* dE, __nv_bfloat16* dE_t, float* colsum, cudaStream_t st);
-// Adam on a flat fp32 parameter vector.
+// Adam on a flat fp32 parameter vector, with decoupled weight decay wd
+// (w -= lr * (m_hat / (sqrt(v_hat) + eps) + wd * w)).
 cudaError_t launch_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
-                        float eps, float bc1, float bc2, cudaStream_t st);
+                        float eps, float bc1, float bc2, float wd, cudaStream_t st);
 // bf16 copy and bf16 transpose of an fp32 [R x C] matrix.
 cudaError_t launch_publish(const float* W, int R, int C, __nv_bfloat16* Wb, __nv_bfloat16* Wt, cudaStream_t st);
 

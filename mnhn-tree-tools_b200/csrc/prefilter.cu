@@ -315,8 +315,10 @@ swe_status swe_prefilter_loss_grad(swe_ctx* ctx, const int* a, const int* b, con
 }
 
 swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int64_t npairs,
-                               int epochs, int batch_pairs, float lr, uint64_t seed, float* epoch_loss) {
-  if (!ctx || npairs <= 0 || !a || !b || !dist || epochs < 0 || batch_pairs <= 0 || !(lr > 0))
+                               int epochs, int batch_pairs, float lr, float weight_decay, uint64_t seed,
+                               float* epoch_loss) {
+  if (!ctx || npairs <= 0 || !a || !b || !dist || epochs < 0 || batch_pairs <= 0 || !(lr > 0) ||
+      !(weight_decay >= 0))
     return SWE_ERR_INVALID;
   if (swe_status s = select_device(ctx)) return s;
   if (swe_status s = pf_need(ctx, true)) return s;
@@ -350,7 +352,8 @@ swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const u
       pf->adam_t++;
       const float bc1 = 1.0f - std::pow(b1, (float)pf->adam_t), bc2 = 1.0f - std::pow(b2, (float)pf->adam_t);
       ctx->stats.kernel_launches += 1;
-      CK(launch_adam(pf->w.p, pf->g.p, pf->m.p, pf->v.p, PS::NPARAM, lr, b1, b2, eps, bc1, bc2, ctx->st));
+      CK(launch_adam(pf->w.p, pf->g.p, pf->m.p, pf->v.p, PS::NPARAM, lr, b1, b2, eps, bc1, bc2, weight_decay,
+                     ctx->st));
       if (swe_status s = publish(ctx)) return s;
     }
     float sum = 0;

@@ -151,17 +151,12 @@ def calibrate_margin(emb_dist, d, lens_a, lens_b, eps: float, q: float) -> float
     return float(np.quantile(r, q, method="higher"))
 
 
-def fit(eng, train_sets, cal_seqs, eps: float, n_train: int = 2_000_000, n_cal: int = 200_000,
-        epochs: int = 8, batch_pairs: int = 4096, lr: float = 1e-3, band_factor: float = 2.0, q: float = 0.9995,
-        seed: int = 0, tune_scale: bool = True):
+def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8, batch_pairs: int = 4096,
+          lr: float = 1e-3, band_factor: float = 2.0, seed: int = 0, weight_decay: float = 0.0):
     """Trains the prefilter on pairs of ``train_sets`` (independent datasets
-    of the target distribution, scored in one pass) and calibrates the margin
-    on held-out pairs of ``cal_seqs`` (another dataset of the distribution,
-    with families the network never saw), per bucket of the longer length.
-    Returns (margins, report); the
-    trained weights stay in ``eng``.  Training pairs: 25% neighbours, 35% near
-    pairs, 40% uniform; calibration pairs: 60% neighbours, 20% near, 20%
-    uniform (the margin is read from the neighbours)."""
+    of the target distribution, scored in one exact pass): 25% neighbours
+    (d <= eps), 35% near pairs (eps < d <= band_factor * eps), 40% uniform.
+    The weights stay in ``eng``.  Returns a report."""
     rng = np.random.default_rng(seed)
     rep = {}
     t0 = time.perf_counter()
@@ -178,11 +173,26 @@ def fit(eng, train_sets, cal_seqs, eps: float, n_train: int = 2_000_000, n_cal: 
     rep["train_pair_scoring_s"] = round(time.perf_counter() - t1, 3)
     eng.prefilter_init(seed=seed + 1)
     t2 = time.perf_counter()
-    losses = eng.prefilter_train(ta, tb, td, epochs=epochs, batch_pairs=batch_pairs, lr=lr, seed=seed + 2)
+    losses = eng.prefilter_train(ta, tb, td, epochs=epochs, batch_pairs=batch_pairs, lr=lr, seed=seed + 2,
+                                 weight_decay=weight_decay)
     rep["train_s"] = round(time.perf_counter() - t2, 3)
     rep["epoch_loss"] = [round(float(x), 6) for x in losses]
-    train_lens = np.array([len(x) for st in train_sets for x in st])
-    # held-out calibration on a dataset of its own
+    rep["n_train"] = int(len(ta))
+    rep["train_pairs"] = (ta, tb, td, np.array([len(x) for st in train_sets for x in st]))
+    return rep
+
+
+def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995, band_factor: float = 2.0,
+              tune_scale: bool = True, seed: int = 0, embeddings=None):
+    """Margins for ``eps`` from held-out pairs of ``cal_seqs`` (a dataset of
+    the distribution with families the network never saw): 60% neighbours,
+    20% near pairs, 20% uniform; per bucket of the longer length the
+    q-quantile margin, then (tune_scale) scaled down while the prefiltered
+    pass itself keeps recall >= q on this dataset.  ``embeddings``: a
+    function of the uploaded engine returning embeddings to use instead of
+    the network's (the method without the network).  Returns (margins, report)."""
+    rng = np.random.default_rng(seed + 7)
+    rep = {}
     eng.upload(cal_seqs)
     eng.score_all_pairs()
     (cal,), cpools = sample_pairs(eng, eps, band_factor * eps,
@@ -190,21 +200,35 @@ def fit(eng, train_sets, cal_seqs, eps: float, n_train: int = 2_000_000, n_cal: 
     ca, cb = cal
     cd = eng.score_pairs(ca, cb)
     lens = np.array([len(x) for x in cal_seqs])
-    ed = eng.prefilter_pair_dist(ca, cb)
-    margin = calibrate_buckets(ed, cd, lens[ca], lens[cb], eps, q)
-    rep["margins_pairs"] = margin
+    if embeddings is not None:
+        emb = embeddings(eng)
+        eng.prefilter_set_embeddings(emb)
+        ed = np.linalg.norm(emb[ca].astype(np.float64) - emb[cb], axis=1)
+    else:
+        ed = eng.prefilter_pair_dist(ca, cb)
+    margins = calibrate_buckets(ed, cd, lens[ca], lens[cb], eps, q)
+    rep["margins_pairs"] = margins
+    rep["cal_pools"] = [int(x) for x in cpools]
+    rep["cal_neighbours"] = int((cd <= math.floor(eps)).sum())
+    rep["n_cal"] = int(len(ca))
+    rep["cal_pairs"] = (ca, cb, cd, lens)
     if tune_scale:
         # the prefiltered pass scores whole tiles, so it finds more neighbours
         # than the candidate test alone: shrink the margins while the pass
         # itself keeps the recall on this held-out dataset
-        margin, rep["scale"], rep["scale_trials"] = calibrate_scale(eng, eps, margin, q)
-    rep["margins"] = margin
-    rep["cal_pools"] = [int(x) for x in cpools]
-    rep["cal_neighbours"] = int((cd <= math.floor(eps)).sum())
-    rep["n_train"], rep["n_cal"] = int(len(ta)), int(len(ca))
-    rep["train_pairs"] = (ta, tb, td, train_lens)
-    rep["cal_pairs"] = (ca, cb, cd, lens)
-    return margin, rep
+        margins, rep["scale"], rep["scale_trials"] = calibrate_scale(eng, eps, margins, q)
+    rep["margins"] = margins
+    return margins, rep
+
+
+def fit(eng, train_sets, cal_seqs, eps: float, n_train: int = 2_000_000, n_cal: int = 200_000,
+        epochs: int = 8, batch_pairs: int = 4096, lr: float = 1e-3, band_factor: float = 2.0, q: float = 0.9995,
+        seed: int = 0, tune_scale: bool = True):
+    """``train`` then ``calibrate`` for one eps; returns (margins, report)."""
+    rep = train(eng, train_sets, eps, n_train, epochs, batch_pairs, lr, band_factor, seed)
+    margins, crep = calibrate(eng, cal_seqs, eps, n_cal, q, band_factor, tune_scale, seed)
+    rep.update(crep)
+    return margins, rep
 
 
 def projection_embeddings(features: np.ndarray, seed: int = 0, dim: int = 128) -> np.ndarray:
@@ -215,21 +239,17 @@ def projection_embeddings(features: np.ndarray, seed: int = 0, dim: int = 128) -
     return (features.astype(np.float64) @ R).astype(np.float32)
 
 
-def fit_projection(F_train: np.ndarray, train_pairs, F_cal: np.ndarray, cal_pairs, eps: float, q: float,
-                   seed: int = 0):
-    """The same recipe without the network: scale s of the projection fit by
-    least squares on the training pairs (s * ||P x_a - P x_b|| ~ d / (4 max
-    len)), margin calibrated on the held-out pairs like the learned one's."""
-    def dist(F, a, b):
-        P = projection_embeddings(F, seed)
-        return np.linalg.norm(P[a] - P[b], axis=1).astype(np.float64)
-    ta, tb, td, tl = train_pairs
-    e = dist(F_train, ta, tb)
-    t = np.asarray(td, dtype=np.float64) / (4.0 * np.maximum(np.maximum(tl[ta], tl[tb]), 1))
-    s = float((e * t).sum() / max((e * e).sum(), 1e-30))
-    ca, cb, cd, cl = cal_pairs
-    margins = calibrate_buckets(s * dist(F_cal, ca, cb), cd, cl[ca], cl[cb], eps, q)
-    return s, margins
+def projection_scale(features: np.ndarray, a, b, d, lens, seed: int = 0) -> float:
+    """Scale s of the projection fit by least squares on exact-scored pairs:
+    s * ||P x_a - P x_b|| ~ d / (4 max(len_a, len_b)).  With it, the method
+    without the network runs the same recipe (``calibrate`` with
+    ``embeddings``) as the learned embedding."""
+    P = projection_embeddings(features, seed)
+    a, b = np.asarray(a), np.asarray(b)
+    lens = np.asarray(lens)
+    e = np.linalg.norm(P[a] - P[b], axis=1).astype(np.float64)
+    t = np.asarray(d, dtype=np.float64) / (4.0 * np.maximum(np.maximum(lens[a], lens[b]), 1))
+    return float((e * t).sum() / max((e * e).sum(), 1e-30))
 
 
 def labels_from_split(split, n: int) -> np.ndarray:

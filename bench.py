@@ -59,6 +59,23 @@ WORKLOADS = {
 }
 
 
+def dataset_seed(config: str, rank: int) -> int:
+    """Seed of the dataset a rank works on: rank r of an N-GPU run scores its
+    own independently seeded dataset of the same configuration (weak scaling,
+    no data-path collective); rank 0 has the single-GPU dataset."""
+    return {"2": 2, "3": 3, "4": 2, "5": 5}[config] + rank
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (one all-reduce; x itself without a group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), \
         int(os.environ.get("WORLD_SIZE", "1"))
@@ -234,7 +251,7 @@ def run_gpu(args):
 
     wl = WORKLOADS[args.config]
     gen = getattr(W, wl["gen"])
-    seqs, _ = gen(seed=(2 if args.config == "2" else 3) + rank)
+    seqs, _ = gen(seed=dataset_seed(args.config, rank))
     if args.n:
         seqs = seqs[:args.n]
     cells = W.cells(seqs)
@@ -282,10 +299,7 @@ def run_gpu(args):
     clk = clocks.stop()
     st1 = eng.stats()
     total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
     ms_per_step = total_ms / args.steps
     value = cells * world / (ms_per_step * 1e-3) / 1e9
     launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
@@ -310,10 +324,7 @@ def run_gpu(args):
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     b1 = eng.stats()
     e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(e2e_total, dist, f"cuda:{dev}")
     e2e_value = cells * world / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
     # upload() resets the counters, so the last step's totals are the per-step figures
     h2d = b1["h2d_bytes"]
@@ -402,7 +413,7 @@ def run_gpu_multi(args):
     dev = local
     torch.cuda.set_device(dev)
     wl = WORKLOADS[args.config]
-    sets, _ = W.config5(seed=5 + rank)
+    sets, _ = W.config5(seed=dataset_seed(args.config, rank))
     if args.n:
         sets = sets[:args.n]
     cells = sum(W.cells(st) for st in sets)
@@ -448,10 +459,7 @@ def run_gpu_multi(args):
     clk = clocks.stop()
     st1 = eng.stats()
     total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
     ms_per_step = total_ms / args.steps
     value = cells * world / (ms_per_step * 1e-3) / 1e9
     launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
@@ -468,10 +476,7 @@ def run_gpu_multi(args):
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     b1 = eng.stats()
     e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(e2e_total, dist, f"cuda:{dev}")
     e2e_value = cells * world / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
 
     # the same sets one by one (upload, score pass, sweep per set), rank 0 only
@@ -566,7 +571,7 @@ def run_gpu_prefilter(args):
     t0 = time.perf_counter()
     train_sets = [W.config2(seed=1000 + k, n=6000, n_fam=60)[0] for k in range(60)]
     cal_seqs, _ = W.config2(seed=101)
-    test, _ = W.config2(seed=2 + rank)
+    test, _ = W.config2(seed=dataset_seed(args.config, rank))
     if args.n:
         test = test[:args.n]
     gen_s = time.perf_counter() - t0

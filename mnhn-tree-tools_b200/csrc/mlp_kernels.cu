@@ -95,6 +95,9 @@ constexpr int G_BM = 128, G_BN = 128, G_BK = 64, G_STAGES = 4;
 constexpr int G_TILE_BYTES = G_BM * G_BK * 2;  // 16 KB per operand tile (A and B tiles are both 128 x 64)
 constexpr int G_STAGE_BYTES = 2 * G_TILE_BYTES;
 constexpr int G_TMEM_COLS = 128;
+// 8 warps: warp w drains accumulator rows 32*(w%4) .. +31 (the tensor-memory
+// lanes its quarter may read) and columns 64*(w/4) .. +63
+constexpr int G_THREADS = 256;
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -149,8 +152,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
 
 // One CTA per 128 x 128 tile of C.  Warp 0 lane 0 feeds the stage ring with
 // TMA, warp 1 lane 0 issues the MMAs (4 per 64-wide K step) and commits each
-// stage back to the producer; then all four warps drain the accumulator.
-__global__ void __launch_bounds__(128, 1) gemm_bf16_tn_kernel(const __grid_constant__ CUtensorMap ta,
+// stage back to the producer; then all eight warps drain the accumulator.
+__global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid_constant__ CUtensorMap ta,
                                                               const __grid_constant__ CUtensorMap tb, int M, int N,
                                                               int K, GemmEpi ep) {
   extern __shared__ uint8_t g_smem_raw[];
@@ -218,39 +221,68 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tn_kernel(const __grid_const
   }
   __syncwarp();
 
-  // epilogue: warp w owns accumulator rows 32w .. 32w+31 (tensor-memory lanes)
+  // epilogue: warp w drains rows 32*(w%4) .. +31 (its tensor-memory lane
+  // quarter) and columns 64*(w/4) .. +63
   int ok = 0;
   if (lane == 0) ok = mbar_wait_bounded(&done_bar, 0, ep.wait_limit) ? 1 : 0;
   ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
   if (!ok && lane == 0) atomicOr(ep.status, KST_TIMEOUT);
   tc_fence_after();
-  const int m = m0 + warp * 32 + lane;
+  const int quarter = warp & 3, half = warp >> 2;
+  const int m = m0 + quarter * 32 + lane;
   if (ok) {
-    for (int c = 0; c < G_BN; c += 16) {
+    for (int c = half * (G_BN / 2); c < (half + 1) * (G_BN / 2); c += 16) {
       uint32_t r[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+      tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
+      const long long rowoff = (long long)m * N + n0 + c;
       float v[16];
+      if (ep.gelu_in) {
+        const float4* gi = reinterpret_cast<const float4*>(ep.gelu_in + rowoff);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int n = n0 + c + j;
-        float x = __uint_as_float(r[j]);
-        if (ep.gelu_in) x *= gelu_grad(ep.gelu_in[(long long)m * N + n]);
-        if (ep.bias) x += ep.bias[n];
-        if (ep.out_pre) ep.out_pre[(long long)m * N + n] = x;
-        if (ep.act) x = gelu_ref(x);
-        v[j] = x;
+        for (int q = 0; q < 4; ++q) {
+          const float4 z = gi[q];
+          v[4 * q] = z.x, v[4 * q + 1] = z.y, v[4 * q + 2] = z.z, v[4 * q + 3] = z.w;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]) * gelu_grad(v[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
       }
-      if (ep.out_f32) {
-        float4* o = reinterpret_cast<float4*>(ep.out_f32 + (long long)m * N + n0 + c);
+      if (ep.bias) {
+        const float4* bb = reinterpret_cast<const float4*>(ep.bias + n0 + c);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 b = bb[q];
+          v[4 * q] += b.x, v[4 * q + 1] += b.y, v[4 * q + 2] += b.z, v[4 * q + 3] += b.w;
+        }
+      }
+      if (ep.out_pre) {
+        float4* o = reinterpret_cast<float4*>(ep.out_pre + rowoff);
 #pragma unroll
         for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
       }
-      if (ep.out_bf16) {
-        __nv_bfloat16* o = ep.out_bf16 + (long long)m * N + n0 + c;
+      if (ep.act) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) o[j] = __float2bfloat16_rn(v[j]);
+        for (int j = 0; j < 16; ++j) v[j] = gelu_ref(v[j]);
       }
-      if (ep.out_bf16_t) {
+      if (ep.out_f32) {
+        float4* o = reinterpret_cast<float4*>(ep.out_f32 + rowoff);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      }
+      if (ep.out_bf16) {  // 16 values = two 16-byte stores
+        uint32_t w[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+          w[q] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        uint4* o = reinterpret_cast<uint4*>(ep.out_bf16 + rowoff);
+        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+      }
+      if (ep.out_bf16_t) {  // lanes hold consecutive rows: each store is one 64-byte run
 #pragma unroll
         for (int j = 0; j < 16; ++j) ep.out_bf16_t[(long long)(n0 + c + j) * M + m] = __float2bfloat16_rn(v[j]);
       }
@@ -317,7 +349,11 @@ cudaError_t make_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int 
 cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                                 const GemmEpi& ep, cudaStream_t st) {
   if (M <= 0 || N <= 0 || K <= 0 || M % G_BM || N % G_BN || K % G_BK) return cudaErrorInvalidValue;
-  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) return cudaErrorInvalidValue;
+  // operands and every epilogue array are read and written in 16-byte units
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(ep.bias) |
+       reinterpret_cast<uintptr_t>(ep.gelu_in) | reinterpret_cast<uintptr_t>(ep.out_pre) |
+       reinterpret_cast<uintptr_t>(ep.out_f32) | reinterpret_cast<uintptr_t>(ep.out_bf16)) & 15)
+    return cudaErrorInvalidValue;
   CUtensorMap ma, mb;
   cudaError_t e = make_map(&ma, A, M, K);
   if (e == cudaSuccess) e = make_map(&mb, B, N, K);
@@ -329,7 +365,7 @@ cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, 
     attr = true;
   }
   dim3 grid(N / G_BN, M / G_BM);
-  gemm_bf16_tn_kernel<<<grid, 128, gemm_smem_bytes(), st>>>(ma, mb, M, N, K, ep);
+  gemm_bf16_tn_kernel<<<grid, G_THREADS, gemm_smem_bytes(), st>>>(ma, mb, M, N, K, ep);
   return cudaGetLastError();
 }
 

@@ -217,25 +217,27 @@ def _odd_sequences(rng):
 
 @pytest.mark.gpu
 def test_learned_prefilter_recall_ari_and_gain_over_projection():
-    """The whole recipe at reduced size (eps 200, config-2 distribution):
-    train on exact-scored pairs of 12 datasets, calibrate on a held-out
-    dataset, run the prefiltered pass on a third one.  Its eps-neighbour
-    recall against the exact pass must be >= 0.998 (the calibration target is
-    0.9995; the tolerance covers the smaller held-out sample) and the DBSCAN
-    clusters must agree (adjusted Rand >= 0.99).  The same recipe without the
-    network (a fixed random projection of the same k-mer features, scaled by
-    least squares, calibrated the same way) must need more DP cells for the
-    same recall target: that difference is what the trained network gains."""
+    """The whole recipe of the config-4 benchmark at eps 200 (config-2
+    distribution): train on 2M exact-scored pairs of 60 datasets of 6,000
+    reads, calibrate on a held-out dataset, run the prefiltered pass on a
+    third one.  Its eps-neighbour recall against the exact pass must be
+    >= 0.999 and the DBSCAN clusters must agree (adjusted Rand >= 0.99).  The
+    same recipe without the network (a fixed random projection of the same
+    k-mer features, scaled by least squares, calibrated the same way) must
+    need more DP cells for the same recall target: that difference is what
+    the trained network gains.  (With a tenth of the training data the
+    network does not beat the projection: it needs many families to learn a
+    similarity that holds for families it has not seen.)"""
     from swgpu import prefilter as PF
     eps = 200.0
-    train_sets = [W.config2(seed=3000 + k, n=3000, n_fam=30)[0] for k in range(12)]
-    cal_seqs, _ = W.config2(seed=3101, n=6000, n_fam=60)
-    test, _ = W.config2(seed=3202, n=6000, n_fam=60)
+    train_sets = [W.config2(seed=1000 + k, n=6000, n_fam=60)[0] for k in range(60)]
+    cal_seqs, _ = W.config2(seed=101)
+    test, _ = W.config2(seed=2)
     n = len(test)
     e = swgpu.Engine()
-    rep = PF.train(e, train_sets, eps, n_train=400_000, epochs=8, seed=0)
+    rep = PF.train(e, train_sets, eps, seed=0)
     assert rep["epoch_loss"][-1] < 0.5 * rep["epoch_loss"][0]
-    margins, _ = PF.calibrate(e, cal_seqs, eps, n_cal=60_000, seed=0)
+    margins, _ = PF.calibrate(e, cal_seqs, eps, seed=0)
     e.upload(test)
     e.score_all_pairs()
     full_cells = e.stats()["tile_cells"]
@@ -247,17 +249,17 @@ def test_learned_prefilter_recall_ari_and_gain_over_projection():
     rp, _ = e.neighbors(eps)
     recall = (int(rp[-1]) - n) / exact
     ari = PF.adjusted_rand(PF.labels_from_split(lab_ex, n), PF.labels_from_split(lab_pf, n))
-    assert recall >= 0.998, (recall, st)
+    assert recall >= 0.999, (recall, st)
     assert ari >= 0.99, ari
-    assert st["tile_cells"] < 0.5 * full_cells, (st["tile_cells"], full_cells)
+    assert st["tile_cells"] < 0.2 * full_cells, (st["tile_cells"], full_cells)
     # without the network
     ta, tb, td, tl = rep["train_pairs"]
-    e.upload_sets(train_sets[:3])
+    e.upload_sets(train_sets[:5])
     nsub = e.n
     keep = (ta < nsub) & (tb < nsub)
     scale = PF.projection_scale(e.kmer_features(5), ta[keep], tb[keep], td[keep], tl)
     proj = lambda en: (scale * PF.projection_embeddings(en.kmer_features(5))).astype(np.float32)
-    m2, _ = PF.calibrate(e, cal_seqs, eps, n_cal=60_000, seed=0, embeddings=proj)
+    m2, _ = PF.calibrate(e, cal_seqs, eps, seed=0, embeddings=proj)
     e.upload(test)
     e.prefilter_set_embeddings(proj(e))
     st2 = e.score_prefiltered(eps, m2)

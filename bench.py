@@ -358,6 +358,8 @@ def run_gpu(args):
                        "parallelism": f"{world} independent datasets (one per GPU)",
                        "l2": "256 MB buffer written between timed steps (L2 flush); distance matrix 800 MB"},
             "dbscan_sec": round(ms_per_step * 1e-3, 4),
+            "rerun_pairs": int(st1["reruns"]),
+            "rerun_fraction": st1["reruns"] / max(len(seqs) * (len(seqs) - 1) // 2, 1),
             "score_pass_ms": round(statistics.median(score_ms), 2),
             "sweep_ms": round(sweep_s * 1e3, 2),
             "roofline": {"bound": "int", "kernel": "fast_all_pairs_kernel", "achieved": round(fast_gcups, 1),

@@ -247,8 +247,8 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
       for (int pl = b; pl < std::min(npk, b + PB); ++pl) {
         const int g = f + 2 * pl;
         const bool pair = 2 * pl + 1 < nf;
-        // an even row count: the 16x2 kernel processes two rows per step
-        const int R = (std::max(ctx->len[ctx->order[g]], pair ? ctx->len[ctx->order[g + 1]] : 0) + 1) & ~1;
+        // a row count that is a multiple of 4: the 16x2 kernel processes four rows per step
+        const int R = (std::max(ctx->len[ctx->order[g]], pair ? ctx->len[ctx->order[g + 1]] : 0) + 3) & ~3;
         pack_first.push_back(g);
         pack_pair.push_back(pair ? 1 : 0);
         pack_off.push_back((int)row);

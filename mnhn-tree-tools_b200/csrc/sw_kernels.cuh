@@ -50,7 +50,7 @@ struct FastParams {
   const int* pack_first;     // [npacks] global sorted index of a pack's first sequence
   const uint8_t* pack_pair;  // [npacks] 1 when the pack has a second sequence (pack_first + 1)
   const int* pack_row_off;   // [npacks] start row of each pack (blocks 8-row aligned)
-  const int* pack_rows;      // [npacks] rows of each pack (even)
+  const int* pack_rows;      // [npacks] rows of each pack (a multiple of 4)
   const int* block_first;    // [nblocks] first pack of each row block
   const int* block_npacks;   // [nblocks] packs in each row block
   int max_packs_per_block;   // PB

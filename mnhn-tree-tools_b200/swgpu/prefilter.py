@@ -20,7 +20,7 @@ prefilter is used on):
   5. the prefiltered pass scores whole tiles around the candidates, so it
      finds more neighbours than the candidate test: on the held-out dataset
      the margins are scaled down (bisection) while the pass's own
-     eps-neighbour recall stays >= q.
+     eps-neighbour recall stays >= q_pass (0.9998, above the 0.999 target).
 """
 from __future__ import annotations
 
@@ -183,14 +183,17 @@ def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8
 
 
 def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995, band_factor: float = 2.0,
-              tune_scale: bool = True, seed: int = 0, embeddings=None):
+              tune_scale: bool = True, seed: int = 0, embeddings=None, q_pass: float = 0.9998):
     """Margins for ``eps`` from held-out pairs of ``cal_seqs`` (a dataset of
     the distribution with families the network never saw): 60% neighbours,
     20% near pairs, 20% uniform; per bucket of the longer length the
     q-quantile margin, then (tune_scale) scaled down while the prefiltered
-    pass itself keeps recall >= q on this dataset.  ``embeddings``: a
-    function of the uploaded engine returning embeddings to use instead of
-    the network's (the method without the network).  Returns (margins, report)."""
+    pass itself keeps recall >= q_pass on this dataset.  q_pass sits above
+    the 0.999 recall target because the recall of one pass varies from
+    dataset to dataset by a few parts in 10^4 (families differ).
+    ``embeddings``: a function of the uploaded engine returning embeddings
+    to use instead of the network's (the method without the network).
+    Returns (margins, report)."""
     rng = np.random.default_rng(seed + 7)
     rep = {}
     eng.upload(cal_seqs)
@@ -216,7 +219,7 @@ def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995
         # the prefiltered pass scores whole tiles, so it finds more neighbours
         # than the candidate test alone: shrink the margins while the pass
         # itself keeps the recall on this held-out dataset
-        margins, rep["scale"], rep["scale_trials"] = calibrate_scale(eng, eps, margins, q)
+        margins, rep["scale"], rep["scale_trials"] = calibrate_scale(eng, eps, margins, q_pass)
     rep["margins"] = margins
     return margins, rep
 

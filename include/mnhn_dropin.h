@@ -79,8 +79,41 @@ cluster_connections* generate_split_set_relation(split_set ancient, split_set ne
 /* cluster_io.c:722-729. */
 void free_split_set_and_associated_clusters(split_set s);
 
+/* ---- callers of score() around the path (comparison.h, filter.h, dataset.h) ----
+   Two datasets are scored in one pass on the GPU; results equal the
+   reference's single-threaded results (n_threads only sets the reference's
+   thread count and is ignored here). */
+
+/* comparison.c:84-112: n1 x n2 distances, row i = ds_one[i]; malloc'd. */
+unsigned long* smith_waterman_distances_matrix(dataset ds_one, dataset ds_two);
+/* comparison.c:156-193: mean distance over ds_one x ds_two. */
+double mean_from_smith_waterman_datasets(dataset ds_one, dataset ds_two, size_t n_threads);
+/* comparison.c:241-280: sqrt(sum of the integer parts of (d - mean)^2) / (n1 + n2). */
+double sigma_from_smith_waterman_datasets(double mean, dataset ds_one, dataset ds_two, size_t n_threads);
+/* comparison.c:20-82, 282-323: mean silhouette of ds_one against ds_two. */
+double silhouette_from_smith_waterman_datasets(dataset ds_one, dataset ds_two, size_t n_threads);
+/* comparison.c:325-350, 388-403: statistics of a caller's matrix (host). */
+double mean_from_smith_waterman_distance_matrix(unsigned long* matrix, dataset ds_one, dataset ds_two);
+double sigma_from_smith_waterman_distance_matrix(unsigned long* matrix, double mean, dataset ds_one,
+                                                 dataset ds_two);
+void shortest_longest_distance_in_matrix(unsigned long* matrix, unsigned long* shortest, unsigned long* largest,
+                                         dataset ds_one, dataset ds_two);
+/* comparison.c:352-386: "i j SW L1 L2" lines for every pair j < i (the L2
+   column first, as the reference prints it). */
+void print_SW_PCA_L_comparison(FILE* f, dataset ds);
+/* filter.c:18-50: sequences with size - minus <= length <= size + plus. */
+dataset filter_ds_by_size(dataset in_set, size_t size, size_t plus, size_t minus);
+/* filter.c:52-140: sequences within max_distance of target (one query on the GPU). */
+dataset filter_by_SW_distance(dataset in_set, char* target, size_t target_length, unsigned int max_distance,
+                              int n_threads);
+/* dataset.c:85-110: ">sequence_<j>" records, 50 symbols per line. */
+void dataset_to_fasta(FILE* f, dataset ds);
+/* dataset.c:427-471: `dimensions` floats per sequence into ds->values[dimension][sequence]. */
+void load_projections_from_file_into_dataset(FILE* projections, size_t dimensions, dataset* ds);
+
 /* Status of the last drop-in call that can fail without a return code
-   (adaptive_dbscan, dbscan_SW, score): 0 on success, else an swe_status. */
+   (adaptive_dbscan, dbscan_SW, score and the calls above): 0 on success, else
+   an swe_status. */
 int swgpu_last_dropin_status(void);
 
 #ifdef __cplusplus

@@ -105,6 +105,17 @@ swe_status swe_score_all_pairs(swe_ctx* ctx);
 /* n_s x n_s distance matrix of one set (n_s = its size), row-major in the
    set's index order. */
 swe_status swe_copy_set_distances(swe_ctx* ctx, int set, uint32_t* out);
+/* Rows [row0, row1) of that matrix ((row1-row0) x n_s entries). */
+swe_status swe_copy_set_rows(swe_ctx* ctx, int set, int row0, int row1, uint32_t* out);
+
+/* Statistics of the block rows [r0, r1) x columns [c0, c1) of one set's
+   distance matrix (indices inside the set), without copying it: per row the
+   sum of the distances (row_sum) and the sum of floor((d - mean)^2) with each
+   square rounded once in double (row_sqdev), both r1-r0 entries or NULL, and
+   the block's smallest and largest distance.  The reductions of
+   comparison.c:84-403 (mean, sigma, silhouette, extremes) are built on it. */
+swe_status swe_block_stats(swe_ctx* ctx, int set, int r0, int r1, int c0, int c1, double mean, uint64_t* row_sum,
+                           uint64_t* row_sqdev, uint32_t* min, uint32_t* max);
 
 /* Copies the n x n distance matrix to host memory (out holds n*n entries). */
 swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out);

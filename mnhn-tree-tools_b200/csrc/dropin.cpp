@@ -97,6 +97,16 @@ split_set dbscan_locked(const dataset& ds, float epsilon, int minpts) {
 
 }  // namespace
 
+namespace swgpu {
+
+std::mutex& dropin_mutex() { return g_mu; }
+swe_ctx* dropin_ctx() { return default_ctx(); }
+int dropin_scored(swe_ctx* ctx, const dataset& ds) { return ensure_scored(ctx, ds); }
+void dropin_forget() { g_have = false; }
+void dropin_set_status(int s) { g_status = s; }
+
+}  // namespace swgpu
+
 extern "C" {
 
 int swgpu_last_dropin_status(void) { return g_status; }

@@ -674,27 +674,34 @@ static const uint32_t* set_D32(const swe_ctx* ctx, int s) {
   return ctx->d_D32.p ? ctx->d_D32.p + ctx->set_base[s] : nullptr;
 }
 
-swe_status swe_copy_set_distances(swe_ctx* ctx, int s, uint32_t* out) {
+swe_status swe_copy_set_rows(swe_ctx* ctx, int s, int row0, int row1, uint32_t* out) {
   if (!ctx) return SWE_ERR_INVALID;
   if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
   if (s < 0 || s >= ctx->n_sets) return fail(ctx, SWE_ERR_INVALID, "no such set");
   if (swe_status st = select_device(ctx)) return st;
   const int first = ctx->set_first[s], ns = ctx->set_first[s + 1] - first;
-  if (ns == 0) return SWE_OK;
+  if (row0 < 0 || row1 < row0 || row1 > ns) return fail(ctx, SWE_ERR_INVALID, "bad row range");
+  if (ns == 0 || row1 == row0) return SWE_OK;
   if (!out) return SWE_ERR_INVALID;
   // rows in original order, in chunks of about 64 Mi entries
-  const int rows = (int)std::max<long long>(1, std::min<long long>(ns, (64LL << 20) / ns));
+  const int rows = (int)std::max<long long>(1, std::min<long long>(row1 - row0, (64LL << 20) / ns));
   DevBuf<uint32_t> tmp;
   CK(tmp.alloc((size_t)rows * ns));
-  for (int r0 = 0; r0 < ns; r0 += rows) {
-    const int r1 = std::min(ns, r0 + rows);
+  for (int r0 = row0; r0 < row1; r0 += rows) {
+    const int r1 = std::min(row1, r0 + rows);
     ctx->stats.kernel_launches += 1;
     CK(launch_unpermute_set(set_D16(ctx, s), set_D32(ctx, s), ctx->d_pos.p + first, ns, r0, r1, tmp.p, ctx->st));
-    CK(cpy(ctx, out + (size_t)r0 * ns, tmp.p, sizeof(uint32_t) * (size_t)(r1 - r0) * ns, cudaMemcpyDeviceToHost,
-           ctx->st));
+    CK(cpy(ctx, out + (size_t)(r0 - row0) * ns, tmp.p, sizeof(uint32_t) * (size_t)(r1 - r0) * ns,
+           cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
   }
   return SWE_OK;
+}
+
+swe_status swe_copy_set_distances(swe_ctx* ctx, int s, uint32_t* out) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (s < 0 || s >= ctx->n_sets) return fail(ctx, SWE_ERR_INVALID, "no such set");
+  return swe_copy_set_rows(ctx, s, 0, ctx->set_first[s + 1] - ctx->set_first[s], out);
 }
 
 swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out) {
@@ -702,6 +709,35 @@ swe_status swe_copy_distances(swe_ctx* ctx, uint32_t* out) {
   if (ctx->n_sets > 1) return fail(ctx, SWE_ERR_STATE, "several sets uploaded: use swe_copy_set_distances");
   if (ctx->n == 0) return SWE_OK;
   return swe_copy_set_distances(ctx, 0, out);
+}
+
+swe_status swe_block_stats(swe_ctx* ctx, int set, int r0, int r1, int c0, int c1, double mean, uint64_t* row_sum,
+                           uint64_t* row_sqdev, uint32_t* min, uint32_t* max) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (set < 0 || set >= ctx->n_sets) return fail(ctx, SWE_ERR_INVALID, "no such set");
+  const int first = ctx->set_first[set], ns = ctx->set_first[set + 1] - first;
+  if (r0 < 0 || r1 < r0 || r1 > ns || c0 < 0 || c1 < c0 || c1 > ns) return fail(ctx, SWE_ERR_INVALID, "bad block");
+  if (swe_status st = select_device(ctx)) return st;
+  const int rows = r1 - r0;
+  DevBuf<unsigned long long> dsum, dsq;
+  DevBuf<unsigned> mm;
+  CK(dsum.alloc(std::max(rows, 1)));
+  CK(dsq.alloc(std::max(rows, 1)));
+  CK(mm.alloc(2));
+  const unsigned init[2] = {0xFFFFFFFFu, 0u};
+  CK(cpy(ctx, mm.p, init, sizeof(init), cudaMemcpyHostToDevice, ctx->st));
+  ctx->stats.kernel_launches += 1;
+  CK(launch_block_stats(set_D16(ctx, set), set_D32(ctx, set), ctx->d_pos.p + first, ns, r0, r1, c0, c1, mean,
+                        dsum.p, dsq.p, mm.p, mm.p + 1, ctx->st));
+  unsigned hm[2] = {0, 0};
+  if (row_sum && rows) CK(cpy(ctx, row_sum, dsum.p, sizeof(uint64_t) * rows, cudaMemcpyDeviceToHost, ctx->st));
+  if (row_sqdev && rows) CK(cpy(ctx, row_sqdev, dsq.p, sizeof(uint64_t) * rows, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cpy(ctx, hm, mm.p, sizeof(hm), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (min) *min = hm[0];
+  if (max) *max = hm[1];
+  return SWE_OK;
 }
 
 }  // extern "C"

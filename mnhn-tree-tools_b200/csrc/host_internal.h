@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <functional>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -115,5 +116,15 @@ swe_status score_raw(swe_ctx* ctx, const char* A, size_t la, const char* B, size
 // The eps printed for kept layer i (dbscan.c:1323-1324):
 // epsilon_start + (i+1) * (float)epsilon_inc, evaluated in float.
 float layer_eps(float eps_start, int i, float eps_inc);
+
+// The drop-in layer's process-wide context (dropin.cpp): its lock, the
+// context itself (null without a device), "make sure ds is uploaded and
+// scored" (cached by content), forgetting that cache after another upload,
+// and the status swgpu_last_dropin_status() reports.
+std::mutex& dropin_mutex();
+swe_ctx* dropin_ctx();
+int dropin_scored(swe_ctx* ctx, const dataset& ds);
+void dropin_forget();
+void dropin_set_status(int s);
 
 }  // namespace swgpu

@@ -679,6 +679,69 @@ cudaError_t launch_unpermute_set(const uint16_t* D16set, const uint32_t* D32set,
   return cudaGetLastError();
 }
 
+// Statistics of a block of one set's matrix (original indices): one CTA per
+// row of [r0, r1) over the columns [c0, c1).
+template <typename DT>
+__global__ void __launch_bounds__(256) block_stats_kernel(const DT* __restrict__ Dset, const int* __restrict__ pos,
+                                                          int ns, int r0, int r1, int c0, int c1, double mean,
+                                                          unsigned long long* __restrict__ row_sum,
+                                                          unsigned long long* __restrict__ row_sqdev,
+                                                          unsigned* bmin, unsigned* bmax) {
+  __shared__ unsigned long long s_sum[8], s_sq[8];
+  __shared__ unsigned s_min[8], s_max[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int i = r0 + blockIdx.x; i < r1; i += gridDim.x) {
+    const DT* row = Dset + (long long)pos[i] * ns;
+    unsigned long long sum = 0, sq = 0;
+    unsigned mn = 0xFFFFFFFFu, mx = 0u;
+    for (int k = c0 + threadIdx.x; k < c1; k += blockDim.x) {
+      const unsigned v = row[pos[k]];
+      sum += v;
+      const double d = (double)v - mean;
+      sq += (unsigned long long)floor(__dmul_rn(d, d));  // no contraction into a later add
+      mn = min(mn, v);
+      mx = max(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+      sq += __shfl_xor_sync(0xFFFFFFFFu, sq, o);
+      mn = min(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+      mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    }
+    if (lane == 0) s_sum[warp] = sum, s_sq[warp] = sq, s_min[warp] = mn, s_max[warp] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int w = 1; w < nwarps; ++w) {
+        sum += s_sum[w];
+        sq += s_sq[w];
+        mn = min(mn, s_min[w]);
+        mx = max(mx, s_max[w]);
+      }
+      if (row_sum) row_sum[i - r0] = sum;
+      if (row_sqdev) row_sqdev[i - r0] = sq;
+      if (c1 > c0) {
+        atomicMin(bmin, mn);
+        atomicMax(bmax, mx);
+      }
+    }
+    __syncthreads();  // s_* are reused by the next row
+  }
+}
+
+cudaError_t launch_block_stats(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s, int r0,
+                               int r1, int c0, int c1, double mean, unsigned long long* row_sum,
+                               unsigned long long* row_sqdev, unsigned* bmin, unsigned* bmax, cudaStream_t st) {
+  if (n_s <= 0 || r1 <= r0) return cudaSuccess;
+  const int grid = min(r1 - r0, 148 * 8);
+  if (D16set)
+    block_stats_kernel<uint16_t><<<grid, 256, 0, st>>>(D16set, pos, n_s, r0, r1, c0, c1, mean, row_sum, row_sqdev,
+                                                       bmin, bmax);
+  else
+    block_stats_kernel<uint32_t><<<grid, 256, 0, st>>>(D32set, pos, n_s, r0, r1, c0, c1, mean, row_sum, row_sqdev,
+                                                       bmin, bmax);
+  return cudaGetLastError();
+}
+
 __global__ void __launch_bounds__(256) csr_fill_kernel(const uint64_t* __restrict__ bits, int n, int wpr,
                                                        const long long* __restrict__ row_ptr,
                                                        int* __restrict__ cols) {

@@ -151,6 +151,13 @@ struct ThrPlan {
 };
 ThrPlan threshold_plan(int max_n_s, int dist_bytes);
 cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const ThrPlan& plan, cudaStream_t st);
+// Block [r0, r1) x [c0, c1) (original indices) of one set's matrix: per row the
+// sum of the distances and the sum of floor((d - mean)^2) (each square rounded
+// once in double), over the block the minimum and maximum (atomicMin / Max on
+// *bmin / *bmax, which the caller initialises).
+cudaError_t launch_block_stats(const uint16_t* D16set, const uint32_t* D32set, const int* pos, int n_s, int r0,
+                               int r1, int c0, int c1, double mean, unsigned long long* row_sum,
+                               unsigned long long* row_sqdev, unsigned* bmin, unsigned* bmax, cudaStream_t st);
 // CSR from a bitmap: ascending column indices per row at row_ptr[i].
 cudaError_t launch_csr_fill(const uint64_t* bits, int n, int words_per_row, const long long* row_ptr,
                             int* cols, cudaStream_t st);

@@ -303,11 +303,44 @@ def kmer_golden():
     (OUT / "kmer_counts.json").write_text(json.dumps(cases))
 
 
+def score_callers_golden():
+    """stdout of the reference's compareSW, silhouette, compare_norms and
+    find_satellite (built from its sources into oracle/_ref, one thread) on
+    seeded inputs: two families sets for the comparisons, projections with six
+    decimals, a satellite filter with a size window and a distance bound."""
+    rng = np.random.default_rng(91)
+    one = small_family_set(91, 3, 20, 180)
+    two = small_family_set(92, 2, 15, 200)
+    one += [rand_seq(rng, int(rng.integers(60, 260))) for _ in range(5)]
+    two += [with_n_runs(rng, rand_seq(rng, int(rng.integers(60, 260)))) for _ in range(5)]
+    proj = rng.normal(0, 3, size=(len(one), 3))
+    proj_text = "".join(" ".join(f"{v:.6f}" for v in row) + "\n" for row in proj)
+    target = one[0]
+    runs = []
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        W.write_fasta(d / "one.fa", one)
+        W.write_fasta(d / "two.fa", two)
+        W.write_fasta(d / "target.fa", [target])
+        (d / "proj.txt").write_text(proj_text)
+        cases = [("compareSW", ["one.fa", "two.fa", "1"]), ("silhouette", ["one.fa", "two.fa", "1"]),
+                 ("silhouette", ["two.fa", "one.fa", "1"]), ("compare_norms", ["one.fa", "proj.txt", "3"]),
+                 ("find_satellite", ["one.fa", "target.fa", "180", "30", "40", "400", "1"]),
+                 ("find_satellite", ["one.fa", "target.fa", "100", "500", "90", "5000", "1"])]
+        for tool, args in cases:
+            rc, out = run_tool(tool, args, d)
+            assert rc == 0, (tool, out[-500:])
+            runs.append({"tool": tool, "args": args, "stdout": out})
+    doc = {"one": [s.decode("latin-1") for s in one], "two": [s.decode("latin-1") for s in two],
+           "target": target.decode("latin-1"), "proj": proj_text, "runs": runs}
+    (OUT / "score_callers.json").write_text(json.dumps(doc))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         O.build()
     which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
-                             "kmer"]
+                             "kmer", "callers"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -326,3 +359,5 @@ if __name__ == "__main__":
         subset_goldens()
     if "kmer" in which:
         kmer_golden()
+    if "callers" in which:
+        score_callers_golden()

@@ -457,6 +457,57 @@ def test_reference_mains_linked_on_libswgpu(tmp_path):
         assert (tmp_path / "o.fa").read_text() == run["out"]
 
 
+def test_score_callers_linked_on_libswgpu(tmp_path):
+    """The reference's compareSW.c, silhouette.c, compare_norms.c and
+    find_satellite.c (the other callers of score(): comparison.c, filter.c),
+    linked against libswgpu, print byte for byte what the reference tools
+    print (golden stdout, one thread)."""
+    doc = load_golden("score_callers.json")
+    W.write_fasta(tmp_path / "one.fa", [s.encode("latin-1") for s in doc["one"]])
+    W.write_fasta(tmp_path / "two.fa", [s.encode("latin-1") for s in doc["two"]])
+    W.write_fasta(tmp_path / "target.fa", [doc["target"].encode("latin-1")])
+    (tmp_path / "proj.txt").write_text(doc["proj"])
+    for run in doc["runs"]:
+        r = subprocess.run([str(_ref_main(run["tool"]))] + run["args"], cwd=tmp_path, capture_output=True,
+                           timeout=600)
+        assert r.returncode == 0, (run["tool"], r.stderr.decode()[-500:])
+        assert r.stdout.decode("latin-1") == run["stdout"], (run["tool"], run["args"])
+
+
+def test_comparison_statistics_match_oracle(eng):
+    """mean / sigma / silhouette / matrix through the C ABI against the same
+    quantities computed from the oracle's distances (larger sets than the
+    golden case, uneven sizes)."""
+    import ctypes as C
+    pool, _ = W.config2(n=900, seed=40)
+    one, two = pool[:530], pool[530:]
+    D = O.all_pairs(pool)
+    cross = D[:530, 530:].astype(np.float64)
+    L = swgpu.lib()
+    for name in ("mean_from_smith_waterman_datasets", "silhouette_from_smith_waterman_datasets"):
+        getattr(L, name).restype = C.c_double
+        getattr(L, name).argtypes = [swgpu.Dataset, swgpu.Dataset, C.c_size_t]
+    L.sigma_from_smith_waterman_datasets.restype = C.c_double
+    L.sigma_from_smith_waterman_datasets.argtypes = [C.c_double, swgpu.Dataset, swgpu.Dataset, C.c_size_t]
+    L.smith_waterman_distances_matrix.restype = C.POINTER(C.c_ulong)
+    L.smith_waterman_distances_matrix.argtypes = [swgpu.Dataset, swgpu.Dataset]
+    b1, b2 = swgpu.SeqBuffer(one), swgpu.SeqBuffer(two)
+    mean = L.mean_from_smith_waterman_datasets(b1.dataset(), b2.dataset(), 4)
+    assert mean == cross.sum() / (530.0 * 370.0)
+    sigma = L.sigma_from_smith_waterman_datasets(mean, b1.dataset(), b2.dataset(), 4)
+    want = np.sqrt(np.floor((cross - mean) * (cross - mean)).sum()) / 900
+    assert sigma == pytest.approx(want, rel=1e-12)
+    sil = L.silhouette_from_smith_waterman_datasets(b1.dataset(), b2.dataset(), 4)
+    a = D[:530, :530].sum(axis=1) / 529.0
+    b = cross.sum(axis=1) / 370.0
+    s = np.where(a < b, 1 - a / b, np.where(a > b, b / a - 1, 0.0))
+    assert sil == pytest.approx(s.sum() / 530, rel=1e-12)
+    m = L.smith_waterman_distances_matrix(b1.dataset(), b2.dataset())
+    got = np.ctypeslib.as_array(m, shape=(530 * 370,)).reshape(530, 370).copy()
+    swgpu.lib().swe_free(C.cast(m, C.c_void_p))
+    assert np.array_equal(got, D[:530, 530:])
+
+
 # ---------------------------------------------------------------------------
 # size-independent properties at the full config-2 size
 # ---------------------------------------------------------------------------

@@ -2,9 +2,9 @@
  * Drop-in entry points: the functions of MNHN-Tree-Tools' Smith-Waterman path,
  * with the reference's names and CPU-build signatures, exported by
  * libswgpu.so.  A caller written against the reference (cluster_dbscan_SW.c,
- * adaptive_clustering.c, find_closest_sequence_SW.c, filter.c, comparison.c)
- * links against libswgpu.so instead of smith_waterman.o, dbscan_SW.o,
- * dataset.o and cluster_io.o.  All distance work runs on the GPU; there is no
+ * adaptive_clustering.c, find_closest_sequence_SW.c, filter.c, comparison.c,
+ * fasta2kmer.c) links against libswgpu.so instead of smith_waterman.o,
+ * dbscan_SW.o, dataset.o, cluster_io.o and kmers.o.  All distance work runs on the GPU; there is no
  * CPU fallback.  When no usable GPU is present the functions print an error
  * and return the empty result documented below.
  *
@@ -110,6 +110,20 @@ dataset filter_by_SW_distance(dataset in_set, char* target, size_t target_length
 void dataset_to_fasta(FILE* f, dataset ds);
 /* dataset.c:427-471: `dimensions` floats per sequence into ds->values[dimension][sequence]. */
 void load_projections_from_file_into_dataset(FILE* projections, size_t dimensions, dataset* ds);
+
+/* ---- fasta2kmer (kmers.h) ---- */
+
+/* kmers.c:292-371: one row of swe_kmer_count(kmer_length, protein) counts per
+   sequence (malloc'd rows), computed on the GPU over strlen(sequence) bytes;
+   semantics of swe_kmer_counts.  n_threads is ignored.  kmer_length must be
+   1..15 (DNA) or 1..7 (protein); otherwise, or on a GPU error, the result has
+   frequencies == NULL and n_seq == 0. */
+kmer_frequencies frequencies_from_dataset(dataset ds, size_t kmer_length, int n_threads, int protein);
+/* kmers.c:373-385: "sequence_<i>" and the row's counts as "%hi", tab
+   separated, one line per sequence; the text is formatted on the GPU. */
+void write_kmer_base(FILE* f, kmer_frequencies freq);
+/* kmers.c:387-396. */
+void free_kmer_frequencies(kmer_frequencies freq);
 
 /* Status of the last drop-in call that can fail without a return code
    (adaptive_dbscan, dbscan_SW, score and the calls above): 0 on success, else

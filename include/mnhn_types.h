@@ -7,6 +7,7 @@
  *   split_set            cluster.h:20-23
  *   cluster_connections  cluster.h:28-31
  *   neighbors            dbscan.h:5-8
+ *   kmer_frequencies     kmers.h:17-21
  *
  * Ownership follows the reference: arrays inside returned structs come from
  * malloc and are released with free() (free_split_set_and_associated_clusters,
@@ -51,6 +52,14 @@ typedef struct {
   int* members;   /* ascending dataset indices, the query point included */
   int n_members;
 } neighbors;
+
+/* kmers.h:17-21: frequencies[sequence][k-mer index], one malloc'd row per
+   sequence (free_kmer_frequencies releases them). */
+typedef struct {
+  short int** frequencies;
+  size_t n_kmers;
+  size_t n_seq;
+} kmer_frequencies;
 
 #ifdef __cplusplus
 }

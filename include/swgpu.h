@@ -52,6 +52,8 @@ typedef struct {
                           (bulk-copied rows, double-buffered), 1 = rows read
                           from global memory, 2 = positions staged in shared
                           memory too, 3 = one bulk-copy row buffer */
+  int kmer_batch_kb;   /* test hook: device batch of the k-mer calls in KB
+                          (0 = 1 GB of counts and 256 MB of text) */
 } swe_opts;
 
 typedef struct {
@@ -309,6 +311,43 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
    M and N multiples of 128, K a multiple of 64. */
 swe_status swe_gemm_bf16(int device, const void* A, const void* B, int M, int N, int K, const float* bias, int act,
                          float* C);
+
+/* ------------------------------------------------------------------------
+   k-mer frequency tables of fasta2kmer (kmers.c:157-389).  Independent of
+   the uploaded dataset: sequences are passed in and counted on the GPU.
+   ------------------------------------------------------------------------ */
+
+#define SWE_KMER_MAX_DNA 15     /* gen_dna_kmers builds its table with int shifts (kmers.c:87-107) */
+#define SWE_KMER_MAX_PROTEIN 7  /* 20^7 counts per sequence; longer k-mers exceed any row the reference allocates */
+
+/* Number of k-mers: 4^k (kmers.c:65-73) or 20^k with protein != 0
+   (kmers.c:75-83); 0 when k is outside 1..SWE_KMER_MAX_DNA / _PROTEIN. */
+int64_t swe_kmer_count(int k, int protein);
+
+/* Counts of every k-mer in the sequences seqs[i], len[i] bytes each (the
+   caller passes strlen, kmers.c:162).  Semantics of
+   frequence_of_kmer_in_sequence (kmers.c:157-241) for each table entry:
+   windows start at 0 .. len-k-1 (the window ending at the last symbol is never
+   counted, and len <= k gives all zeros), symbols compare as raw bytes
+   against 'A','C','G','T' (index bits 2p..2p+1 = symbol p, A0 C1 G2 T3,
+   kmers.c:26-107) or, with protein != 0, against the 20 letters
+   ACDEFGHIKLMNPQRSTVWY (index = base-20 number with symbol 0 most
+   significant, kmers.c:109-155), and a count keeps the low 16 bits of the
+   true count as a signed short.  Row i of the result goes to rows[i]
+   (swe_kmer_count(k, protein) shorts). */
+swe_status swe_kmer_counts(swe_ctx* ctx, const char* const* seqs, const int64_t* len, int64_t n, int k, int protein,
+                           int16_t* const* rows);
+
+/* Receives consecutive pieces of a text; returns 0 to go on, else stops the
+   producer (which then returns SWE_ERR_IO). */
+typedef int (*swe_text_sink)(const char* data, size_t size, void* user);
+
+/* The text write_kmer_base prints for a frequency table (kmers.c:373-385):
+   per row i "sequence_<i>" then each count as "%hi", separated by tabs,
+   ending in a newline.  The digits are formatted on the GPU; the text is
+   handed to `sink` in pieces in order. */
+swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int64_t nk, swe_text_sink sink,
+                        void* user);
 
 void swe_free(void* p);
 

@@ -139,6 +139,7 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
   }
   if (opts && opts->inject_timeout) ctx->inject_timeout = 1;
   if (opts && opts->threshold_path >= 0 && opts->threshold_path <= 3) ctx->threshold_path = opts->threshold_path;
+  if (opts && opts->kmer_batch_kb > 0) ctx->kmer_batch_bytes = (size_t)opts->kmer_batch_kb << 10;
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
   for (auto& ev : ctx->ev)

@@ -63,6 +63,8 @@ struct HostPinned {
 
 struct PrefilterState;
 void prefilter_destroy(PrefilterState* pf);
+struct KmerState;
+void kmer_state_destroy(KmerState* km);
 
 }  // namespace swgpu
 
@@ -77,6 +79,7 @@ struct swe_ctx {
   int threads = 256;
   int inject_timeout = 0;
   int threshold_path = 0;
+  size_t kmer_batch_bytes = 0;  // k-mer calls' device batch (0 = their defaults)
   int graph_kernels = 0;
   std::string err;
 
@@ -171,10 +174,13 @@ struct swe_ctx {
 
   // learned prefilter (null until first used)
   swgpu::PrefilterState* pf = nullptr;
+  // k-mer tables: device buffers and pinned staging (null until first used)
+  swgpu::KmerState* km = nullptr;
 
   ~swe_ctx() {
     cudaSetDevice(device);
     swgpu::prefilter_destroy(pf);
+    swgpu::kmer_state_destroy(km);
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);

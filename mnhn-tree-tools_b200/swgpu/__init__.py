@@ -58,7 +58,7 @@ class SplitSet(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("sat_limit", C.c_int), ("packs_per_block", C.c_int),
                 ("threads", C.c_int), ("inject_timeout", C.c_int),
-                ("threshold_path", C.c_int)]
+                ("threshold_path", C.c_int), ("kmer_batch_kb", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -107,6 +107,13 @@ class SweepResult(C.Structure):
 
 
 DBSCANNER = C.CFUNCTYPE(SplitSet, Dataset, C.c_float, C.c_int)
+TEXT_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+class KmerFrequencies(C.Structure):
+    # kmers.h:17-21
+    _fields_ = [("frequencies", C.POINTER(C.POINTER(C.c_short))), ("n_kmers", C.c_size_t),
+                ("n_seq", C.c_size_t)]
 
 # Every symbol the public headers declare (checked by the CPU test suite).
 EXPORTS = [
@@ -120,11 +127,13 @@ EXPORTS = [
     "swe_kmer_features", "swe_prefilter_init", "swe_prefilter_param_count", "swe_prefilter_params",
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
+    "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
     "data_not_in_clusters", "intersection_of_clusters", "generate_split_set_relation",
     "free_split_set_and_associated_clusters", "swgpu_last_dropin_status",
+    "frequencies_from_dataset", "write_kmer_base", "free_kmer_frequencies",
 ]
 
 _lib = None
@@ -230,6 +239,19 @@ def lib():
         L.read_split_set.restype = SplitSet
         L.read_split_set.argtypes = [C.c_char_p]
         L.swgpu_last_dropin_status.restype = C.c_int
+        L.swe_kmer_count.restype = C.c_int64
+        L.swe_kmer_count.argtypes = [C.c_int, C.c_int]
+        L.swe_kmer_counts.restype = C.c_int
+        L.swe_kmer_counts.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                      C.c_void_p]
+        L.swe_kmer_tsv.restype = C.c_int
+        L.swe_kmer_tsv.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, TEXT_SINK, C.c_void_p]
+        L.frequencies_from_dataset.restype = KmerFrequencies
+        L.frequencies_from_dataset.argtypes = [Dataset, C.c_size_t, C.c_int, C.c_int]
+        L.write_kmer_base.restype = None
+        L.write_kmer_base.argtypes = [C.c_void_p, KmerFrequencies]
+        L.free_kmer_frequencies.restype = None
+        L.free_kmer_frequencies.argtypes = [KmerFrequencies]
         _lib = L
     return _lib
 
@@ -264,9 +286,9 @@ class Engine:
     """One engine context (one CUDA stream on one device)."""
 
     def __init__(self, device: int = 0, sat_limit: int = 0, packs_per_block: int = 0, threads: int = 0,
-                 inject_timeout: int = 0, threshold_path: int = 0):
+                 inject_timeout: int = 0, threshold_path: int = 0, kmer_batch_kb: int = 0):
         self.ctx = C.c_void_p()
-        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path)
+        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path, kmer_batch_kb)
         _check(lib().swe_create(C.byref(self.ctx), C.byref(opts)))
         self.n = 0
         self._buf = None
@@ -396,6 +418,40 @@ class Engine:
                         "done_ms": r.done_ms})
         lib().swe_free_sweep_results(res, S)
         return out
+
+    # ---------------------------------------------------------------- fasta2kmer
+    @staticmethod
+    def _row_ptrs(table: np.ndarray):
+        n, nk = table.shape
+        base = table.ctypes.data
+        return (C.c_void_p * max(1, n))(*[base + i * nk * 2 for i in range(n)])
+
+    def kmer_counts(self, seqs, k: int, protein: bool = False) -> np.ndarray:
+        """k-mer frequency table of frequencies_from_dataset (kmers.c:292-371)
+        over len(s) bytes of each sequence: int16 array (n, 4^k or 20^k)."""
+        nk = lib().swe_kmer_count(k, int(bool(protein)))
+        if nk == 0:
+            raise SwgpuError(1, "k-mer length out of range")
+        buf = SeqBuffer(seqs)
+        n = len(seqs)
+        out = np.zeros((n, nk), dtype=np.int16)
+        lens = (C.c_int64 * max(1, n))(*[len(s) for s in seqs])
+        _check(lib().swe_kmer_counts(self.ctx, buf.ptrs, lens, n, k, int(bool(protein)), self._row_ptrs(out)),
+               self.ctx)
+        return out
+
+    def kmer_tsv(self, table: np.ndarray) -> bytes:
+        """The text write_kmer_base (kmers.c:373-385) prints for a table."""
+        t = np.ascontiguousarray(table, dtype=np.int16)
+        chunks = []
+
+        @TEXT_SINK
+        def sink(data, size, _user):
+            chunks.append(C.string_at(data, size))
+            return 0
+
+        _check(lib().swe_kmer_tsv(self.ctx, self._row_ptrs(t), t.shape[0], t.shape[1], sink, None), self.ctx)
+        return b"".join(chunks)
 
     # ---------------------------------------------------------------- prefilter
     def kmer_features(self, k: int = 5) -> np.ndarray:

@@ -63,6 +63,7 @@ def lib():
                                      C.POINTER(C.c_void_p), C.POINTER(C.c_int)]
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_kmer_counts.argtypes = [C.c_char_p, C.c_size_t, C.c_int, C.c_void_p]
+        L.orc_kmer_frequencies.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -166,6 +167,25 @@ def kmer_counts(seq: bytes, k: int) -> np.ndarray:
     out = np.zeros(4 ** k, dtype=np.int16)
     lib().orc_kmer_counts(bytes(seq), len(seq), k, out.ctypes.data)
     return out
+
+
+def kmer_table(seqs, k: int, protein: bool = False) -> np.ndarray:
+    """frequencies_from_dataset (kmers.c:292-371) over NUL-terminated
+    sequences: one int16 row of 4^k (or 20^k) counts per sequence."""
+    nk = (20 if protein else 4) ** k
+    out = np.zeros((len(seqs), nk), dtype=np.int16)
+    for i, s in enumerate(seqs):
+        lib().orc_kmer_frequencies(bytes(s), k, int(bool(protein)), out[i].ctypes.data)
+    return out
+
+
+def kmer_tsv(table: np.ndarray) -> bytes:
+    """write_kmer_base (kmers.c:373-385): "sequence_%i" then "%hi" counts,
+    tab separated, one line per row."""
+    lines = []
+    for i, row in enumerate(np.asarray(table, dtype=np.int16)):
+        lines.append("sequence_%d\t" % i + "\t".join(str(int(v)) for v in row) + "\n")
+    return "".join(lines).encode()
 
 
 # --------------------------------------------------------------------------

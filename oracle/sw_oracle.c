@@ -340,3 +340,41 @@ void orc_kmer_counts(const char* s, size_t len, int k, int16_t* out) {
     if (ok) out[idx]++;
   }
 }
+
+/* The frequency row of frequencies_from_dataset (kmers.c:292-371) for one
+   NUL-terminated sequence: entry b counts the windows that equal k-mer b in
+   frequence_of_kmer_in_sequence (kmers.c:157-241): sequence length is
+   strlen(s) (kmers.c:162), windows start at 0 .. len-k-1 (kmers.c:172, 230),
+   bytes compare raw.  DNA k-mer b has symbol p = "ACGT"[(b >> 2p) & 3]
+   (gen_dna_string_from_binary, kmers.c:26-63); protein k-mer b is the base-20
+   number over "ACDEFGHIKLMNPQRSTVWY" with symbol 0 most significant (the
+   recursion of kmers.c:109-130, first position outermost).  Counts are kept
+   in a short as the reference does (the low 16 bits, kmers.c:171, 211).
+   This loops over windows, not over the 4^k / 20^k table entries: the same
+   counts, found by decoding each window once.  out[] has 4^k or 20^k
+   entries. */
+void orc_kmer_frequencies(const char* s, int k, int protein, int16_t* out) {
+  static const char dna[] = "ACGT", prot[] = "ACDEFGHIKLMNPQRSTVWY";
+  const char* alpha = protein ? prot : dna;
+  const int base = protein ? 20 : 4;
+  size_t nk = 1;
+  for (int i = 0; i < k; i++) nk *= (size_t)base;
+  memset(out, 0, sizeof(int16_t) * nk);
+  const size_t len = strlen(s);
+  if ((size_t)k > len) return;
+  for (size_t w = 0; w + (size_t)k < len; w++) {
+    size_t idx = 0;
+    int ok = 1;
+    for (int p = 0; p < k && ok; p++) {
+      const char* hit = memchr(alpha, s[w + (size_t)p], (size_t)base);
+      if (!hit || s[w + (size_t)p] == 0) {
+        ok = 0;
+        break;
+      }
+      const size_t c = (size_t)(hit - alpha);
+      if (protein) idx = idx * 20 + c;
+      else idx |= c << (2 * p);
+    }
+    if (ok) out[idx] = (int16_t)(uint16_t)((uint16_t)out[idx] + 1u);
+  }
+}

@@ -57,6 +57,20 @@ def golden():
     return load_golden
 
 
+def fasta2kmer_input(doc, name: str) -> list[bytes]:
+    """Sequences of one input of tests/golden/fasta2kmer.json: literal
+    strings, or {"unit": u, "length": n} for u repeated to n symbols (the rule
+    of make_golden.kmer_inputs)."""
+    out = []
+    for x in doc["inputs"][name]:
+        if isinstance(x, str):
+            out.append(x.encode("latin-1"))
+        else:
+            u = x["unit"]
+            out.append((u * (x["length"] // len(u) + 1))[:x["length"]].encode("latin-1"))
+    return out
+
+
 def gpu_available() -> bool:
     try:
         import torch

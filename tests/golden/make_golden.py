@@ -303,6 +303,67 @@ def kmer_golden():
     (OUT / "kmer_counts.json").write_text(json.dumps(cases))
 
 
+def kmer_inputs(doc):
+    """Sequences of one fasta2kmer_golden input: literal strings, or
+    {"unit": u, "length": n} for u repeated to n symbols."""
+    out = []
+    for x in doc:
+        if isinstance(x, str):
+            out.append(x.encode("latin-1"))
+        else:
+            u = x["unit"]
+            out.append((u * (x["length"] // len(u) + 1))[:x["length"]].encode("latin-1"))
+    return out
+
+
+def fasta2kmer_golden():
+    """stdout of the reference's fasta2kmer (fasta2kmer.c, kmers.c, built from
+    its sources into oracle/_ref) as sha256 + size, on seeded DNA and protein
+    reads (lengths 1..300, N runs, IUPAC and lower-case symbols, symbols outside
+    the alphabet) and on long repeats whose counts pass 32767 and 65535 (the
+    reference keeps them in a short)."""
+    rng = np.random.default_rng(123)
+    dna = [b"A", b"AC", b"ACG", b"ACGT", b"ACGTA", b"ACGTAC", b"ACGTACGT", b"TTTTTTTTT", b"ACGTN" * 7,
+           b"acgtacgtaaccggtt", b"ACGTRYKMACGTACGTAAA"]
+    for L in [15, 16, 17, 31, 33, 64, 100, 180, 300]:
+        dna.append(rand_seq(rng, L))
+    for L in [50, 140, 290]:
+        dna.append(with_n_runs(rng, rand_seq(rng, L), 0.08))
+    for L in [80, 200]:
+        b = bytearray(rand_seq(rng, L))
+        for _ in range(6):
+            b[int(rng.integers(0, L))] = IUPAC[int(rng.integers(0, len(IUPAC)))]
+        dna.append(bytes(b))
+    aa = b"ACDEFGHIKLMNPQRSTVWY"
+    prot = [b"M", b"MK", b"MKV", b"WWWW", b"ACDEFGHIKLMNPQRSTVWY", b"mkvlaagg", b"MXBZU*MKV"]
+    for L in [10, 19, 20, 21, 40, 90, 160, 200]:
+        prot.append(rand_seq(rng, L, aa))
+    for L in [60, 150]:
+        b = bytearray(rand_seq(rng, L, aa))
+        for _ in range(5):
+            b[int(rng.integers(0, L))] = b"XBZJOU"[int(rng.integers(0, 6))]
+        prot.append(bytes(b))
+    long_doc = [{"unit": "A", "length": 66000}, {"unit": "C", "length": 33000},
+                {"unit": "ACGT", "length": 68000}, {"unit": "ACGTTGCA", "length": 70001}]
+    inputs = {"dna": [x.decode("latin-1") for x in dna], "protein": [x.decode("latin-1") for x in prot],
+              "long": long_doc}
+    runs = [("dna", k, 0) for k in (1, 2, 3, 5, 6, 7, 8, 9)] + [("protein", k, 1) for k in (1, 2, 3, 4)] + \
+           [("dna", 3, 1), ("protein", 2, 0)] + [("long", k, 0) for k in (1, 2, 4, 8)] + [("long", 2, 1)]
+    doc = {"inputs": inputs, "runs": []}
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        for name in inputs:
+            seqs = kmer_inputs(inputs[name]) if name == "long" else [x.encode("latin-1") for x in inputs[name]]
+            W.write_fasta(d / (name + ".fa"), seqs)
+        for name, k, protein in runs:
+            r = O.run_ref_tool("fasta2kmer", [name + ".fa", str(k), "4", str(protein)], d)
+            assert r.returncode == 0, (name, k, r.stdout[-300:])
+            doc["runs"].append({"input": name, "k": k, "protein": protein, "bytes": len(r.stdout),
+                                "sha256": hashlib.sha256(r.stdout).hexdigest()})
+            print("fasta2kmer", name, k, protein, len(r.stdout))
+    (OUT / "fasta2kmer.json").write_text(json.dumps(doc, indent=0))
+
+
 def score_callers_golden():
     """stdout of the reference's compareSW, silhouette, compare_norms and
     find_satellite (built from its sources into oracle/_ref, one thread) on
@@ -340,7 +401,7 @@ if __name__ == "__main__":
     if not O.ref_available():
         O.build()
     which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
-                             "kmer", "callers"]
+                             "kmer", "callers", "fasta2kmer"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -361,3 +422,5 @@ if __name__ == "__main__":
         kmer_golden()
     if "callers" in which:
         score_callers_golden()
+    if "fasta2kmer" in which:
+        fasta2kmer_golden()

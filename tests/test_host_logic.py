@@ -27,6 +27,8 @@ def _declared_functions():
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", text, flags=re.M):
             name = m.group(1)
+            if m.group(0).startswith("typedef"):  # function-pointer types
+                continue
             if name not in {"if", "while", "for", "return", "sizeof"}:
                 names.add(name)
     return names

@@ -104,3 +104,31 @@ def test_config1_rows_match_reference_golden():
     R = O.score_rows(seqs, rows).astype("<u2")
     for k, r in enumerate(rows):
         assert zlib.crc32(R[k].tobytes()) == g["row_crc32"][r], r
+
+
+def test_kmer_table_oracle_matches_reference_fasta2kmer(tmp_path):
+    """The oracle's frequency table + text (kmers.c:157-389) reproduces the
+    reference fasta2kmer's stdout byte for byte (sha256) on every golden run:
+    DNA k = 1..9, protein k = 1..4, each alphabet over the other's input, and
+    repeats whose counts pass 32767 and 65535."""
+    from conftest import fasta2kmer_input
+    from swgpu import workloads as W
+    doc = load_golden("fasta2kmer.json")
+    loaded = {}
+    for run in doc["runs"]:
+        name = run["input"]
+        if name not in loaded:
+            p = tmp_path / f"{name}.fa"
+            W.write_fasta(p, fasta2kmer_input(doc, name))
+            loaded[name] = O.fasta_load(p)
+        text = O.kmer_tsv(O.kmer_table(loaded[name], run["k"], bool(run["protein"])))
+        assert len(text) == run["bytes"], run
+        assert hashlib.sha256(text).hexdigest() == run["sha256"], run
+
+
+def test_kmer_table_short_wrap():
+    # counts live in a short (kmers.c:171): 65999 A's -> 463, 32999 C's -> -32537
+    t = O.kmer_table([b"A" * 66000, b"C" * 33000], 1)
+    assert t[0, 0] == 65999 - 65536 and t[1, 1] == 32999 - 65536
+    assert O.kmer_table([b"ACGT"], 4).sum() == 0     # the window ending at the last symbol is skipped
+    assert O.kmer_table([b"ACGTA"], 4)[0, 0b11100100] == 1

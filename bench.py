@@ -19,6 +19,11 @@ buffers (upload, score pass, sweep, results back on the host) every step.
 `--impl reference` times the reference's own CPU score() (compiled from its
 sources into oracle/_ref) on all host cores on a bounded row sample of the
 same workload and prints the same metric from it.
+
+On config 2 the line also carries `fasta2kmer`: the k-mer table and its text
+(fasta2kmer's frequencies_from_dataset + write_kmer_base, k = 5) for the same
+reads through the drop-in C ABI, beside the reference's own two functions on
+all host cores.
 """
 from __future__ import annotations
 
@@ -115,6 +120,67 @@ def reference_sample(seqs, target_s: float = 12.0, threads: int = 0):
             "sample": f"{n_rows} query rows x all {len(seqs)} sequences of the same workload, "
                       f"region_query order (every ordered pair), {cells:.3e} cells"}
     return rate / 1e9, info
+
+
+def fasta2kmer_leg(seqs, k: int = 5, cpu: bool = True, reps: int = 3):
+    """fasta2kmer's two calls (kmers.c:292-385) on the same reads through the
+    drop-in C ABI: frequencies_from_dataset (host sequences in, malloc'd host
+    rows out) and write_kmer_base (text to /dev/null, so the file system is
+    not timed), median of `reps` after one warm-up.  With cpu, the reference's
+    own two functions (oracle/_ref/libref.so) on all host cores, timed the
+    same way (one repetition)."""
+    import ctypes as C
+
+    import swgpu
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    buf = swgpu.SeqBuffer(seqs)
+    ds = buf.dataset()
+
+    def timed(lib_, threads):
+        t0 = time.perf_counter()
+        f = lib_.frequencies_from_dataset(ds, k, threads, 0)
+        t1 = time.perf_counter()
+        fp = libc.fopen(b"/dev/null", b"w")
+        lib_.write_kmer_base(fp, f)
+        libc.fclose(fp)
+        t2 = time.perf_counter()
+        ok = bool(f.frequencies) and f.n_seq == len(seqs)
+        lib_.free_kmer_frequencies(f)
+        if not ok:
+            raise RuntimeError("frequencies_from_dataset failed")
+        return 1e3 * (t1 - t0), 1e3 * (t2 - t1)
+
+    L = swgpu.lib()
+    timed(L, 1)
+    runs = [timed(L, 1) for _ in range(reps)]
+    counts_ms = statistics.median(r[0] for r in runs)
+    text_ms = statistics.median(r[1] for r in runs)
+    out = {"workload": f"fasta2kmer k={k} DNA over the same {len(seqs)} reads ({4 ** k} columns): "
+                       "frequencies_from_dataset + write_kmer_base to /dev/null, host buffers",
+           "counts_ms": round(counts_ms, 2), "text_ms": round(text_ms, 2),
+           "e2e_ms": round(counts_ms + text_ms, 2), "cpu_baseline": None}
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        if (O.REF_DIR / "libref.so").exists():
+            R = O.ref_lib()
+            R.frequencies_from_dataset.restype = swgpu.KmerFrequencies
+            R.frequencies_from_dataset.argtypes = [swgpu.Dataset, C.c_size_t, C.c_int, C.c_int]
+            R.write_kmer_base.restype = None
+            R.write_kmer_base.argtypes = [C.c_void_p, swgpu.KmerFrequencies]
+            R.free_kmer_frequencies.restype = None
+            R.free_kmer_frequencies.argtypes = [swgpu.KmerFrequencies]
+            threads = os.cpu_count() or 1
+            rc, rt = timed(R, threads)
+            out["cpu_baseline"] = {"kind": "reference", "cores": threads, "counts_ms": round(rc, 1),
+                                   "text_ms": round(rt, 1), "e2e_ms": round(rc + rt, 1),
+                                   "sample": "the whole workload, one repetition (write_kmer_base is "
+                                             "single-threaded in the reference)"}
+            out["speedup_e2e"] = round((rc + rt) / (counts_ms + text_ms), 1)
+    return out
 
 
 def run_reference(args):
@@ -382,6 +448,8 @@ def run_gpu(args):
             "clocks": clk,
             "prefilter_speedup": None,
         }
+        if world == 1 and wl["gen"] == "config2" and not args.no_kmer:
+            line["fasta2kmer"] = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     eng.close()
     del flush
@@ -741,6 +809,7 @@ def main():
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
     ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
+    ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer leg")
     ap.add_argument("--weight-decay", type=float, default=0.0, help="config 4: decoupled weight decay of Adam")
     args = ap.parse_args()
     if args.impl == "reference":

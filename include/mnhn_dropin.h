@@ -41,11 +41,23 @@ void free_sequences_from_dataset(dataset ds);
    on the same sequences.  Returns {0, NULL} on a GPU error. */
 split_set dbscan_SW(dataset ds, float epsilon, int minpts);
 
+/* dbscan.h:28-29 / dbscan.c:563-779, 950-1047.  DBSCAN over ds.values
+   (values[dimension][point], n_dimensions x n_values) with the L1 distance
+   (neighbours: d <= epsilon) or the squared L2 distance (d <= epsilon*epsilon),
+   accumulated in float over the dimensions in order as the reference's
+   AVX/FMA build does; same defaults, seed and expansion rules and cluster
+   order as dbscan_SW.  The distances of a point set are computed once on the
+   GPU and reused by later calls on the same values.  Returns {0, NULL} on a
+   GPU error. */
+split_set dbscan_L1(dataset ds, float epsilon, int minpts);
+split_set dbscan_L2(dataset ds, float epsilon, int minpts);
+
 /* dbscan.h:72-81 / dbscan.c:1117-1380.  Adaptive eps sweep: halving search for
    a start with more than one cluster, eps += inc until one cluster remains,
    layers kept when their cluster count strictly drops, log lines on stdout,
-   split sets written to <prefix>%04d.  When `dbscanner` is dbscan_SW the
-   distances are scored once for the whole sweep.  Layers are produced in eps
+   split sets written to <prefix>%04d.  When `dbscanner` is dbscan_SW,
+   dbscan_L1 or dbscan_L2 the distances are computed once for the whole
+   sweep.  Layers are produced in eps
    order whatever `n_threads` is.  Where the reference calls _exit(1) this
    function prints the same message and returns; swgpu_last_dropin_status()
    then returns non-zero. */
@@ -110,6 +122,22 @@ dataset filter_by_SW_distance(dataset in_set, char* target, size_t target_length
 void dataset_to_fasta(FILE* f, dataset ds);
 /* dataset.c:427-471: `dimensions` floats per sequence into ds->values[dimension][sequence]. */
 void load_projections_from_file_into_dataset(FILE* projections, size_t dimensions, dataset* ds);
+
+/* ---- point datasets of the k-mer / PCA DBSCAN tools (dataset.h, cluster.h) ---- */
+
+/* dataset.c:346-381: n_features = tabs in the first line, n_samples =
+   newlines from the end of the first line on. */
+data_shape shape_from_kmer_file(int infile);
+/* dataset.c:384-425: a label then n_features numbers per sample into
+   values[feature][sample] (32-byte aligned rows); other fields zeroed. */
+dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape);
+/* dataset.c:629-635, 646-649. */
+void free_values_from_dataset(dataset ds);
+void free_dataset(dataset ds);
+/* cluster_io.c:343-379: per member its values, "%f" tab separated, one line
+   each; files <prefix>-%03d. */
+void create_single_cluster_file_with_values(char* filename, cluster cl, dataset ds);
+void create_cluster_files_with_values(char* prefix, split_set s, dataset ds);
 
 /* ---- fasta2kmer (kmers.h) ---- */
 

@@ -8,6 +8,7 @@
  *   cluster_connections  cluster.h:28-31
  *   neighbors            dbscan.h:5-8
  *   kmer_frequencies     kmers.h:17-21
+ *   data_shape           dataset.h:37-40
  *
  * Ownership follows the reference: arrays inside returned structs come from
  * malloc and are released with free() (free_split_set_and_associated_clusters,
@@ -27,8 +28,8 @@ typedef struct {
   size_t* sequence_lengths;  /* strlen of each sequence */
   void** binary_sequences;   /* unused on this path */
   int n_values;              /* number of sequences */
-  float** values;            /* unused on this path */
-  int n_dimensions;          /* unused on this path */
+  float** values;            /* values[dimension][point] (k-mer / PCA DBSCAN) */
+  int n_dimensions;          /* number of dimensions of values */
   size_t max_sequence_length;
 } dataset;
 
@@ -52,6 +53,12 @@ typedef struct {
   int* members;   /* ascending dataset indices, the query point included */
   int n_members;
 } neighbors;
+
+/* dataset.h:37-40: columns and rows of a k-mer table file. */
+typedef struct {
+  size_t n_features;
+  size_t n_samples;
+} data_shape;
 
 /* kmers.h:17-21: frequencies[sequence][k-mer index], one malloc'd row per
    sequence (free_kmer_frequencies releases them). */

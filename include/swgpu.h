@@ -100,6 +100,22 @@ swe_status swe_upload_sets(swe_ctx* ctx, const char* const* seqs, const size_t* 
                            const int* set_first, int n_sets);
 int swe_set_count(const swe_ctx* ctx);
 
+/* Point datasets (dbscan_L1 / dbscan_L2, dbscan.c:563-779): n points of
+   `dims` float coordinates with values[d][i] = coordinate d of point i (the
+   reference dataset's values[dimension][point] layout).  The upload computes
+   every pair's distance on the GPU with the reference's float arithmetic
+   (L1: sum over d in order of |a_d - b_d|; L2: squared distance accumulated
+   over d in order with fused multiply-adds, the reference's AVX/FMA build),
+   so the single-set calls below (swe_copy_distances, swe_neighbors,
+   swe_dbscan, swe_adaptive and their _set forms with set 0) work on points
+   with the reference's neighbour test: d <= eps (L1) or d <= eps*eps (L2).
+   swe_copy_distances then returns each distance's float bit pattern;
+   swe_score_all_pairs does nothing; calls that score sequences return
+   SWE_ERR_STATE until the next sequence upload. */
+#define SWE_METRIC_L1 1
+#define SWE_METRIC_L2 2
+swe_status swe_upload_points(swe_ctx* ctx, const float* const* values, int dims, int n, int metric);
+
 /* Scores every pair of the uploaded sequences into the device distance matrix
    (one pass; later neighbour/DBSCAN calls reuse it). */
 swe_status swe_score_all_pairs(swe_ctx* ctx);

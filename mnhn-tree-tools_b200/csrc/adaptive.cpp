@@ -119,7 +119,7 @@ void SweepMachine::next_sweep_batch() {
     const float e = eps_now_;
     eps_now_ = eps_now_ + eps_inc_;
     req_.push_back(e);
-    if ((fixed_ >= 0 && eps_threshold(e) >= fixed_) || !(eps_now_ > e)) {
+    if ((fixed_ >= 0 && (key_ ? key_(e) : eps_threshold(e)) >= fixed_) || !(eps_now_ > e)) {
       terminal_ = true;
       break;
     }
@@ -252,6 +252,7 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
                    const DbscanProvider& prov, bool dbscan_sw_warnings, long long fixed_point,
                    std::vector<split_set>* kept, std::string* err, int max_steps) {
   SweepMachine m(n, eps_start, eps_inc, minpts, max_steps, prov.batch, dbscan_sw_warnings, fixed_point);
+  if (prov.key) m.set_key(prov.key);
   auto flush = [&]() {
     const std::string t = m.take_log();
     if (!t.empty()) fwrite(t.data(), 1, t.size(), log);

@@ -467,6 +467,9 @@ static swe_status upload_sets(swe_ctx* ctx, const char* const* seqs, const size_
   ctx->scored = false;
   ctx->bits_T = LLONG_MIN;
   ctx->bits_set = -1;
+  ctx->metric = 0;
+  ctx->dims = 0;
+  ctx->d_points.release();
   ctx->n = n;
   ctx->len.assign(n, 0);
   ctx->off.assign(n, 0);
@@ -623,6 +626,7 @@ static swe_status build_score_graph(swe_ctx* ctx) {
 
 swe_status swe_score_all_pairs(swe_ctx* ctx) {
   if (!ctx) return SWE_ERR_INVALID;
+  if (ctx->metric != 0) return SWE_OK;  // point distances are computed by the upload
   if (swe_status s = select_device(ctx)) return s;
   if (ctx->masked)  // back from a prefiltered pass: every tile again, longest first
     if (swe_status s = build_layout(ctx, nullptr, nullptr)) return s;
@@ -716,6 +720,7 @@ swe_status swe_block_stats(swe_ctx* ctx, int set, int r0, int r1, int c0, int c1
                            uint64_t* row_sqdev, uint32_t* min, uint32_t* max) {
   if (!ctx) return SWE_ERR_INVALID;
   if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = need_sequences(ctx)) return s;
   if (set < 0 || set >= ctx->n_sets) return fail(ctx, SWE_ERR_INVALID, "no such set");
   const int first = ctx->set_first[set], ns = ctx->set_first[set + 1] - first;
   if (r0 < 0 || r1 < r0 || r1 > ns || c0 < 0 || c1 < c0 || c1 > ns) return fail(ctx, SWE_ERR_INVALID, "bad block");
@@ -880,7 +885,7 @@ static swe_status check_set(swe_ctx* ctx, int s) {
 swe_status swe_neighbors_set(swe_ctx* ctx, int set, float eps, int64_t** row_ptr, int** cols) {
   if (!ctx || !row_ptr || !cols) return SWE_ERR_INVALID;
   if (swe_status s = check_set(ctx, set)) return s;
-  const long long T = eps_threshold(eps);
+  const long long T = ctx_threshold(ctx, eps);
   if (swe_status s = ensure_bitmap(ctx, set, T)) return s;
   const int n = ctx->set_first[set + 1] - ctx->set_first[set];
   int64_t* rp = (int64_t*)malloc(sizeof(int64_t) * (n + 1));
@@ -929,7 +934,7 @@ swe_status swe_dbscan_set(swe_ctx* ctx, int set, float eps, int minpts, split_se
   if (swe_status s = check_set(ctx, set)) return s;
   if (eps == -1) eps = 0.015f;  // dbscan.c:980-984
   if (minpts == -1) minpts = 5; // dbscan.c:985-989
-  const long long T = eps_threshold(eps);
+  const long long T = ctx_threshold(ctx, eps);
   if (swe_status s = ensure_bitmap(ctx, set, T)) return s;
   const int n = ctx->set_first[set + 1] - ctx->set_first[set];
   const int rc = dbscan_replay_bitmap(n, ctx->h_bits.p, ctx->wpr, ctx->h_counts.p, minpts, out);
@@ -954,9 +959,10 @@ swe_status swe_adaptive_set(swe_ctx* ctx, int set, float eps_start, float eps_in
     return engine_dbscan_batch(ctx, set, e, c, minpts, o);
   };
   prov.batch = engine_batch_size(ctx, set);
+  prov.key = [ctx](float e) { return ctx_sweep_key(ctx, e); };
   std::vector<split_set> kept;
   std::string err;
-  const long long fixed = 4LL * ctx->max_len;  // every distance is <= 4*max_len
+  const long long fixed = ctx_fixed_point(ctx);
   const int n = ctx->set_first[set + 1] - ctx->set_first[set];
   const int rc = adaptive_sweep(n, eps_start, eps_inc, minpts, prefix, log ? log : stdout, prov, true, fixed,
                                 &kept, &err);
@@ -1035,14 +1041,17 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
   const auto t0 = std::chrono::steady_clock::now();
   const int S = ctx->n_sets;
   for (int k = 0; k < S; ++k) results[k] = swe_sweep_result{};
-  const long long fixed = 4LL * ctx->max_len;  // every distance is <= 4*max_len
+  const long long fixed = ctx_fixed_point(ctx);
   const int mp = minpts == -1 ? 5 : minpts;    // dbscan.c:985-989
   const int batch = max_steps > 0 ? std::min(8, max_steps) : 8;
   std::vector<std::unique_ptr<SweepMachine>> m(S);
   std::vector<std::string> logs(S);
   for (int k = 0; k < S; ++k)
+  for (int k = 0; k < S; ++k) {
     m[k].reset(new SweepMachine(ctx->set_first[k + 1] - ctx->set_first[k], eps_start, eps_inc, minpts, max_steps,
                                 batch, true, fixed));
+    m[k]->set_key([ctx](float e) { return ctx_sweep_key(ctx, e); });
+  }
   auto finish_set = [&](int k) {
     std::vector<split_set> kept;
     std::string pre;
@@ -1091,7 +1100,7 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
         std::vector<long long> launchT;
         std::vector<long long> uniq;
         for (float e : m[k]->request()) {
-          const long long T = eps_threshold(e == -1 ? 0.015f : e);  // dbscan.c:980-984
+          const long long T = ctx_threshold(ctx, e == -1 ? 0.015f : e);  // dbscan.c:980-984
           if (std::find(uniq.begin(), uniq.end(), T) == uniq.end()) uniq.push_back(T);
         }
         for (long long T : uniq)
@@ -1160,7 +1169,7 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
           m[k]->abort(rc, "dbscan replay failed");
         } else {
           for (size_t e = 0; e < req.size(); ++e) {
-            const long long T = eps_threshold(req[e] == -1 ? 0.015f : req[e]);
+            const long long T = ctx_threshold(ctx, req[e] == -1 ? 0.015f : req[e]);
             size_t q = job_first[x];
             while (jobs[q].T != T) ++q;
             const size_t u = q - job_first[x];
@@ -1200,6 +1209,7 @@ void swe_free_sweep_results(swe_sweep_result* results, int n) {
 
 swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsigned* out) {
   if (!ctx || (!q && qlen > 0) || (!out && ctx->n > 0)) return SWE_ERR_INVALID;
+  if (swe_status s = need_sequences(ctx)) return s;
   if (swe_status s = select_device(ctx)) return s;
   if (ctx->n == 0) return SWE_OK;
   if (qlen > (size_t)(INT_MAX / 8)) return fail(ctx, SWE_ERR_INVALID, "query too long");
@@ -1242,6 +1252,7 @@ swe_status swe_score_one_to_many(swe_ctx* ctx, const char* q, size_t qlen, unsig
 
 swe_status swe_score_pairs(swe_ctx* ctx, const int* a, const int* b, int64_t npairs, unsigned* out) {
   if (!ctx || npairs < 0 || (npairs > 0 && (!a || !b || !out))) return SWE_ERR_INVALID;
+  if (swe_status s = need_sequences(ctx)) return s;
   if (npairs == 0) return SWE_OK;
   if (swe_status s = select_device(ctx)) return s;
   std::vector<int2> pr(npairs);
@@ -1346,7 +1357,7 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
   std::vector<long long> uniq;
   std::vector<int> slot(count);
   for (int k = 0; k < count; ++k) {
-    const long long T = eps_threshold(eps[k] == -1 ? 0.015f : eps[k]);
+    const long long T = ctx_threshold(ctx, eps[k] == -1 ? 0.015f : eps[k]);
     const auto it = std::find(uniq.begin(), uniq.end(), T);
     slot[k] = (int)(it - uniq.begin());
     if (it == uniq.end()) uniq.push_back(T);

@@ -83,6 +83,13 @@ struct swe_ctx {
   int graph_kernels = 0;
   std::string err;
 
+  // what the upload holds: 0 = sequences (Smith-Waterman distances), else
+  // points with SWE_METRIC_L1 / SWE_METRIC_L2 float distances
+  int metric = 0;
+  int dims = 0;
+  uint32_t point_max_bits = 0;      // bit pattern of the largest point distance
+  swgpu::DevBuf<float> d_points;    // dims x n_pad, dimension-major
+
   // dataset (host)
   int n = 0;
   int max_len = 0;
@@ -198,6 +205,19 @@ swe_status check_kernel_status(swe_ctx* ctx, unsigned status);
 // Stream-ordered copy that also counts the bytes crossing PCIe.
 cudaError_t cpy(swe_ctx* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st);
 swe_status select_device(swe_ctx* ctx);
+// SWE_ERR_STATE unless the upload holds sequences (calls that score
+// sequences refuse a point upload).
+swe_status need_sequences(swe_ctx* ctx);
+// Neighbour threshold of eps for the current upload, compared with the stored
+// distance as an unsigned integer: floor(eps) for Smith-Waterman distances,
+// the bit pattern of eps*eps (L2) or eps (L1) for point distances (their bit
+// patterns order like the non-negative floats they hold); -1 = no neighbour.
+long long ctx_threshold(const swe_ctx* ctx, float eps);
+// A threshold at or above which every larger eps gives the same neighbours
+// (-1 when there is none), and the key of eps that a sweep compares with it
+// (-1 where thresholds do not grow with eps: negative eps under L2).
+long long ctx_fixed_point(const swe_ctx* ctx);
+long long ctx_sweep_key(const swe_ctx* ctx, float eps);
 // Rebuilds the sorted layout (see build_layout in engine.cu) and runs one
 // score pass over the current layout.
 swe_status engine_relayout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand);

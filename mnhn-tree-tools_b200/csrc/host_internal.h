@@ -32,6 +32,8 @@ int dbscan_replay_bitmap(int n, const uint64_t* bits, int words_per_row, const i
 struct DbscanProvider {
   std::function<int(const float* eps, int count, split_set* out)> run;
   int batch = 1;
+  // the sweep key of an eps (see SweepMachine::set_key); empty = eps_threshold
+  std::function<long long(float)> key;
 };
 
 // Adaptive sweep of dbscan.c:1117-1380 as a state machine: request() holds
@@ -46,7 +48,8 @@ struct DbscanProvider {
 // sweep consumes, where the reference's dbscanner calls would print them.
 // `fixed_point` (when >= 0) is a threshold at or above which every eps gives
 // the same result, used to stop sweeps that could never reach one cluster
-// (the reference loops forever there).  max_steps > 0 bounds the DBSCAN runs
+// (the reference loops forever there); an eps is compared with it through its
+// key (eps_threshold unless set_key gives another).  max_steps > 0 bounds the DBSCAN runs
 // of the sweep phase (after the starting eps); a sweep that reaches the bound
 // before a one-cluster result keeps the layers found so far (truncated()).
 // max_steps == 0 is the reference's unbounded sweep.
@@ -57,6 +60,7 @@ class SweepMachine {
   ~SweepMachine();
   SweepMachine(const SweepMachine&) = delete;
   SweepMachine& operator=(const SweepMachine&) = delete;
+  void set_key(std::function<long long(float)> key) { key_ = std::move(key); }
   bool done() const { return phase_ == DONE; }
   const std::vector<float>& request() const { return req_; }
   void consume(split_set* res);
@@ -79,6 +83,7 @@ class SweepMachine {
   int minpts_, max_steps_, batch_;
   bool warnings_;
   long long fixed_;
+  std::function<long long(float)> key_;
   Phase phase_ = FIRST;
   std::vector<float> req_;
   std::vector<split_set> sets_;
@@ -103,6 +108,10 @@ float coverage(int not_covered, int n);
 // parallel.  Semantics of swe_dbscan_set for each eps.
 int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int minpts, split_set* out);
 int engine_batch_size(const swe_ctx* ctx, int set);
+// The sweep's fixed point and eps key for the current upload (see
+// SweepMachine): Smith-Waterman or point distances.
+long long engine_fixed_point(const swe_ctx* ctx);
+long long engine_sweep_key(const swe_ctx* ctx, float eps);
 
 // Deep copy of a split set (malloc'd like the original).
 split_set copy_split_set(const split_set& s);

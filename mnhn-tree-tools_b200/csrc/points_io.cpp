@@ -1,0 +1,177 @@
+// Point-dataset files of the k-mer / PCA DBSCAN tools (cluster_dbscan_kmer.c,
+// cluster_dbscan_pca.c, adaptive_clustering.c): the k-mer table loader of
+// dataset.c:346-425, the value frees of dataset.c:629-649 and the cluster
+// files with values of cluster_io.c:343-379.
+//
+// load_kmer_from_file_into_dataset reads the reference's token stream (a
+// label, then n_features numbers, per sample, whitespace anywhere) with strtof
+// on host threads: the file is cut at whitespace, each piece counts its
+// tokens, and token t of the stream is field t % (n_features + 1) of sample
+// t / (n_features + 1), which is what the reference's fscanf("%s") /
+// fscanf("%f") sequence assigns.  strtof gives the same float as fscanf("%f")
+// for every number; a token that is not a number reads as 0 (the reference
+// leaves the value unset and stops advancing).
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "host_internal.h"
+
+namespace {
+
+inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
+
+float* alloc_values(size_t n) {
+  void* p = nullptr;
+  const size_t padded = (n + 8) & ~size_t(7);  // whole 8-float vectors, as the reference's AVX loop reads
+  if (posix_memalign(&p, 32, sizeof(float) * std::max<size_t>(padded, 8)) != 0) return nullptr;
+  memset(p, 0, sizeof(float) * std::max<size_t>(padded, 8));
+  return static_cast<float*>(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+data_shape shape_from_kmer_file(int infile) {
+  data_shape s{0, 0};
+  const off_t size = lseek(infile, 0, SEEK_END);
+  lseek(infile, 0, SEEK_SET);
+  if (size <= 0) return s;
+  std::vector<char> buf((size_t)size);
+  if (read(infile, buf.data(), (size_t)size) != (ssize_t)size) {
+    printf("Could not read file in order to read obtain data shape\n");
+    swgpu::dropin_set_status(SWE_ERR_IO);
+    return s;
+  }
+  size_t i = 0;
+  while (i < buf.size() && buf[i] != '\n') {  // dataset.c:370-373: tabs of the first line
+    if (buf[i] == '\t') s.n_features++;
+    i++;
+  }
+  for (; i < buf.size(); i++)  // dataset.c:375-378: newlines from the first one on
+    if (buf[i] == '\n') s.n_samples++;
+  return s;
+}
+
+dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape) {
+  dataset ds;
+  memset(&ds, 0, sizeof ds);
+  ds.n_dimensions = (int)shape.n_features;
+  ds.n_values = (int)shape.n_samples;
+  ds.values = static_cast<float**>(malloc(sizeof(float*) * std::max<size_t>(shape.n_features, 1)));
+  for (size_t d = 0; d < shape.n_features; ++d) {
+    ds.values[d] = alloc_values(shape.n_samples);
+    if (!ds.values[d]) {
+      printf("Error allocating aligned memory for kmers \n");
+      swgpu::dropin_set_status(SWE_ERR_OOM);
+      return ds;
+    }
+  }
+  rewind(in_file);
+  std::vector<char> text;
+  {
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = fread(chunk, 1, sizeof chunk, in_file)) > 0) text.insert(text.end(), chunk, chunk + got);
+  }
+  text.push_back('\0');
+  const size_t len = text.size() - 1;
+  const size_t fields = shape.n_features + 1;
+  const uint64_t want = (uint64_t)fields * shape.n_samples;
+  if (want == 0) return ds;
+  // pieces cut at whitespace
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int T = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(hw, 16), len >> 20));
+  std::vector<size_t> cut(T + 1, len);
+  cut[0] = 0;
+  for (int t = 1; t < T; ++t) {
+    size_t p = std::max(cut[t - 1], len * t / T);
+    while (p < len && !is_space(text[p])) ++p;
+    cut[t] = p;
+  }
+  auto tokens = [&](size_t a, size_t b, auto&& on_token) {
+    size_t p = a;
+    uint64_t k = 0;
+    while (p < b) {
+      while (p < b && is_space(text[p])) ++p;
+      if (p >= b) break;
+      const size_t q0 = p;
+      while (p < b && !is_space(text[p])) ++p;
+      on_token(k++, q0, p);
+    }
+    return k;
+  };
+  std::vector<uint64_t> count(T, 0), first(T + 1, 0);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+      th.emplace_back([&, t]() { count[t] = tokens(cut[t], cut[t + 1], [](uint64_t, size_t, size_t) {}); });
+    for (auto& x : th) x.join();
+  }
+  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; ++t)
+    th.emplace_back([&, t]() {
+      char tmp[128];
+      tokens(cut[t], cut[t + 1], [&](uint64_t k, size_t q0, size_t q1) {
+        const uint64_t g = first[t] + k;
+        if (g >= want) return;
+        const uint64_t sample = g / fields, field = g % fields;
+        if (field == 0) return;  // the label, read with "%s"
+        const size_t L = q1 - q0;
+        float v = 0.0f;
+        if (L < sizeof tmp) {
+          memcpy(tmp, text.data() + q0, L);
+          tmp[L] = '\0';
+          v = strtof(tmp, nullptr);
+        } else {
+          std::string s(text.data() + q0, L);
+          v = strtof(s.c_str(), nullptr);
+        }
+        ds.values[field - 1][sample] = v;
+      });
+    });
+  for (auto& x : th) x.join();
+  return ds;
+}
+
+void free_values_from_dataset(dataset ds) {
+  for (int i = 0; i < ds.n_dimensions; i++) free(ds.values[i]);
+  free(ds.values);
+}
+
+void free_dataset(dataset ds) {
+  free_values_from_dataset(ds);
+  free_sequences_from_dataset(ds);
+}
+
+void create_single_cluster_file_with_values(char* filename, cluster cl, dataset ds) {
+  FILE* f = fopen(filename, "w");
+  if (!f) {
+    swgpu::dropin_set_status(SWE_ERR_IO);
+    return;
+  }
+  for (int j = 0; j < cl.n_members; j++) {
+    for (int k = 0; k < ds.n_dimensions - 1; k++) fprintf(f, "%f\t", ds.values[k][cl.members[j]]);
+    if (ds.n_dimensions > 0) fprintf(f, "%f\n", ds.values[ds.n_dimensions - 1][cl.members[j]]);
+    else fputc('\n', f);
+  }
+  fclose(f);
+}
+
+void create_cluster_files_with_values(char* prefix, split_set s, dataset ds) {
+  std::vector<char> name(strlen(prefix) + 32);
+  for (int i = 0; i < s.n_clusters; i++) {
+    snprintf(name.data(), name.size(), "%s-%03d", prefix, i);
+    create_single_cluster_file_with_values(name.data(), s.clusters[i], ds);
+  }
+}
+
+}  // extern "C"

@@ -60,6 +60,7 @@ namespace {
 using PS = PrefilterState;
 
 swe_status pf_need(swe_ctx* ctx, bool need_init) {
+  if (swe_status s = need_sequences(ctx)) return s;
   if (!ctx->pf) ctx->pf = new PrefilterState();
   if (need_init && !ctx->pf->init) return fail(ctx, SWE_ERR_STATE, "prefilter not initialised");
   return SWE_OK;
@@ -225,6 +226,7 @@ extern "C" {
 
 swe_status swe_kmer_features(swe_ctx* ctx, int k, float* out) {
   if (!ctx || k < 1 || k > 6) return SWE_ERR_INVALID;
+  if (swe_status s = need_sequences(ctx)) return s;
   if (swe_status s = select_device(ctx)) return s;
   if (ctx->n == 0) return SWE_OK;
   const size_t nb = (size_t)1 << (2 * k);

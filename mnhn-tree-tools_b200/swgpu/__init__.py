@@ -127,13 +127,15 @@ EXPORTS = [
     "swe_kmer_features", "swe_prefilter_init", "swe_prefilter_param_count", "swe_prefilter_params",
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
-    "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv",
+    "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
     "data_not_in_clusters", "intersection_of_clusters", "generate_split_set_relation",
     "free_split_set_and_associated_clusters", "swgpu_last_dropin_status",
-    "frequencies_from_dataset", "write_kmer_base", "free_kmer_frequencies",
+    "frequencies_from_dataset", "write_kmer_base", "free_kmer_frequencies", "dbscan_L1", "dbscan_L2",
+    "shape_from_kmer_file", "load_kmer_from_file_into_dataset", "free_values_from_dataset", "free_dataset",
+    "create_single_cluster_file_with_values", "create_cluster_files_with_values",
 ]
 
 _lib = None
@@ -239,6 +241,8 @@ def lib():
         L.read_split_set.restype = SplitSet
         L.read_split_set.argtypes = [C.c_char_p]
         L.swgpu_last_dropin_status.restype = C.c_int
+        L.swe_upload_points.restype = C.c_int
+        L.swe_upload_points.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.swe_kmer_count.restype = C.c_int64
         L.swe_kmer_count.argtypes = [C.c_int, C.c_int]
         L.swe_kmer_counts.restype = C.c_int
@@ -309,6 +313,21 @@ class Engine:
         _check(lib().swe_upload(self.ctx, self._buf.ptrs, self._buf.lens, self._buf.n), self.ctx)
         self.n = self._buf.n
         self.set_first = [0, self.n]
+
+    def upload_points(self, values: np.ndarray, metric: int):
+        """Points values[dim][point] (float32) with the L1 (metric 1) or L2
+        (metric 2) distances of dbscan_L1 / dbscan_L2, computed on upload;
+        distances() then returns their float bit patterns."""
+        V = np.ascontiguousarray(values, dtype=np.float32)
+        if V.ndim != 2:
+            raise ValueError("values must be dims x n")
+        dims, n = V.shape
+        self._pts = V
+        ptrs = (C.c_void_p * max(1, dims))(*[V.ctypes.data + k * n * 4 for k in range(dims)])
+        _check(lib().swe_upload_points(self.ctx, ptrs, dims, n, metric), self.ctx)
+        self._buf = None
+        self.n = n
+        self.set_first = [0, n]
 
     def upload_sets(self, sets):
         """Uploads independent sets (a list of sequence lists); pairs are

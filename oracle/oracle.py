@@ -64,6 +64,10 @@ def lib():
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_kmer_counts.argtypes = [C.c_char_p, C.c_size_t, C.c_int, C.c_void_p]
         L.orc_kmer_frequencies.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
+        L.orc_points_dist.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_dbscan_points.restype = C.c_int
+        L.orc_dbscan_points.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_int, C.c_void_p,
+                                        C.c_void_p]
         _lib = L
     return _lib
 
@@ -141,6 +145,77 @@ def dbscan(D: np.ndarray, eps: float, minpts: int):
     sizes = np.zeros(max(1, n), dtype=np.int32)
     nc = lib().orc_dbscan(D.ctypes.data, n, C.c_float(eps), minpts, members.ctypes.data,
                           sizes.ctypes.data)
+    out, pos = [], 0
+    for c in range(nc):
+        out.append(members[pos:pos + sizes[c]].tolist())
+        pos += sizes[c]
+    return out
+
+
+def points_dist(values: np.ndarray, metric: int) -> np.ndarray:
+    """dbscan_L1 (metric 1) / dbscan_L2 (metric 2) pair distances
+    (dbscan.c:563-779) of points values[dim][point]: float32 n x n, row =
+    query point."""
+    V = np.ascontiguousarray(values, dtype=np.float32)
+    dims, n = V.shape
+    D = np.zeros((n, n), dtype=np.float32)
+    lib().orc_points_dist(V.ctypes.data, dims, n, metric, D.ctypes.data)
+    return D
+
+
+_libc = None
+
+
+def _strtof(tok: str) -> float:
+    """C strtof (what fscanf "%f" stores for a number token)."""
+    global _libc
+    if _libc is None:
+        _libc = C.CDLL(None)
+        _libc.strtof.restype = C.c_float
+        _libc.strtof.argtypes = [C.c_char_p, C.c_void_p]
+    return _libc.strtof(tok.encode(), None)
+
+
+def load_kmer_text(text: str) -> np.ndarray:
+    """load_kmer_from_file_into_dataset over shape_from_kmer_file (dataset.c:
+    346-425): n_features = tabs of the first line, n_samples = newlines from
+    the end of the first line on; the token stream is a label then n_features
+    numbers per sample.  Returns values[feature][sample] as float32."""
+    first_nl = text.index("\n") if "\n" in text else len(text)
+    nf = text[:first_nl].count("\t")
+    ns = text[first_nl:].count("\n")
+    toks = text.split()
+    V = np.zeros((nf, ns), dtype=np.float32)
+    for s in range(ns):
+        for f in range(nf):
+            V[f, s] = _strtof(toks[s * (nf + 1) + 1 + f])
+    return V
+
+
+def load_projection_text(text: str, dims: int, n: int) -> np.ndarray:
+    """load_projections_from_file_into_dataset (dataset.c:427-469): n samples
+    of `dims` numbers, values[dim][sample] as float32."""
+    toks = text.split()
+    V = np.zeros((dims, n), dtype=np.float32)
+    for i in range(n):
+        for j in range(dims):
+            V[j, i] = _strtof(toks[i * dims + j])
+    return V
+
+
+def cluster_values_text(members, V: np.ndarray) -> str:
+    """create_single_cluster_file_with_values (cluster_io.c:343-356)."""
+    return "".join("\t".join("%f" % float(V[k, m]) for k in range(V.shape[0])) + "\n" for m in members)
+
+
+def dbscan_points(D: np.ndarray, eps: float, minpts: int, metric: int):
+    """dbscan_L1 / dbscan_L2 (dbscan.c:950-1047) over points_dist's matrix."""
+    D = np.ascontiguousarray(D, dtype=np.float32)
+    n = D.shape[0]
+    members = np.zeros(max(1, n), dtype=np.int32)
+    sizes = np.zeros(max(1, n), dtype=np.int32)
+    nc = lib().orc_dbscan_points(D.ctypes.data, n, C.c_float(eps), minpts, metric, members.ctypes.data,
+                                 sizes.ctypes.data)
     out, pos = [], 0
     for c in range(nc):
         out.append(members[pos:pos + sizes[c]].tolist())
@@ -345,7 +420,7 @@ def cluster_fasta_text(members, seqs) -> str:
 
 
 def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_steps: int = 100000,
-             truncate: bool = False):
+             truncate: bool = False, dbscan_fn=None):
     """adaptive_dbscan, dbscan.c:1117-1380, single thread, over a distance matrix.
 
     Returns (stdout text, kept split sets).  Float semantics follow the
@@ -356,6 +431,8 @@ def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_s
     The reference's sweep is unbounded.  With truncate=True a sweep that has
     not reached one cluster after max_steps DBSCAN runs keeps the layers found
     so far (the engine's bounded sweep for many sets); otherwise it raises.
+    dbscan_fn(eps, minpts) replaces the Smith-Waterman DBSCAN over D (the
+    dbscan_L1 / dbscan_L2 builds of the same driver).
     """
     n = D.shape[0]
     out = []
@@ -368,6 +445,8 @@ def adaptive(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, max_s
         if f32(eps) == f32(-1):
             out.append("Warning @dbscan: epsilon value is: %f\n" % float(f32(eps)))
             out.append("Warning @dbscan: epsilon was changed to: %f\n" % float(f32(0.015)))
+        if dbscan_fn is not None:
+            return dbscan_fn(float(f32(eps)), minpts)
         return dbscan(D, float(f32(eps)), minpts)
 
     first = run(start)

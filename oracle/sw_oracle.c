@@ -17,6 +17,7 @@
  * the reference project root).
  */
 #define _GNU_SOURCE
+#include <math.h>
 #include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -119,13 +120,61 @@ int orc_all_pairs(const char* const* seqs, const size_t* lens, int n, uint32_t* 
 
 /* region_query, dbscan.c:525-561: ascending k with (float)d(k,point) <= eps,
    the point itself included. */
-static int orc_region(const uint32_t* D, int n, int point, float eps, int* out) {
+static int orc_region(const void* Dv, int n, int point, float eps, int* out) {
+  const uint32_t* D = (const uint32_t*)Dv;
   int m = 0;
   for (int k = 0; k < n; k++) {
     float d = (float)D[(size_t)point * (size_t)n + (size_t)k];
     if (d <= eps) out[m++] = k;
   }
   return m;
+}
+
+/* region_query of dbscan_L1 / dbscan_L2 (dbscan.c:563-779) over a float
+   matrix of point distances: d <= epsilon (L1), d <= epsilon*epsilon with
+   the square rounded to float (L2, dbscan.c:578). */
+static int orc_region_l1(const void* Dv, int n, int point, float eps, int* out) {
+  const float* D = (const float*)Dv;
+  int m = 0;
+  for (int k = 0; k < n; k++)
+    if (D[(size_t)point * (size_t)n + (size_t)k] <= eps) out[m++] = k;
+  return m;
+}
+
+static int orc_region_l2(const void* Dv, int n, int point, float eps, int* out) {
+  const float* D = (const float*)Dv;
+  const float eps2 = eps * eps;
+  int m = 0;
+  for (int k = 0; k < n; k++)
+    if (D[(size_t)point * (size_t)n + (size_t)k] <= eps2) out[m++] = k;
+  return m;
+}
+
+typedef int (*orc_region_fn)(const void* D, int n, int point, float eps, int* out);
+static int dbscan_core(const void* D, int n, float eps, int minpts, orc_region_fn region, int* members, int* sizes);
+
+/* The pair distances of dbscan_L1 / dbscan_L2's region_query (dbscan.c:
+   563-779, the AVX build with FMA): for query point p and point i, over the
+   dimensions k in order from +0, L2 dist = fmaf(v_p - v_i, v_p - v_i, dist)
+   (dbscan.c:661-665), L1 dist = dist + |v_p - v_i| (dbscan.c:672-675).  V is
+   dimension-major (V[k*n + i], the reference's values[k][i]); D[p*n + i]
+   receives the distance.  metric 1 = L1, 2 = L2. */
+void orc_points_dist(const float* V, int dims, int n, int metric, float* D) {
+  for (int p = 0; p < n; p++)
+    for (int i = 0; i < n; i++) {
+      float acc = 0.0f;
+      for (int k = 0; k < dims; k++) {
+        const float d = V[(size_t)k * (size_t)n + (size_t)p] - V[(size_t)k * (size_t)n + (size_t)i];
+        acc = metric == 2 ? fmaf(d, d, acc) : acc + fabsf(d);
+      }
+      D[(size_t)p * (size_t)n + (size_t)i] = acc;
+    }
+}
+
+/* dbscan_L1 / dbscan_L2 (dbscan.c:950-1047 with the region queries above)
+   over that matrix; output as orc_dbscan. */
+int orc_dbscan_points(const float* D, int n, float eps, int minpts, int metric, int* members, int* sizes) {
+  return dbscan_core(D, n, eps, minpts, metric == 2 ? orc_region_l2 : orc_region_l1, members, sizes);
 }
 
 /*
@@ -149,6 +198,11 @@ static int orc_region(const uint32_t* D, int n, int point, float eps, int* out) 
  * order, sizes[c] their counts.  Returns the number of clusters.
  */
 int orc_dbscan(const uint32_t* D, int n, float eps, int minpts, int* members, int* sizes) {
+  return dbscan_core(D, n, eps, minpts, orc_region, members, sizes);
+}
+
+static int dbscan_core(const void* D, int n, float eps, int minpts, orc_region_fn region, int* members,
+                       int* sizes) {
   /* dbscan.c:980-989 defaults */
   if (eps == -1) eps = 0.015f;
   if (minpts == -1) minpts = 5;
@@ -163,7 +217,7 @@ int orc_dbscan(const uint32_t* D, int n, float eps, int minpts, int* members, in
   for (int i = 0; i < n; i++) {
     if (visited[i]) continue;
     visited[i] = 1;
-    int n_nb = orc_region(D, n, i, eps, nb);
+    int n_nb = region(D, n, i, eps, nb);
     if (!(minpts < n_nb)) continue;
     /* expand_cluster */
     int* cl = members + out_pos;
@@ -176,7 +230,7 @@ int orc_dbscan(const uint32_t* D, int n, float eps, int minpts, int* members, in
       int q = frontier[f];
       if (!visited[q]) {
         visited[q] = 1;
-        int n_q = orc_region(D, n, q, eps, nbq);
+        int n_q = region(D, n, q, eps, nbq);
         if (n_q >= minpts) {
           /* sorted merge of nb and nbq; the members of nbq missing from nb go
              to the frontier in ascending order */

@@ -364,6 +364,75 @@ def fasta2kmer_golden():
     (OUT / "fasta2kmer.json").write_text(json.dumps(doc, indent=0))
 
 
+STALE_ENV = {"GLIBC_TUNABLES": "glibc.malloc.tcache_count=0:glibc.malloc.perturb=165"}
+
+
+def points_golden():
+    """The reference's k-mer / PCA DBSCAN tools (cluster_dbscan_kmerL1/L2,
+    cluster_dbscan_pca, adaptive_clustering_kmer_L1/L2, adaptive_clustering_PCA,
+    built from its sources into oracle/_ref): stdout and every file they write,
+    on two-level read families (hier_set), their 3-mer and 4-mer tables from
+    the reference's own fasta2kmer, and 3-D projections of three groups of two
+    Gaussian blobs printed with six decimals (so sweeps keep several layers).
+
+    The tools run with glibc's malloc cache off and fresh blocks filled with a
+    byte pattern (STALE_ENV): expand_cluster reads right_in_left one slot past
+    its filled length (dbscan.c:896), i.e. memory malloc did not initialise,
+    and when that stale word equals a later neighbour the neighbour is dropped
+    from the frontier.  With the pattern the word is never a point index, so
+    the outputs are the reference's intended set difference; without it they
+    depend on heap history (this data set's adaptive_clustering_PCA run keeps
+    its first layer one eps step later)."""
+    seqs = hier_set(31, n_top=2, n_sub=3, per_sub=15, root_len=160)
+    n = len(seqs)
+    rng = np.random.default_rng(31)
+    sup = rng.normal(0, 8, size=(3, 3))
+    sub = sup[:, None, :] + rng.normal(0, 2.5, size=(3, 2, 3))
+    proj = np.array([sub[i % 3, (i // 3) % 2] + rng.normal(0, 0.5, size=3) for i in range(n)])
+    proj_text = "".join(" ".join(f"{v:.6f}" for v in row) + "\n" for row in proj)
+    doc = {"seqs": [s.decode("latin-1") for s in seqs], "proj": proj_text, "kmer": {}, "runs": [],
+           "env": STALE_ENV}
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        W.write_fasta(d / "in.fa", seqs)
+        (d / "proj.txt").write_text(proj_text)
+        for k in (3, 4):
+            r = O.run_ref_tool("fasta2kmer", ["in.fa", str(k), "1", "0"], d)
+            assert r.returncode == 0
+            (d / f"k{k}.tsv").write_bytes(r.stdout)
+            doc["kmer"][str(k)] = r.stdout.decode()
+        # eps values from the distance distributions (float64, only to pick parameters)
+        def dists(X, p):
+            diff = X[:, None, :] - X[None, :, :]
+            return np.abs(diff).sum(-1) if p == 1 else np.sqrt((diff ** 2).sum(-1))
+        k3 = np.loadtxt(d / "k3.tsv", usecols=range(1, 65))
+        k4 = np.loadtxt(d / "k4.tsv", usecols=range(1, 257))
+        q = lambda D, f: float(np.quantile(D[np.triu_indices(n, 1)], f))
+        cases = []
+        for name, X, p in (("k3", k3, 1), ("k4", k4, 2)):
+            D = dists(X, p)
+            tool = "cluster_dbscan_kmerL1" if p == 1 else "cluster_dbscan_kmerL2"
+            for f, mp in ((0.02, 4), (0.08, 5), (0.3, 3)):
+                cases.append((tool, ["in.fa", f"{name}.tsv", f"{q(D, f):.3f}", str(mp), "out_cl"], "out_"))
+            atool = "adaptive_clustering_kmer_L1" if p == 1 else "adaptive_clustering_kmer_L2"
+            cases.append((atool, [f"{name}.tsv", f"{q(D, 0.02):.3f}", f"{q(D, 0.03) - q(D, 0.02):.3f}", "4",
+                                  "out_layer", "1"], "out_"))
+        Dp = dists(proj, 2)
+        for f, mp in ((0.03, 4), (0.3, 5)):
+            cases.append(("cluster_dbscan_pca", ["in.fa", "proj.txt", "3", f"{q(Dp, f):.4f}", str(mp), "out_pc",
+                                                 "out_pv"], "out_"))
+        cases.append(("adaptive_clustering_PCA", ["in.fa", f"{q(Dp, 0.02):.4f}", f"{q(Dp, 0.04) - q(Dp, 0.02):.4f}",
+                                                  "4", "out_player", "1", "3", "proj.txt"], "out_"))
+        for tool, args, prefix in cases:
+            for old in d.glob(prefix + "*"):
+                old.unlink()
+            rc, out = run_tool(tool, args, d, env=STALE_ENV)
+            assert rc == 0, (tool, out[-400:])
+            doc["runs"].append({"tool": tool, "args": args, "stdout": out, "files": files_b64(d, prefix)})
+            print(tool, args, [ln for ln in out.splitlines() if "clusters" in ln][-3:], len(doc["runs"][-1]["files"]))
+    (OUT / "points.json").write_text(json.dumps(doc))
+
+
 def score_callers_golden():
     """stdout of the reference's compareSW, silhouette, compare_norms and
     find_satellite (built from its sources into oracle/_ref, one thread) on
@@ -401,7 +470,7 @@ if __name__ == "__main__":
     if not O.ref_available():
         O.build()
     which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
-                             "kmer", "callers", "fasta2kmer"]
+                             "kmer", "callers", "fasta2kmer", "points"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -424,3 +493,5 @@ if __name__ == "__main__":
         score_callers_golden()
     if "fasta2kmer" in which:
         fasta2kmer_golden()
+    if "points" in which:
+        points_golden()

@@ -183,6 +183,116 @@ def fasta2kmer_leg(seqs, k: int = 5, cpu: bool = True, reps: int = 3):
     return out
 
 
+def kmer_dbscan_leg(eng, seqs, dev, k: int = 5, cpu: bool = True, reps: int = 3):
+    """dbscan_L2 over the k-mer tables of the same reads (the k-mer / PCA
+    DBSCAN path, dbscan.c:563-779): the table from the GPU, then through the C
+    ABI with host buffers the point upload (every L2 distance on the GPU) and
+    one DBSCAN, median of `reps`.  The distance kernel's CUDA-event time gives
+    its roofline: 2 FP32 instructions (subtract, fused multiply-add) per pair
+    and dimension against 148 SMs x 128 FP32 lanes at the sampled clock.  With
+    cpu, the reference's own dbscan_L2 (oracle/_ref/libref_l2.so, single
+    threaded as the reference is) on the first m points, m sized for about
+    10 s."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import swgpu
+    table = eng.kmer_counts(seqs, k)
+    V = np.ascontiguousarray(table.T, dtype=np.float32)  # values[dim][point]
+    dims, n = V.shape
+    rng = np.random.default_rng(0)
+    sample = rng.choice(n, size=(64, 2))
+    d = np.sqrt(((V[:, sample[:, 0]] - V[:, sample[:, 1]]) ** 2).sum(0))
+    eps = float(np.quantile(d, 0.02))
+    up, db, kern = [], [], []
+    clusters = None
+    for r in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        eng.upload_points(V, 2)  # SWE_METRIC_L2
+        t1 = time.perf_counter()
+        clusters = eng.dbscan(eps, 5)
+        t2 = time.perf_counter()
+        if r:
+            up.append(1e3 * (t1 - t0))
+            db.append(1e3 * (t2 - t1))
+            kern.append(eng.stats()["ms_score_pass"])
+    kms = statistics.median(kern)
+    pair_dims = n * (n - 1) / 2 * dims
+    props = torch.cuda.get_device_properties(dev)
+    peak = props.multi_processor_count * 128 * 1.965e9  # FP32 lanes x clocks.max.sm
+    out = {"workload": f"dbscan_L2 (eps {eps:.3f}, minpts 5) over the {k}-mer tables of the same {n} reads "
+                       f"({dims} dimensions), host values in, clusters out",
+           "upload_ms": round(statistics.median(up), 2), "dbscan_ms": round(statistics.median(db), 2),
+           "e2e_ms": round(statistics.median(up) + statistics.median(db), 2), "clusters": len(clusters),
+           "kernel": {"name": "point_dist_kernel", "ms": round(kms, 3),
+                      "unique_pair_dims_per_s": round(pair_dims / (kms * 1e-3), 1),
+                      "bound": "fp32", "achieved": round(2 * pair_dims / (kms * 1e-3) / 1e12, 3),
+                      "peak": round(peak / 1e12, 3), "unit": "T FP32 lane-instructions/s",
+                      "frac": round(2 * pair_dims / (kms * 1e-3) / peak, 4),
+                      "peak_source": "SMs x 128 FP32 lanes x 1,965 MHz (clocks.max.sm)"},
+           "cpu_baseline": None}
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        lib_path = O.REF_DIR / "libref_l2.so"
+        if lib_path.exists():
+            R = C.CDLL(str(lib_path))
+            R.dbscan_L2.restype = swgpu.SplitSet
+            R.dbscan_L2.argtypes = [swgpu.Dataset, C.c_float, C.c_int]
+            R.free_split_set_and_associated_clusters.argtypes = [swgpu.SplitSet]
+
+            def aligned_row(x):
+                # the reference's AVX loads need 32-byte aligned rows, readable in whole 8-float vectors
+                buf = np.zeros(len(x) + 16, dtype=np.float32)
+                off = (-buf.ctypes.data % 32) // 4
+                row = buf[off:off + len(x) + 8]
+                row[:len(x)] = x
+                return row
+
+            def ref_run(m):
+                rows = [aligned_row(V[j, :m]) for j in range(dims)]
+                ptrs = (C.c_void_p * dims)(*[r.ctypes.data for r in rows])
+                ds = swgpu.Dataset(None, None, None, m, C.cast(ptrs, C.c_void_p), dims, 0)
+                t0 = time.perf_counter()
+                s = R.dbscan_L2(ds, C.c_float(eps), 5)
+                dt = time.perf_counter() - t0
+                R.free_split_set_and_associated_clusters(s)
+                return dt
+
+            m = min(n, 1000)
+            dt = ref_run(m)
+            m = int(min(n, m * (10.0 / max(dt, 1e-3)) ** 0.5))
+            dt = ref_run(m)
+            rate = m * m * dims / dt
+            out["cpu_baseline"] = {"kind": "reference", "cores": 1, "seconds": round(dt, 3),
+                                   "pair_dims_per_s": round(rate, 1),
+                                   "sample": f"the reference's dbscan_L2 on the first {m} points (every region "
+                                             f"query scans all {m} points: {m}^2 x {dims} pair-dimensions)"}
+            # the reference evaluates every ordered pair in its region queries: n^2 x dims per pass
+            out["dbscan_vs_cpu"] = round((n * n * dims / rate) / (out["e2e_ms"] * 1e-3), 1)
+    return out
+
+
+def run_leg(args):
+    """One side leg alone (profiling a small case of its kernels)."""
+    import swgpu
+    from swgpu import workloads as W
+    seqs, _ = W.config2(seed=dataset_seed("2", 0))
+    if args.n:
+        seqs = seqs[:args.n]
+    if args.leg == "fasta2kmer":
+        out = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
+    else:
+        eng = swgpu.Engine(device=0)
+        out = kmer_dbscan_leg(eng, seqs, 0, cpu=not args.no_cpu_baseline)
+        eng.close()
+    print(json.dumps({"leg": args.leg, **out}), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank, _, world = env_rank()
     if rank != 0:
@@ -450,6 +560,7 @@ def run_gpu(args):
         }
         if world == 1 and wl["gen"] == "config2" and not args.no_kmer:
             line["fasta2kmer"] = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
+            line["kmer_dbscan"] = kmer_dbscan_leg(eng, seqs, dev, cpu=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     eng.close()
     del flush
@@ -809,9 +920,13 @@ def main():
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
     ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
-    ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer leg")
+    ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer and k-mer DBSCAN legs")
+    ap.add_argument("--leg", choices=["fasta2kmer", "kmer_dbscan"],
+                    help="run one side leg alone on the config-2 reads (the first --n) and print its object")
     ap.add_argument("--weight-decay", type=float, default=0.0, help="config 4: decoupled weight decay of Adam")
     args = ap.parse_args()
+    if args.leg:
+        return run_leg(args)
     if args.impl == "reference":
         return run_reference(args)
     if WORKLOADS[args.config]["mode"] == "multi":

@@ -65,6 +65,8 @@ struct PrefilterState;
 void prefilter_destroy(PrefilterState* pf);
 struct KmerState;
 void kmer_state_destroy(KmerState* km);
+struct Staging;
+void staging_destroy(Staging* sg);
 
 }  // namespace swgpu
 
@@ -183,11 +185,14 @@ struct swe_ctx {
   swgpu::PrefilterState* pf = nullptr;
   // k-mer tables: device buffers and pinned staging (null until first used)
   swgpu::KmerState* km = nullptr;
+  // pinned staging chunks of the chunked transfers (null until first used)
+  swgpu::Staging* stage = nullptr;
 
   ~swe_ctx() {
     cudaSetDevice(device);
     swgpu::prefilter_destroy(pf);
     swgpu::kmer_state_destroy(km);
+    swgpu::staging_destroy(stage);
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);

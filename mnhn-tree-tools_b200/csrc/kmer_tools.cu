@@ -22,9 +22,8 @@
 
 #include <algorithm>
 #include <cstring>
-#include <thread>
 
-#include "engine_ctx.cuh"
+#include "staging.cuh"
 
 namespace swgpu {
 namespace {
@@ -307,40 +306,6 @@ __global__ void kmer_tsv_write_kernel(const int16_t* __restrict__ counts, SegGeo
   }
 }
 
-// f(t) for t in [0, tasks) on up to `threads` host threads.
-template <class F>
-void host_parallel(int64_t tasks, int threads, F&& f) {
-  threads = (int)std::min<int64_t>(std::max(threads, 1), tasks);
-  if (threads <= 1) {
-    for (int64_t t = 0; t < tasks; ++t) f(t);
-    return;
-  }
-  std::vector<std::thread> th;
-  th.reserve(threads);
-  for (int w = 0; w < threads; ++w)
-    th.emplace_back([&, w]() {
-      for (int64_t t = w; t < tasks; t += threads) f(t);
-    });
-  for (auto& x : th) x.join();
-}
-
-// Host threads for a copy of `bytes` (about 1 MB each, at most 8).
-int copy_threads(size_t bytes) {
-  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  return (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(hw, 8), bytes >> 20));
-}
-
-// copy(a, b) over [a, b) split into one sub-range per host thread.
-template <class F>
-void split_copy(size_t a, size_t b, F&& copy) {
-  const int T = copy_threads(b - a);
-  const size_t step = (b - a + T - 1) / T;
-  host_parallel(T, T, [&](int64_t t) {
-    const size_t x = a + (size_t)t * step, y = std::min(b, x + step);
-    if (x < y) copy(x, y);
-  });
-}
-
 int grid_for(const swe_ctx* ctx, int64_t units, int per_sm) {
   const int64_t cap = (int64_t)ctx->num_sms * per_sm;
   return (int)std::max<int64_t>(1, std::min(units, cap));
@@ -348,86 +313,40 @@ int grid_for(const swe_ctx* ctx, int64_t units, int per_sm) {
 
 }  // namespace
 
-// Device buffers and two pinned staging chunks kept by a context between calls.
+// Device buffers kept by a context between k-mer calls.
 struct KmerState {
   DevBuf<int16_t> d_out, d_cnt;
   DevBuf<uint8_t> d_seq;
   DevBuf<int64_t> d_off, d_len, d_list, d_segoff;
   DevBuf<uint32_t> d_wide, d_seglen;
   DevBuf<char> d_text;
-  HostPinned<char> pin[2];
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  ~KmerState() {
-    for (auto e : ev)
-      if (e) cudaEventDestroy(e);
-  }
 };
 
 void kmer_state_destroy(KmerState* km) { delete km; }
 
+void staging_destroy(Staging* sg) { delete sg; }
+
+swe_status staging_ready(swe_ctx* ctx, size_t chunk, Staging** out) {
+  if (!ctx->stage) {
+    ctx->stage = new (std::nothrow) Staging();
+    if (!ctx->stage) return fail(ctx, SWE_ERR_OOM, "staging buffers");
+    for (auto& e : ctx->stage->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  for (auto& p : ctx->stage->pin) CK(p.alloc(chunk));
+  *out = ctx->stage;
+  return SWE_OK;
+}
+
 namespace {
 
-constexpr size_t KM_CHUNK = size_t(8) << 20;  // bytes per pinned staging chunk
-
-// The context's k-mer state with both staging chunks of `chunk` bytes.
-swe_status kmer_state(swe_ctx* ctx, size_t chunk, KmerState** out) {
+// The context's k-mer buffers and its staging chunks.
+swe_status kmer_state(swe_ctx* ctx, size_t chunk, KmerState** out, Staging** sg) {
   if (!ctx->km) {
     ctx->km = new (std::nothrow) KmerState();
     if (!ctx->km) return fail(ctx, SWE_ERR_OOM, "k-mer state");
-    for (auto& e : ctx->km->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  for (auto& p : ctx->km->pin) CK(p.alloc(chunk));
   *out = ctx->km;
-  return SWE_OK;
-}
-
-size_t stage_chunk(const swe_ctx* ctx) {
-  const size_t c = ctx->kmer_batch_bytes ? std::min(ctx->kmer_batch_bytes, KM_CHUNK) : KM_CHUNK;
-  return std::max<size_t>(16, c & ~size_t(15));
-}
-
-// Host -> device copy of `total` bytes assembled by gather(dst, a, b) (source
-// bytes [a, b) into dst), chunk by chunk through the two pinned buffers: the
-// gather of one chunk overlaps the copy of the previous one.
-template <class G>
-swe_status staged_h2d(swe_ctx* ctx, KmerState* km, size_t chunk, void* d_dst, size_t total, G&& gather) {
-  size_t j = 0;
-  for (size_t a = 0; a < total; a += chunk, ++j) {
-    const int slot = (int)(j & 1);
-    const size_t b = std::min(total, a + chunk);
-    CK(cudaEventSynchronize(km->ev[slot]));  // the copy that last read this buffer
-    gather(km->pin[slot].p, a, b);
-    CK(cpy(ctx, static_cast<char*>(d_dst) + a, km->pin[slot].p, b - a, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaEventRecord(km->ev[slot], ctx->st));
-  }
-  return SWE_OK;
-}
-
-// Device -> host copy of `total` bytes of d_src, handed to consume(src, a, b)
-// (host bytes [a, b)) in order; the copy of the next chunk overlaps the
-// consumer.  A consumer returning false stops the transfer (SWE_ERR_IO).
-template <class C>
-swe_status staged_d2h(swe_ctx* ctx, KmerState* km, size_t chunk, const void* d_src, size_t total, C&& consume) {
-  if (total == 0) return SWE_OK;
-  const size_t nch = (total + chunk - 1) / chunk;
-  auto issue = [&](size_t j) -> cudaError_t {
-    const size_t a = j * chunk, b = std::min(total, a + chunk);
-    cudaError_t e = cpy(ctx, km->pin[j & 1].p, static_cast<const char*>(d_src) + a, b - a,
-                        cudaMemcpyDeviceToHost, ctx->st);
-    if (e == cudaSuccess) e = cudaEventRecord(km->ev[j & 1], ctx->st);
-    return e;
-  };
-  CK(issue(0));
-  for (size_t j = 0; j < nch; ++j) {
-    if (j + 1 < nch) CK(issue(j + 1));
-    CK(cudaEventSynchronize(km->ev[j & 1]));
-    const size_t a = j * chunk, b = std::min(total, a + chunk);
-    if (!consume(km->pin[j & 1].p, a, b)) {
-      CK(cudaStreamSynchronize(ctx->st));
-      return fail(ctx, SWE_ERR_IO, "text sink stopped");
-    }
-  }
-  return SWE_OK;
+  return staging_ready(ctx, chunk, sg);
 }
 
 }  // namespace
@@ -456,7 +375,8 @@ swe_status swe_kmer_counts(swe_ctx* ctx, const char* const* seqs, const int64_t*
   if (swe_status st = select_device(ctx)) return st;
   const size_t chunk = stage_chunk(ctx);
   KmerState* km = nullptr;
-  if (swe_status st = kmer_state(ctx, chunk, &km)) return st;
+  Staging* sg = nullptr;
+  if (swe_status st = kmer_state(ctx, chunk, &km, &sg)) return st;
   uint64_t top = 1;
   for (int i = 0; i < k - 1; ++i) top *= protein ? 20 : 4;
 
@@ -492,7 +412,7 @@ swe_status swe_kmer_counts(swe_ctx* ctx, const char* const* seqs, const int64_t*
     CK(km->d_len.alloc(nb));
     CK(km->d_out.alloc((size_t)nb * nk));
     // the batch's sequences, packed back to back
-    swe_status st = staged_h2d(ctx, km, chunk, km->d_seq.p, (size_t)bytes, [&](char* dst, size_t a, size_t b) {
+    swe_status st = staged_h2d(ctx, sg, chunk, km->d_seq.p, (size_t)bytes, [&](char* dst, size_t a, size_t b) {
       split_copy(a, b, [&](size_t x, size_t y) {
         int64_t i = std::upper_bound(b_off.begin(), b_off.end(), (int64_t)x) - b_off.begin() - 1;
         for (size_t p = x; p < y; ++i) {
@@ -553,7 +473,7 @@ swe_status swe_kmer_counts(swe_ctx* ctx, const char* const* seqs, const int64_t*
       }
     }
     // rows back into the caller's row buffers
-    st = staged_d2h(ctx, km, chunk, km->d_out.p, (size_t)nb * row_bytes, [&](const char* src, size_t a, size_t b) {
+    st = staged_d2h(ctx, sg, chunk, km->d_out.p, (size_t)nb * row_bytes, [&](const char* src, size_t a, size_t b) {
       split_copy(a, b, [&](size_t x, size_t y) {
         for (size_t p = x; p < y;) {
           const size_t r = p / row_bytes, in = p - r * row_bytes;
@@ -581,7 +501,8 @@ swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int
   if (swe_status st = select_device(ctx)) return st;
   const size_t chunk = stage_chunk(ctx);
   KmerState* km = nullptr;
-  if (swe_status st = kmer_state(ctx, chunk, &km)) return st;
+  Staging* sg = nullptr;
+  if (swe_status st = kmer_state(ctx, chunk, &km, &sg)) return st;
 
   const int64_t spr = (nk + KM_SEG - 1) / KM_SEG;
   const int64_t seg_cols = std::min(nk, KM_SEG);
@@ -601,7 +522,7 @@ swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int
     const size_t bytes = (size_t)(e1 - e0) * sizeof(int16_t);
     const size_t base = (size_t)e0 * sizeof(int16_t);
     CK(km->d_cnt.alloc((size_t)(e1 - e0)));
-    swe_status st = staged_h2d(ctx, km, chunk, km->d_cnt.p, bytes, [&](char* dst, size_t a, size_t b) {
+    swe_status st = staged_h2d(ctx, sg, chunk, km->d_cnt.p, bytes, [&](char* dst, size_t a, size_t b) {
       split_copy(base + a, base + b, [&](size_t x, size_t y) {
         for (size_t p = x; p < y;) {
           const size_t r = p / row_bytes, in = p - r * row_bytes;
@@ -628,7 +549,7 @@ swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int
     CK(km->d_text.alloc((size_t)std::max<int64_t>(total, 1)));
     kmer_tsv_write_kernel<<<grid, 32 * warps_per_block, 0, ctx->st>>>(km->d_cnt.p, g, km->d_segoff.p, km->d_text.p);
     CK(cudaGetLastError());
-    st = staged_d2h(ctx, km, chunk, km->d_text.p, (size_t)total,
+    st = staged_d2h(ctx, sg, chunk, km->d_text.p, (size_t)total,
                     [&](const char* src, size_t a, size_t b) { return sink(src, b - a, user) == 0; });
     if (st) return st;
   }

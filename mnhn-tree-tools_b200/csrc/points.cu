@@ -19,7 +19,7 @@
 #include <cstring>
 #include <vector>
 
-#include "engine_ctx.cuh"
+#include "staging.cuh"
 
 namespace swgpu {
 namespace {
@@ -245,12 +245,24 @@ swe_status swe_upload_points(swe_ctx* ctx, const float* const* values, int dims,
   const int64_t n_pad = (int64_t)nt * PT_TILE;
   CK(ctx->d_points.alloc((size_t)std::max<int64_t>((int64_t)dims * n_pad, 4)));
   if (dims > 0) {
-    CK(cudaMemsetAsync(ctx->d_points.p, 0, sizeof(float) * dims * n_pad, st));
-    std::vector<float> h((size_t)n_pad);
-    for (int d = 0; d < dims; ++d) {
-      memcpy(h.data(), values[d], sizeof(float) * n);
-      CK(cpy(ctx, ctx->d_points.p + (int64_t)d * n_pad, h.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
-    }
+    // dimension-major rows of n_pad floats (zeros after point n-1), assembled
+    // chunk by chunk in the pinned staging buffers
+    const size_t chunk = stage_chunk(ctx);
+    Staging* sg = nullptr;
+    if (swe_status s = staging_ready(ctx, chunk, &sg)) return s;
+    const size_t row_bytes = sizeof(float) * (size_t)n_pad, used = sizeof(float) * (size_t)n;
+    swe_status s = staged_h2d(ctx, sg, chunk, ctx->d_points.p, row_bytes * dims, [&](char* dst, size_t a, size_t b) {
+      split_copy(a, b, [&](size_t x, size_t y) {
+        for (size_t p = x; p < y;) {
+          const size_t d = p / row_bytes, in = p - d * row_bytes, e = std::min(y, (d + 1) * row_bytes);
+          const size_t real = in < used ? std::min(e - p, used - in) : 0;
+          if (real) memcpy(dst + (p - a), reinterpret_cast<const char*>(values[d]) + in, real);
+          if (e - p > real) memset(dst + (p - a) + real, 0, e - p - real);
+          p = e;
+        }
+      });
+    });
+    if (s) return s;
   }
   std::vector<int2> tiles;
   tiles.reserve((size_t)nt * (nt + 1) / 2);

@@ -47,7 +47,9 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_cli_tools_built():
-    for t in ("cluster_dbscan_SW", "adaptive_clustering_SW", "find_closest_sequence_SW"):
+    for t in ("cluster_dbscan_SW", "adaptive_clustering_SW", "find_closest_sequence_SW", "fasta2kmer",
+              "cluster_dbscan_kmerL1", "cluster_dbscan_kmerL2", "cluster_dbscan_pca", "adaptive_clustering_kmer_L1",
+              "adaptive_clustering_kmer_L2", "adaptive_clustering_PCA"):
         assert (swgpu.BIN_DIR / t).exists()
 
 

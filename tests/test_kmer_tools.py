@@ -112,12 +112,14 @@ def test_empty_and_invalid(eng):
             eng.kmer_counts([b"ACGT"], k, protein)
 
 
-def test_fasta2kmer_main_relinked_on_libswgpu(tmp_path):
-    """The reference's own fasta2kmer.c main() linked against libswgpu.so
-    prints the reference's stdout byte for byte."""
-    exe = O.REF_DIR / "fasta2kmer_on_swgpu"
+@pytest.mark.parametrize("build", ["reference_main", "cli"])
+def test_fasta2kmer_main_relinked_on_libswgpu(tmp_path, build):
+    """The reference's own fasta2kmer.c main() linked against libswgpu.so, and
+    this package's fasta2kmer CLI, print the reference's stdout byte for
+    byte."""
+    exe = O.REF_DIR / "fasta2kmer_on_swgpu" if build == "reference_main" else swgpu.BIN_DIR / "fasta2kmer"
     if not exe.exists():
-        pytest.skip("reference drop-in build not present")
+        pytest.skip("drop-in build not present")
     doc = load_golden("fasta2kmer.json")
     for name in doc["inputs"]:
         W.write_fasta(tmp_path / f"{name}.fa", fasta2kmer_input(doc, name))

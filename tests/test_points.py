@@ -170,13 +170,18 @@ def test_point_dbscan_and_sweep_match_oracle(eng, metric):
 
 
 @pytest.mark.gpu
-def test_point_tools_relinked_on_libswgpu(tmp_path):
+@pytest.mark.parametrize("build", ["reference_main", "cli"])
+def test_point_tools_relinked_on_libswgpu(tmp_path, build):
     """The reference's cluster_dbscan_kmer (L1, L2), cluster_dbscan_pca and
-    adaptive_clustering (kmer L1, L2, PCA) mains on libswgpu reproduce the
-    reference tools' stdout and files byte for byte."""
+    adaptive_clustering (kmer L1, L2, PCA) mains on libswgpu, and this
+    package's own CLIs of the same names, reproduce the reference tools'
+    stdout and files byte for byte."""
+    import swgpu
     doc = load_golden("points.json")
-    if not (O.REF_DIR / "cluster_dbscan_kmerL1_on_swgpu").exists():
-        pytest.skip("reference drop-in builds not present")
+    exe = {r["tool"]: (O.REF_DIR / (r["tool"] + "_on_swgpu") if build == "reference_main" else
+                       swgpu.BIN_DIR / r["tool"]) for r in doc["runs"]}
+    if not all(p.exists() for p in exe.values()):
+        pytest.skip("drop-in builds not present")
     W.write_fasta(tmp_path / "in.fa", _inputs(doc))
     (tmp_path / "proj.txt").write_text(doc["proj"])
     for k, text in doc["kmer"].items():
@@ -184,8 +189,7 @@ def test_point_tools_relinked_on_libswgpu(tmp_path):
     for run in doc["runs"]:
         for old in tmp_path.glob("out_*"):
             old.unlink()
-        r = subprocess.run([str(O.REF_DIR / (run["tool"] + "_on_swgpu"))] + run["args"], cwd=tmp_path,
-                           capture_output=True, timeout=600)
+        r = subprocess.run([str(exe[run["tool"]])] + run["args"], cwd=tmp_path, capture_output=True, timeout=600)
         assert r.returncode == 0, (run["tool"], r.stderr[-300:])
         assert r.stdout.decode() == run["stdout"], run["tool"]
         got = {p.name: p.read_bytes() for p in sorted(tmp_path.glob("out_*"))}

@@ -73,6 +73,9 @@ typedef struct {
   int64_t h2d_bytes;       /* host->device bytes since the last upload began */
   int64_t d2h_bytes;       /* device->host bytes since the last upload began */
   int64_t kernel_launches; /* this library's kernel launches since the last upload began */
+  double ms_last_batch;    /* host time of the last batched DBSCAN (threshold launch, bitmap copies,
+                              order-faithful replays) */
+  double ms_last_replay;   /* the longest single replay of that batch */
 } swe_stats;
 
 const char* swe_strerror(swe_status s);
@@ -152,7 +155,8 @@ swe_status swe_dbscan(swe_ctx* ctx, float eps, int minpts, split_set* out);
    lines go to `log` (stdout when NULL); split sets are written to
    <prefix>%04d unless prefix is NULL.  If out_sets is not NULL it receives a
    malloc'd array of the kept layers (free each with
-   free_split_set_and_associated_clusters, then the array with swe_free). */
+   free_split_set_and_associated_clusters, then the array with swe_free);
+   out_n_sets (if not NULL) receives their number. */
 swe_status swe_adaptive(swe_ctx* ctx, float eps_start, float eps_inc, int minpts, const char* prefix,
                         FILE* log, split_set** out_sets, int* out_n_sets);
 

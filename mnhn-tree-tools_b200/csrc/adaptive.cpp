@@ -91,8 +91,8 @@ SweepMachine::SweepMachine(int n, float eps_start, float eps_inc, int minpts, in
       "epsilon_start: %f\n"
       "epsilon_inc: %f\n",
       minpts, eps_start, eps_inc);
-  req_.assign(1, eps_start_);
   phase_ = FIRST;
+  request_start();
 }
 
 SweepMachine::~SweepMachine() {
@@ -106,24 +106,41 @@ void SweepMachine::fail(int status, const char* why) {
   phase_ = DONE;
 }
 
-void SweepMachine::next_sweep_batch() {
+std::vector<float> SweepMachine::sweep_batch(float* eps_now, bool* terminal) const {
   // the next eps values of the sweep, evaluated together; a value past the
   // largest distance (every later eps gives the same result) or an increment
   // too small to move eps ends the batch, since the reference would loop
   // forever after it
-  req_.clear();
-  terminal_ = false;
+  std::vector<float> out;
+  *terminal = false;
   int room = batch_;
   if (max_steps_ > 0) room = std::min(room, max_steps_ - steps_);
-  while ((int)req_.size() < room) {
-    const float e = eps_now_;
-    eps_now_ = eps_now_ + eps_inc_;
-    req_.push_back(e);
-    if ((fixed_ >= 0 && (key_ ? key_(e) : eps_threshold(e)) >= fixed_) || !(eps_now_ > e)) {
-      terminal_ = true;
+  while ((int)out.size() < room) {
+    const float e = *eps_now;
+    *eps_now = *eps_now + eps_inc_;
+    out.push_back(e);
+    if ((fixed_ >= 0 && (key_ ? key_(e) : eps_threshold(e)) >= fixed_) || !(*eps_now > e)) {
+      *terminal = true;
       break;
     }
   }
+  return out;
+}
+
+void SweepMachine::next_sweep_batch() { req_ = sweep_batch(&eps_now_, &terminal_); }
+
+void SweepMachine::set_speculate(bool on) {
+  speculate_ = on;
+  if (phase_ == FIRST && req_.size() == 1) request_start();
+}
+
+void SweepMachine::request_start() {
+  req_.assign(1, eps_start_);
+  if (!speculate_) return;
+  // the batch next_sweep_batch would request after this start
+  spec_now_ = eps_start_ + eps_inc_;
+  const std::vector<float> more = sweep_batch(&spec_now_, &spec_terminal_);
+  req_.insert(req_.end(), more.begin(), more.end());
 }
 
 void SweepMachine::consume(split_set* res) {
@@ -133,6 +150,7 @@ void SweepMachine::consume(split_set* res) {
     split_set first = res[0];
     if (phase_ == FIRST) say("Initial set obtained with %i clusters\n", first.n_clusters);
     if (first.n_clusters == 1) {
+      for (size_t j = 1; j < count; ++j) free_split_set_and_associated_clusters(res[j]);  // speculative
       if (counter_ == 20 || eps_start_ == 0) {
         say("Error did not find a sufficient starting position in 20 tries \n");
         free_split_set_and_associated_clusters(first);
@@ -143,8 +161,8 @@ void SweepMachine::consume(split_set* res) {
       say("Trying new starting point \n");
       free_split_set_and_associated_clusters(first);
       counter_++;
-      req_.assign(1, eps_start_);
       phase_ = HALVING;
+      request_start();
       return;
     }
     say("Sarting with %i clusters\n", first.n_clusters);
@@ -153,16 +171,28 @@ void SweepMachine::consume(split_set* res) {
     eps_now_ = eps_start_ + eps_inc_;
     phase_ = SWEEP;
     if (max_steps_ > 0 && steps_ >= max_steps_) {
+      for (size_t j = 1; j < count; ++j) free_split_set_and_associated_clusters(res[j]);
       truncated_ = true;
       stop_ = 0;
       req_.clear();
       phase_ = DONE;
       return;
     }
+    if (count > 1) {  // the speculative batch is this sweep's first batch
+      req_.erase(req_.begin());
+      eps_now_ = spec_now_;
+      terminal_ = spec_terminal_;
+      consume_sweep(res + 1, count - 1);
+      return;
+    }
     next_sweep_batch();
     return;
   }
   if (phase_ != SWEEP) return;
+  consume_sweep(res, count);
+}
+
+void SweepMachine::consume_sweep(split_set* res, size_t count) {
   size_t k = 0;
   for (; k < count; ++k) {
     warn(req_[k]);
@@ -253,6 +283,7 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
                    std::vector<split_set>* kept, std::string* err, int max_steps) {
   SweepMachine m(n, eps_start, eps_inc, minpts, max_steps, prov.batch, dbscan_sw_warnings, fixed_point);
   if (prov.key) m.set_key(prov.key);
+  if (prov.speculate) m.set_speculate(true);
   auto flush = [&]() {
     const std::string t = m.take_log();
     if (!t.empty()) fwrite(t.data(), 1, t.size(), log);

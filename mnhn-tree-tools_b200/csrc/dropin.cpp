@@ -237,6 +237,7 @@ void adaptive_dbscan(split_set (*dbscanner)(dataset, float, int), dataset ds, fl
       return swgpu::engine_dbscan_batch(ctx, 0, e, c, minpts, o);
     };
     prov.batch = swgpu::engine_batch_size(ctx, 0);
+    prov.speculate = true;
     size_t mx = 0;
     for (int i = 0; i < ds.n_values; ++i) mx = ds.sequence_lengths[i] > mx ? ds.sequence_lengths[i] : mx;
     fixed = 4LL * (long long)mx;
@@ -254,6 +255,7 @@ void adaptive_dbscan(split_set (*dbscanner)(dataset, float, int), dataset ds, fl
     };
     prov.batch = swgpu::engine_batch_size(ctx, 0);
     prov.key = [ctx](float e) { return swgpu::engine_sweep_key(ctx, e); };
+    prov.speculate = true;
     fixed = swgpu::engine_fixed_point(ctx);
     engine = true;
   } else {

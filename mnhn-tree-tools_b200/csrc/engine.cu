@@ -960,6 +960,7 @@ swe_status swe_adaptive_set(swe_ctx* ctx, int set, float eps_start, float eps_in
   };
   prov.batch = engine_batch_size(ctx, set);
   prov.key = [ctx](float e) { return ctx_sweep_key(ctx, e); };
+  prov.speculate = true;
   std::vector<split_set> kept;
   std::string err;
   const long long fixed = ctx_fixed_point(ctx);
@@ -970,6 +971,7 @@ swe_status swe_adaptive_set(swe_ctx* ctx, int set, float eps_start, float eps_in
     for (auto& s : kept) free_split_set_and_associated_clusters(s);
     return fail(ctx, (swe_status)rc, err);
   }
+  if (out_n_sets) *out_n_sets = (int)kept.size();
   if (out_sets) {
     split_set* arr = (split_set*)malloc(sizeof(split_set) * std::max<size_t>(kept.size(), 1));
     if (!arr) {
@@ -1051,6 +1053,7 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
     m[k].reset(new SweepMachine(ctx->set_first[k + 1] - ctx->set_first[k], eps_start, eps_inc, minpts, max_steps,
                                 batch, true, fixed));
     m[k]->set_key([ctx](float e) { return ctx_sweep_key(ctx, e); });
+    m[k]->set_speculate(true);
   }
   auto finish_set = [&](int k) {
     std::vector<split_set> kept;
@@ -1349,6 +1352,7 @@ int engine_batch_size(const swe_ctx* ctx, int set) {
 int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int minpts, split_set* out) {
   for (int k = 0; k < count; ++k) out[k] = split_set{0, nullptr};
   if (swe_status s = check_set(ctx, set)) return s;
+  const auto t_begin = std::chrono::steady_clock::now();
   if (minpts == -1) minpts = 5;  // dbscan.c:985-989
   const int first = ctx->set_first[set], n = ctx->set_first[set + 1] - first;
   const int wpr = (n + 63) / 64;
@@ -1366,10 +1370,11 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
   CK(ctx->h_bbits.alloc(std::max<size_t>(words * U, 1)));
   CK(ctx->h_bcounts.alloc(std::max<size_t>((size_t)n * U, 1)));
   // thresholds >= 0 first (one launch reads the matrix once for all of them)
-  std::vector<int> launch_idx, none_idx;
+  std::vector<int> launch_idx, none_idx, launch_of(U, -1);
   std::vector<long long> launchT;
   for (int u = 0; u < U; ++u) {
     if (uniq[u] >= 0 && n > 0) {
+      launch_of[u] = (int)launch_idx.size();
       launch_idx.push_back(u);
       launchT.push_back(uniq[u]);
     } else {
@@ -1381,7 +1386,15 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
     if (n) memset(ctx->h_bcounts.p + (size_t)n * u, 0, sizeof(int) * n);
   }
   const int UL = (int)launch_idx.size();
-  float ms = 0;
+  // one event per bitmap copy: each replay starts as soon as its bitmap is on the host
+  std::vector<cudaEvent_t> ready(UL, nullptr);
+  struct EventGuard {
+    std::vector<cudaEvent_t>& ev;
+    ~EventGuard() {
+      for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+    }
+  } guard{ready};
   if (UL > 0) {
     CK(ctx->d_bbits.alloc(words * UL));
     CK(ctx->d_bcounts.alloc((size_t)n * UL));
@@ -1392,33 +1405,51 @@ int engine_dbscan_batch(swe_ctx* ctx, int set, const float* eps, int count, int 
     if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bbits.p, ctx->d_bcounts.p)) return st;
     for (int j = 0; j < UL; ++j) {
       const int u = launch_idx[j];
-      CK(cpy(ctx, ctx->h_bbits.p + words * u, ctx->d_bbits.p + words * j, words * 8, cudaMemcpyDeviceToHost,
-             ctx->st));
+      CK(cudaEventCreateWithFlags(&ready[j], cudaEventDisableTiming));
       CK(cpy(ctx, ctx->h_bcounts.p + (size_t)n * u, ctx->d_bcounts.p + (size_t)n * j, sizeof(int) * n,
              cudaMemcpyDeviceToHost, ctx->st));
+      CK(cpy(ctx, ctx->h_bbits.p + words * u, ctx->d_bbits.p + words * j, words * 8, cudaMemcpyDeviceToHost,
+             ctx->st));
+      CK(cudaEventRecord(ready[j], ctx->st));
     }
-    CK(cudaStreamSynchronize(ctx->st));
-    if (swe_status st = thr_status(ctx)) return st;
+  }
+  // one order-faithful replay per distinct threshold, in parallel, each after its copy
+  std::vector<split_set> res(U, split_set{0, nullptr});
+  std::vector<int> rc(U, 0);
+  std::vector<double> replay_ms(U, 0.0);
+  std::vector<std::thread> th;
+  for (int u = 0; u < U; ++u)
+    th.emplace_back([&, u]() {
+      if (launch_of[u] >= 0 && cudaEventSynchronize(ready[launch_of[u]]) != cudaSuccess) {
+        rc[u] = SWE_ERR_CUDA;
+        return;
+      }
+      const auto t0 = std::chrono::steady_clock::now();
+      rc[u] = dbscan_replay_bitmap(n, ctx->h_bbits.p + words * u, wpr, ctx->h_bcounts.p + (size_t)n * u, minpts,
+                                   &res[u]);
+      replay_ms[u] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    });
+  for (auto& t : th) t.join();
+  CK(cudaStreamSynchronize(ctx->st));
+  float ms = 0;
+  if (UL > 0) {
+    if (swe_status st = thr_status(ctx)) {
+      for (auto& s : res) free_split_set_and_associated_clusters(s);
+      return st;
+    }
     CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
   }
   ctx->stats.ms_last_neighbors = ms;
   ctx->stats.last_neighbor_launches = UL > 0 ? 1 : 0;
-  // one order-faithful replay per distinct threshold, in parallel
-  std::vector<split_set> res(U, split_set{0, nullptr});
-  std::vector<int> rc(U, 0);
-  std::vector<std::thread> th;
-  for (int u = 0; u < U; ++u)
-    th.emplace_back([&, u]() {
-      rc[u] = dbscan_replay_bitmap(n, ctx->h_bbits.p + words * u, wpr, ctx->h_bcounts.p + (size_t)n * u, minpts,
-                                   &res[u]);
-    });
-  for (auto& t : th) t.join();
   int bad = 0;
   for (int u = 0; u < U; ++u) bad = bad ? bad : rc[u];
   if (bad) {
     for (auto& s : res) free_split_set_and_associated_clusters(s);
-    return fail(ctx, (swe_status)bad, "dbscan replay");
+    return fail(ctx, (swe_status)bad, bad == SWE_ERR_CUDA ? "bitmap copy" : "dbscan replay");
   }
+  ctx->stats.ms_last_replay = U ? *std::max_element(replay_ms.begin(), replay_ms.end()) : 0.0;
+  ctx->stats.ms_last_batch =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
   std::vector<bool> used(U, false);
   for (int k = 0; k < count; ++k) {
     const int u = slot[k];

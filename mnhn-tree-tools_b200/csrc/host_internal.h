@@ -34,6 +34,9 @@ struct DbscanProvider {
   int batch = 1;
   // the sweep key of an eps (see SweepMachine::set_key); empty = eps_threshold
   std::function<long long(float)> key;
+  // run without side effects, so the sweep may evaluate eps values
+  // speculatively (SweepMachine::set_speculate)
+  bool speculate = false;
 };
 
 // Adaptive sweep of dbscan.c:1117-1380 as a state machine: request() holds
@@ -60,7 +63,15 @@ class SweepMachine {
   ~SweepMachine();
   SweepMachine(const SweepMachine&) = delete;
   SweepMachine& operator=(const SweepMachine&) = delete;
-  void set_key(std::function<long long(float)> key) { key_ = std::move(key); }
+  void set_key(std::function<long long(float)> key) {
+    key_ = std::move(key);
+    if (phase_ == FIRST) request_start();
+  }
+  // With speculation the request for a starting eps also holds the sweep
+  // batch that follows it when that start gives more than one cluster (the
+  // usual case): one round less.  The results of a start with one cluster are
+  // discarded.  Only for providers without side effects (the engine).
+  void set_speculate(bool on);
   bool done() const { return phase_ == DONE; }
   const std::vector<float>& request() const { return req_; }
   void consume(split_set* res);
@@ -78,12 +89,18 @@ class SweepMachine {
   void warn(float eps);
   void fail(int status, const char* why);
   void next_sweep_batch();
+  std::vector<float> sweep_batch(float* eps_now, bool* terminal) const;
+  void request_start();
+  void consume_sweep(split_set* res, size_t count);
   int n_;
   float eps_start_, eps_inc_;
   int minpts_, max_steps_, batch_;
   bool warnings_;
   long long fixed_;
   std::function<long long(float)> key_;
+  bool speculate_ = false;
+  float spec_now_ = 0;     // eps_now_ after the speculative batch
+  bool spec_terminal_ = false;
   Phase phase_ = FIRST;
   std::vector<float> req_;
   std::vector<split_set> sets_;

@@ -68,7 +68,7 @@ class Stats(C.Structure):
                 ("ms_fast_kernel", C.c_double), ("ms_last_neighbors", C.c_double),
                 ("last_neighbor_launches", C.c_int64),
                 ("dist_bytes", C.c_int), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
-                ("kernel_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("ms_last_batch", C.c_double), ("ms_last_replay", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -376,19 +376,22 @@ class Engine:
         lib().swe_free(cols)
         return row_ptr, c
 
-    def dbscan(self, eps: float, minpts: int, set: int | None = None):
+    def dbscan(self, eps: float, minpts: int, set: int | None = None, lists: bool = True):
+        """Clusters as member lists, or their number with lists=False."""
         s = SplitSet()
         if set is None:
             _check(lib().swe_dbscan(self.ctx, C.c_float(eps), minpts, C.byref(s)), self.ctx)
         else:
             _check(lib().swe_dbscan_set(self.ctx, set, C.c_float(eps), minpts, C.byref(s)), self.ctx)
-        out = split_set_to_lists(s)
+        out = split_set_to_lists(s) if lists else s.n_clusters
         lib().free_split_set_and_associated_clusters(s)
         return out
 
     def adaptive(self, eps_start: float, eps_inc: float, minpts: int, prefix: str | None = None,
-                 log_path: str | None = None, set: int | None = None):
-        """Runs the sweep; returns (log text, kept split sets as lists)."""
+                 log_path: str | None = None, set: int | None = None, layers: bool = True):
+        """Runs the sweep; returns (log text, kept split sets as lists), or
+        (log text, number of kept layers) with layers=False (the layers stay
+        in the library and are freed there)."""
         libc = C.CDLL(None)
         libc.fopen.restype = C.c_void_p
         libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
@@ -403,17 +406,20 @@ class Engine:
         sets = C.POINTER(SplitSet)()
         nsets = C.c_int()
         pre = prefix.encode() if prefix else None
+        out = C.byref(sets) if layers else None
         if set is None:
             st = lib().swe_adaptive(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts, pre, f,
-                                    C.byref(sets), C.byref(nsets))
+                                    out, C.byref(nsets))
         else:
             st = lib().swe_adaptive_set(self.ctx, set, C.c_float(eps_start), C.c_float(eps_inc), minpts, pre, f,
-                                        C.byref(sets), C.byref(nsets))
+                                        out, C.byref(nsets))
         libc.fclose(f)
         text = Path(log_path).read_text()
         if tmp:
             os.unlink(tmp)
         _check(st, self.ctx)
+        if not layers:
+            return text, nsets.value
         kept = [split_set_to_lists(sets[k]) for k in range(nsets.value)]
         for k in range(nsets.value):
             lib().free_split_set_and_associated_clusters(sets[k])

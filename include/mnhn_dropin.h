@@ -139,6 +139,36 @@ void free_dataset(dataset ds);
 void create_single_cluster_file_with_values(char* filename, cluster cl, dataset ds);
 void create_cluster_files_with_values(char* prefix, split_set s, dataset ds);
 
+/* ---- split-set trees (cluster.h, volumes.h): split_sets_to_newick, tree_pureness ---- */
+
+/* cluster_io.c:124-189: the tree of n_layers split sets linked by the
+   relations c[i-1] = generate_split_set_relation(sets[i-1], sets[i]); branch
+   lengths tree_lengths[layer] (1 when NULL, 0 for the last layer).  Returns
+   the first node of the last layer. */
+tree_node* generate_tree(int n_layers, cluster_connections** c, split_set* sets, double* tree_lengths);
+/* cluster_io.c:217-235: Newick text to f; the ":length" parts go to stdout,
+   as in the reference. */
+void print_tree(FILE* f, tree_node* root);
+/* cluster_io.c:191-215: clusters with at least min_size members (ids renumbered). */
+split_set filtered_split_set_by_min_size(split_set s_in, int min_size);
+/* cluster_io.c:14-24: array[i] - array[i+1] (array_length - 1 values, malloc'd). */
+double* array_deltas(double* array, int array_length);
+/* cluster_io.c:26-93: epsilon_start and the "Epsilon at layer" values of an
+   adaptive-clustering log (n_layers values); NULL (with a message) where the
+   reference exits. */
+double* get_epsilon_dist_from_adaptive_clustering_output(FILE* f, int n_layers);
+/* cluster_io.c:95-122: min_points / volume(eps) with the hypercube (type 1)
+   or hypersphere (type 2) volume of volumes.c. */
+double* densities_from_epsilons(int type, int dimensions, double* epsilons, int n_epsilons, int min_points);
+double vol_hypersphere(int dimension, double epsilon);
+double vol_hypercube(int dimension, double epsilon);
+/* cluster_io.c:237-340: per-layer pureness against a target split set, the
+   impure clusters per layer, and the layer/target cluster-count factors. */
+int pureness_from_tree(int n_layers, tree_node* root, split_set* s, split_set target, double** pureness_values,
+                       int** inpure_clusters);
+double* inpures_over_total_fraction(int n_layers, split_set* s, int* inpure_clusters);
+double* clusters_in_layer_vs_target_clusters(int n_layers, split_set* s, split_set target);
+
 /* ---- fasta2kmer (kmers.h) ---- */
 
 /* kmers.c:292-371: one row of swe_kmer_count(kmer_length, protein) counts per

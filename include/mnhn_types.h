@@ -9,6 +9,7 @@
  *   neighbors            dbscan.h:5-8
  *   kmer_frequencies     kmers.h:17-21
  *   data_shape           dataset.h:37-40
+ *   tree_node            cluster.h:41-48
  *
  * Ownership follows the reference: arrays inside returned structs come from
  * malloc and are released with free() (free_split_set_and_associated_clusters,
@@ -59,6 +60,17 @@ typedef struct {
   size_t n_features;
   size_t n_samples;
 } data_shape;
+
+/* cluster.h:41-48: a node of the layer tree (id "L<layer>C<cluster>N<members>",
+   the root "L<layer>C0"; length of the branch to the parent). */
+typedef struct tree_node {
+  char* id;
+  double length;
+  int n_members;
+  struct tree_node* child;
+  struct tree_node* neighbor;
+  struct tree_node* parent;
+} tree_node;
 
 /* kmers.h:17-21: frequencies[sequence][k-mer index], one malloc'd row per
    sequence (free_kmer_frequencies releases them). */

@@ -433,6 +433,44 @@ def points_golden():
     (OUT / "points.json").write_text(json.dumps(doc))
 
 
+def tree_golden():
+    """The reference's split-set tree tools (split_sets_to_newick, tree_pureness,
+    filter_split_sets_by_min, split_set_to_fasta, built from its sources into
+    oracle/_ref) on the layers and logs of two adaptive_clustering_SW golden
+    runs (adaptive_small.json): stdout and files.  filter_split_sets_by_min
+    stores cluster ids the reference never sets (cluster_io.c:191-215); they
+    come from malloc'd memory, i.e. the STALE_ENV pattern here, and are not
+    compared."""
+    src = json.loads((OUT / "adaptive_small.json").read_text())
+    doc = {"source": "adaptive_small.json", "runs": []}
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        W.write_fasta(d / "in.fa", [s.encode() for s in src["seqs"]])
+        for ri in (1, 3):
+            run = src["runs"][ri]
+            names = sorted(run["files"])
+            for nm in names:
+                (d / f"r{ri}_{nm}").write_bytes(base64.b64decode(run["files"][nm]))
+            (d / f"r{ri}.log").write_text(run["stdout"])
+            layers = [f"r{ri}_{nm}" for nm in names]
+            cases = [("split_sets_to_newick", ["0", "0"] + layers),
+                     ("split_sets_to_newick", ["3", "0"] + layers),
+                     ("split_sets_to_newick", ["0", "1", "2", f"r{ri}.log", "5"] + layers),
+                     ("split_sets_to_newick", ["2", "2", "3", f"r{ri}.log", "5"] + layers),
+                     ("tree_pureness", ["in.fa", layers[1]] + layers),
+                     ("filter_split_sets_by_min", ["4", "out_f"] + layers),
+                     ("split_set_to_fasta", ["in.fa", layers[-2], "out_s"])]
+            for tool, args in cases:
+                for old in d.glob("out_*"):
+                    old.unlink()
+                rc, out = run_tool(tool, args, d, env=STALE_ENV)
+                assert rc == 0, (tool, args, out[-300:])
+                doc["runs"].append({"source_run": ri, "tool": tool, "args": args, "stdout": out,
+                                    "files": files_b64(d, "out_")})
+                print(tool, args[:3], out[:80].replace("\n", "|"), len(doc["runs"][-1]["files"]))
+    (OUT / "trees.json").write_text(json.dumps(doc))
+
+
 def score_callers_golden():
     """stdout of the reference's compareSW, silhouette, compare_norms and
     find_satellite (built from its sources into oracle/_ref, one thread) on
@@ -470,7 +508,7 @@ if __name__ == "__main__":
     if not O.ref_available():
         O.build()
     which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
-                             "kmer", "callers", "fasta2kmer", "points"]
+                             "kmer", "callers", "fasta2kmer", "points", "trees"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -495,3 +533,5 @@ if __name__ == "__main__":
         fasta2kmer_golden()
     if "points" in which:
         points_golden()
+    if "trees" in which:
+        tree_golden()

@@ -209,6 +209,16 @@ swe_status swe_get_stats(const swe_ctx* ctx, swe_stats* out);
 swe_status swe_dbscan_bitmap(int n, const uint64_t* bits, int words_per_row, const int* counts, int minpts,
                              split_set* out);
 
+/* The adaptive sweep (dbscan.c:1117-1380 semantics) over a distance matrix the
+   caller holds (row-major n x n, the neighbour test (float)d <= eps); host
+   only, no GPU involved.  batch is the number of eps values evaluated per
+   round; with speculate != 0 the round of the starting eps also evaluates the
+   sweep batch that follows it (the engine's sweeps do both).  Log, files and
+   out_sets as swe_adaptive. */
+swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_start, float eps_inc, int minpts,
+                               const char* prefix, FILE* log, int speculate, int batch, split_set** out_sets,
+                               int* out_n_sets);
+
 /* Measures, on `device`, the issue rate of the 16x2 kernel's per-cell
    instruction mix (one PRMT, three packed add-max, one packed max) on
    independent chains: *cells_per_s DP cells per second (two per packed

@@ -311,3 +311,58 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
 }
 
 }  // namespace swgpu
+
+extern "C" swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_start, float eps_inc, int minpts,
+                                          const char* prefix, FILE* log, int speculate, int batch,
+                                          split_set** out_sets, int* out_n_sets) {
+  if (n < 0 || (n > 0 && !D) || batch < 1) return SWE_ERR_INVALID;
+  const int wpr = (n + 63) / 64;
+  const size_t words = (size_t)n * (size_t)wpr;
+  uint32_t dmax = 0;
+  for (size_t i = 0; i < (size_t)n * (size_t)n; ++i) dmax = D[i] > dmax ? D[i] : dmax;
+  swgpu::DbscanProvider prov;
+  prov.batch = batch;
+  prov.speculate = speculate != 0;
+  prov.run = [&](const float* eps, int count, split_set* out) -> int {
+    std::vector<uint64_t> bits(std::max<size_t>(words, 1));
+    std::vector<int> counts(std::max(n, 1));
+    for (int k = 0; k < count; ++k) {
+      const long long T = swgpu::eps_threshold(eps[k] == -1 ? 0.015f : eps[k]);  // dbscan.c:980-984
+      std::fill(bits.begin(), bits.end(), 0);
+      for (int i = 0; i < n; ++i) {
+        int c = 0;
+        for (int j = 0; j < n && T >= 0; ++j)
+          if ((long long)D[(size_t)i * n + j] <= T) {
+            bits[(size_t)i * wpr + (j >> 6)] |= 1ull << (j & 63);
+            ++c;
+          }
+        counts[i] = c;
+      }
+      const int rc = swgpu::dbscan_replay_bitmap(n, bits.data(), wpr, counts.data(), minpts == -1 ? 5 : minpts,
+                                                 &out[k]);
+      if (rc) return rc;
+    }
+    return 0;
+  };
+  std::vector<split_set> kept;
+  std::string err;
+  const int rc = swgpu::adaptive_sweep(n, eps_start, eps_inc, minpts, prefix, log ? log : stdout, prov, true,
+                                       (long long)dmax, &kept, &err);
+  if (out_n_sets) *out_n_sets = (int)kept.size();
+  if (rc) {
+    for (auto& s : kept) free_split_set_and_associated_clusters(s);
+    return (swe_status)rc;
+  }
+  if (out_sets) {
+    split_set* arr = (split_set*)malloc(sizeof(split_set) * std::max<size_t>(kept.size(), 1));
+    if (!arr) {
+      for (auto& s : kept) free_split_set_and_associated_clusters(s);
+      return SWE_ERR_OOM;
+    }
+    for (size_t k = 0; k < kept.size(); ++k) arr[k] = kept[k];
+    *out_sets = arr;
+  } else {
+    for (auto& s : kept) free_split_set_and_associated_clusters(s);
+  }
+  return SWE_OK;
+}

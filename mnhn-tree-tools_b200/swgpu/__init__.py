@@ -127,7 +127,7 @@ EXPORTS = [
     "swe_kmer_features", "swe_prefilter_init", "swe_prefilter_param_count", "swe_prefilter_params",
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
-    "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points",
+    "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -241,6 +241,9 @@ def lib():
         L.read_split_set.restype = SplitSet
         L.read_split_set.argtypes = [C.c_char_p]
         L.swgpu_last_dropin_status.restype = C.c_int
+        L.swe_adaptive_matrix.restype = C.c_int
+        L.swe_adaptive_matrix.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_void_p,
+                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.swe_upload_points.restype = C.c_int
         L.swe_upload_points.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.swe_kmer_count.restype = C.c_int64
@@ -593,6 +596,37 @@ def dbscan_from_matrix(D: np.ndarray, eps: float, minpts: int):
     out = split_set_to_lists(s)
     lib().free_split_set_and_associated_clusters(s)
     return out
+
+
+def adaptive_from_matrix(D: np.ndarray, eps_start: float, eps_inc: float, minpts: int, speculate: bool = True,
+                         batch: int = 8, prefix: str | None = None):
+    """The adaptive sweep on the host over a distance matrix the caller holds
+    (swe_adaptive_matrix); returns (log text, kept split sets as lists)."""
+    import tempfile
+    D = np.ascontiguousarray(D, dtype=np.uint32)
+    n = D.shape[0]
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    fd, tmp = tempfile.mkstemp(prefix="swgpu_log_")
+    os.close(fd)
+    f = libc.fopen(tmp.encode(), b"w")
+    sets = C.POINTER(SplitSet)()
+    nsets = C.c_int()
+    st = lib().swe_adaptive_matrix(n, D.ctypes.data, C.c_float(eps_start), C.c_float(eps_inc), minpts,
+                                   prefix.encode() if prefix else None, f, int(speculate), batch, C.byref(sets),
+                                   C.byref(nsets))
+    libc.fclose(f)
+    text = Path(tmp).read_text()
+    os.unlink(tmp)
+    if st != 0:
+        return text, None
+    kept = [split_set_to_lists(sets[k]) for k in range(nsets.value)]
+    for k in range(nsets.value):
+        lib().free_split_set_and_associated_clusters(sets[k])
+    lib().swe_free(sets)
+    return text, kept
 
 
 def measure_mix_peak(device: int = 0):

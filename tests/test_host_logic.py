@@ -261,3 +261,34 @@ def test_cluster_files_match_reference(tmp_path):
     L.create_cluster_files(str(tmp_path / "cl").encode(), s, buf.dataset())
     got = {p.name: base64.b64encode(p.read_bytes()).decode() for p in sorted(tmp_path.glob("cl-*"))}
     assert got == doc["files"]
+
+
+@pytest.mark.parametrize("speculate,batch", [(False, 1), (True, 1), (True, 3), (True, 8)])
+def test_sweep_batches_and_speculation_match_reference(tmp_path, speculate, batch):
+    """The sweep state machine the engine drives (rounds of `batch` eps values,
+    and the starting eps evaluated together with the batch after it) over the
+    oracle's matrix reproduces the reference's adaptive_clustering_SW log and
+    split-set files for every golden run, halving starts included."""
+    doc = load_golden("adaptive_small.json")
+    seqs = [s.encode() for s in doc["seqs"]]
+    D = O.all_pairs(seqs)
+    for k, run in enumerate(doc["runs"]):
+        prefix = str(tmp_path / f"s{int(speculate)}b{batch}r{k}_layer")
+        text, kept = swgpu.adaptive_from_matrix(D, run["eps_start"], run["eps_inc"], run["minpts"],
+                                                speculate=speculate, batch=batch, prefix=prefix)
+        assert "Dataset read!\n" + text == run["stdout"], (k, speculate, batch)
+        got = {p.name.split("_", 1)[1]: base64.b64encode(p.read_bytes()).decode()
+               for p in sorted(tmp_path.glob(f"s{int(speculate)}b{batch}r{k}_layer*"))}
+        assert got == run["files"], (k, speculate, batch)
+
+
+def test_sweep_speculation_through_halving():
+    # a start with one cluster: the speculative batch is discarded and the start halved
+    rng = np.random.default_rng(4)
+    pts = np.concatenate([rng.normal(c, 1.0, size=(40, 2)) for c in (0, 12, 30)])
+    D = np.round(np.sqrt(((pts[:, None] - pts[None]) ** 2).sum(-1)) * 10).astype(np.uint32)
+    for start in (400.0, 900.0):
+        want = O.adaptive(D, start, 7.0, 4)
+        for batch in (1, 5):
+            got = swgpu.adaptive_from_matrix(D, start, 7.0, 4, speculate=True, batch=batch)
+            assert got[0] == want[0] and got[1] == want[1], (start, batch)

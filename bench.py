@@ -427,13 +427,22 @@ def run_gpu(args):
 
     wl = WORKLOADS[args.config]
     gen = getattr(W, wl["gen"])
-    seqs, _ = gen(seed=dataset_seed(args.config, rank))
+    split = bool(args.split)  # one data set over all ranks (strong scaling) instead of one per rank
+    seqs, _ = gen(seed=dataset_seed(args.config, 0 if split else rank))
     if args.n:
         seqs = seqs[:args.n]
     cells = W.cells(seqs)
     eng = swgpu.Engine(device=dev)
+    if split:
+        from swgpu import split_pass
+        eng.set_partition(rank, world)
     eng.upload(seqs)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def score():
+        eng.score_all_pairs()
+        if split and world > 1:  # the one exchange: bytewise minimum of the ranks' matrices
+            split_pass.combine_parts(eng, dist, f"cuda:{dev}")
 
     def barrier():
         if dist:
@@ -449,7 +458,7 @@ def run_gpu(args):
 
     def step():
         eng.timer_start()
-        eng.score_all_pairs()
+        score()
         kept = cluster()
         return eng.timer_stop(), kept
 
@@ -478,7 +487,7 @@ def run_gpu(args):
     total_ms = sum(step_ms)
     total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
     ms_per_step = total_ms / args.steps
-    value = cells * world / (ms_per_step * 1e-3) / 1e9
+    value = cells * (1 if split else world) / (ms_per_step * 1e-3) / 1e9
     launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
 
     # the eps threshold kernel alone (HBM-bound): one launch per distinct
@@ -496,20 +505,20 @@ def run_gpu(args):
         barrier()
         t0 = time.perf_counter()
         eng.upload(seqs)
-        eng.score_all_pairs()
+        score()
         cluster()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     b1 = eng.stats()
     e2e_total = sum(e2e_ms)
     e2e_total = max_over_ranks(e2e_total, dist, f"cuda:{dev}")
-    e2e_value = cells * world / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
+    e2e_value = cells * (1 if split else world) / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
     # upload() resets the counters, so the last step's totals are the per-step figures
     h2d = b1["h2d_bytes"]
     d2h = b1["d2h_bytes"]
 
     if rank == 0:
         kms = statistics.median(kernel_ms)
-        fast_gcups = st1["cells"] / (kms * 1e-3) / 1e9
+        fast_gcups = st1["cells"] / (world if split else 1) / (kms * 1e-3) / 1e9
         peak_cells, peak_instr = swgpu.measure_mix_peak(dev)
         # R = 2 * P_int / K: P_int = lane instructions/s of the per-cell mix at full
         # issue on this GPU, K = 4.5 instructions per packed cell pair in that mix
@@ -527,12 +536,12 @@ def run_gpu(args):
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "s16x2", "data": "synthetic",
+            "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "s16x2", "data": "synthetic",
             "config": {"workload": wl["text"], "n_sequences": len(seqs), "cells_per_gpu": cells,
                        "pairs_per_gpu": len(seqs) * (len(seqs) - 1) // 2,
                        "kept_layers" if wl["mode"] == "adaptive" else "clusters":
                            kept,
-                       "parallelism": f"{world} independent datasets (one per GPU)",
+                       "parallelism": (f"one dataset split over {world} GPUs (cost-balanced tile groups, one all-reduce)" if split else f"{world} independent datasets (one per GPU)"),
                        "l2": "256 MB buffer written between timed steps (L2 flush); distance matrix 800 MB"},
             "dbscan_sec": round(ms_per_step * 1e-3, 4),
             "rerun_pairs": int(st1["reruns"]),
@@ -921,6 +930,9 @@ def main():
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
     ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
+    ap.add_argument("--split", action="store_true",
+                    help="config 2/3: one data set split over all ranks (strong scaling: tile groups and one "
+                         "all-reduce of the matrix) instead of one data set per rank")
     ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer and k-mer DBSCAN legs")
     ap.add_argument("--leg", choices=["fasta2kmer", "kmer_dbscan"],
                     help="run one side leg alone on the config-2 reads (the first --n) and print its object")

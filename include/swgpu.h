@@ -119,6 +119,26 @@ int swe_set_count(const swe_ctx* ctx);
 #define SWE_METRIC_L2 2
 swe_status swe_upload_points(swe_ctx* ctx, const float* const* values, int dims, int n, int metric);
 
+/* One data set's score pass split over processes (one per GPU).  The tiles of
+   the pass, in descending cost, go one by one to the least loaded of `nparts`
+   groups (swe_lpt_partition), identically in every process, and this context
+   scores group `part` plus every pair of the 32-bit path; its other pairs hold
+   0xFF bytes.  Each pair is scored by exactly one group, so the bytewise
+   minimum of all processes' distance storage (an all-reduce with the minimum
+   over bytes, e.g. NCCL's ncclMin on ncclUint8, through swe_distance_copy) is
+   the full matrix; after copying it back every call below works as after a
+   whole pass.  nparts = 1 (the default) is the whole pass.  Applies to the
+   current and later uploads. */
+swe_status swe_set_partition(swe_ctx* ctx, int part, int nparts);
+/* Bytes of the distance storage of the current upload, and a device-to-device
+   copy of it to (to_engine = 0) or from (to_engine = 1) a buffer of that size
+   on the context's device. */
+int64_t swe_distance_bytes(const swe_ctx* ctx);
+swe_status swe_distance_copy(swe_ctx* ctx, void* dev_buf, int to_engine);
+/* The assignment swe_set_partition uses: owner[t] for costs cost[0..n) given
+   in descending order. */
+void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
+
 /* Scores every pair of the uploaded sequences into the device distance matrix
    (one pass; later neighbour/DBSCAN calls reuse it). */
 swe_status swe_score_all_pairs(swe_ctx* ctx);

@@ -310,6 +310,17 @@ int adaptive_sweep(int n, float eps_start, float eps_inc, int minpts, const char
   return 0;
 }
 
+void lpt_partition(const double* cost, int64_t n, int nparts, int* owner) {
+  std::vector<double> load((size_t)std::max(nparts, 1), 0.0);
+  for (int64_t t = 0; t < n; ++t) {
+    int best = 0;
+    for (int p = 1; p < nparts; ++p)
+      if (load[p] < load[best]) best = p;
+    owner[t] = best;
+    load[best] += cost[t];
+  }
+}
+
 }  // namespace swgpu
 
 extern "C" swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_start, float eps_inc, int minpts,
@@ -365,4 +376,9 @@ extern "C" swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_st
     for (auto& s : kept) free_split_set_and_associated_clusters(s);
   }
   return SWE_OK;
+}
+
+extern "C" void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner) {
+  if (!cost || !owner || n <= 0 || nparts < 1) return;
+  swgpu::lpt_partition(cost, n, nparts, owner);
 }

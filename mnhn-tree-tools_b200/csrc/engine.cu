@@ -160,6 +160,39 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
   return SWE_OK;
 }
 
+static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand);
+
+swe_status swe_set_partition(swe_ctx* ctx, int part, int nparts) {
+  if (!ctx || nparts < 1 || part < 0 || part >= nparts) return SWE_ERR_INVALID;
+  if (ctx->part == part && ctx->nparts == nparts) return SWE_OK;
+  ctx->part = part;
+  ctx->nparts = nparts;
+  if (ctx->metric != 0 || ctx->n == 0 || ctx->n_sets == 0) return SWE_OK;  // applies at the next upload
+  if (swe_status s = select_device(ctx)) return s;
+  return build_layout(ctx, nullptr, nullptr);
+}
+
+int64_t swe_distance_bytes(const swe_ctx* ctx) {
+  if (!ctx || ctx->n_sets == 0) return 0;
+  return (int64_t)ctx->set_base[ctx->n_sets] * ctx->dist_bytes;
+}
+
+swe_status swe_distance_copy(swe_ctx* ctx, void* dev_buf, int to_engine) {
+  if (!ctx || (!dev_buf && swe_distance_bytes(ctx) > 0)) return SWE_ERR_INVALID;
+  const size_t bytes = (size_t)swe_distance_bytes(ctx);
+  if (bytes == 0) return SWE_OK;
+  if (swe_status s = select_device(ctx)) return s;
+  void* D = ctx->dist_bytes == 2 ? (void*)ctx->d_D16.p : (void*)ctx->d_D32.p;
+  if (!D) return fail(ctx, SWE_ERR_STATE, "no distance storage");
+  CK(cudaMemcpyAsync(to_engine ? D : dev_buf, to_engine ? dev_buf : D, bytes, cudaMemcpyDeviceToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (to_engine) {
+    ctx->bits_T = LLONG_MIN;  // cached neighbour bitmaps no longer match
+    ctx->bits_set = -1;
+  }
+  return SWE_OK;
+}
+
 void swe_destroy(swe_ctx* ctx) { delete ctx; }
 
 // Layout view of the device tables for the kernels.
@@ -347,8 +380,18 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
     std::iota(idx.begin(), idx.end(), 0);
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     std::vector<FastTile> sorted(ctx->tiles.size());
-    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]];
+    std::vector<double> sorted_cost(ctx->tiles.size());
+    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]], sorted_cost[k] = cost[idx[k]];
     ctx->tiles.swap(sorted);
+    if (ctx->nparts > 1) {  // this process's share of the tiles
+      std::vector<int> owner(ctx->tiles.size());
+      lpt_partition(sorted_cost.data(), (int64_t)sorted_cost.size(), ctx->nparts, owner.data());
+      std::vector<FastTile> mine;
+      tile_cells = 0;
+      for (size_t k = 0; k < ctx->tiles.size(); ++k)
+        if (owner[k] == ctx->part) mine.push_back(ctx->tiles[k]), tile_cells += 2.0 * sorted_cost[k];
+      ctx->tiles.swap(mine);
+    }
   }
   ctx->max_cols = cta_warps * 4;
   ctx->smem = fast_smem_bytes(ctx->max_block_rows, ctx->max_cols, PB);
@@ -546,7 +589,8 @@ static swe_status build_score_graph(swe_ctx* ctx) {
   const DistLayout L = layout(ctx);
   CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemsetAsync(ctx->d_ctr.p, 0, 4 * sizeof(unsigned), st);
-  if (e == cudaSuccess && ctx->masked) {  // pairs outside the candidate tiles read as the largest value
+  if (e == cudaSuccess && (ctx->masked || ctx->nparts > 1)) {
+    // pairs outside the scored tiles read as the largest value (0xFF bytes)
     const size_t nn = (size_t)ctx->set_base[ctx->n_sets];
     e = ctx->d_D16.p ? cudaMemsetAsync(ctx->d_D16.p, 0xFF, nn * sizeof(uint16_t), st)
                      : cudaMemsetAsync(ctx->d_D32.p, 0xFF, nn * sizeof(uint32_t), st);

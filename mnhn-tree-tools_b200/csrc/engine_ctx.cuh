@@ -80,6 +80,7 @@ struct swe_ctx {
   int layout_pb = 32;           // the value the current layout was built with
   int threads = 256;
   int inject_timeout = 0;
+  int part = 0, nparts = 1;     // this context scores tile group `part` of `nparts` (swe_set_partition)
   int threshold_path = 0;
   size_t kmer_batch_bytes = 0;  // k-mer calls' device batch (0 = their defaults)
   int graph_kernels = 0;

@@ -130,6 +130,11 @@ int engine_batch_size(const swe_ctx* ctx, int set);
 long long engine_fixed_point(const swe_ctx* ctx);
 long long engine_sweep_key(const swe_ctx* ctx, float eps);
 
+// Tile groups of nearly equal cost for a multi-process score pass: tiles in
+// the given order (descending cost) go one by one to the least loaded group
+// (the lowest index on ties), so every process derives the same groups.
+void lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
+
 // Deep copy of a split set (malloc'd like the original).
 split_set copy_split_set(const split_set& s);
 

@@ -128,6 +128,7 @@ EXPORTS = [
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
+    "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -241,6 +242,14 @@ def lib():
         L.read_split_set.restype = SplitSet
         L.read_split_set.argtypes = [C.c_char_p]
         L.swgpu_last_dropin_status.restype = C.c_int
+        L.swe_set_partition.restype = C.c_int
+        L.swe_set_partition.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.swe_distance_bytes.restype = C.c_int64
+        L.swe_distance_bytes.argtypes = [C.c_void_p]
+        L.swe_distance_copy.restype = C.c_int
+        L.swe_distance_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.swe_lpt_partition.restype = None
+        L.swe_lpt_partition.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         L.swe_adaptive_matrix.restype = C.c_int
         L.swe_adaptive_matrix.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_void_p,
                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p]
@@ -316,6 +325,17 @@ class Engine:
         _check(lib().swe_upload(self.ctx, self._buf.ptrs, self._buf.lens, self._buf.n), self.ctx)
         self.n = self._buf.n
         self.set_first = [0, self.n]
+
+    def set_partition(self, part: int, nparts: int):
+        """Score only tile group `part` of `nparts` (see swgpu.split_pass)."""
+        _check(lib().swe_set_partition(self.ctx, part, nparts), self.ctx)
+
+    def distance_bytes(self) -> int:
+        return int(lib().swe_distance_bytes(self.ctx))
+
+    def distance_copy(self, dev_ptr: int, to_engine: bool):
+        """Device-to-device copy of the distance storage to / from dev_ptr."""
+        _check(lib().swe_distance_copy(self.ctx, C.c_void_p(dev_ptr), int(bool(to_engine))), self.ctx)
 
     def upload_points(self, values: np.ndarray, metric: int):
         """Points values[dim][point] (float32) with the L1 (metric 1) or L2
@@ -627,6 +647,14 @@ def adaptive_from_matrix(D: np.ndarray, eps_start: float, eps_inc: float, minpts
         lib().free_split_set_and_associated_clusters(sets[k])
     lib().swe_free(sets)
     return text, kept
+
+
+def lpt_partition(cost, nparts: int) -> np.ndarray:
+    """Group of each tile (costs in descending order) as swe_set_partition assigns them."""
+    c = np.ascontiguousarray(cost, dtype=np.float64)
+    owner = np.zeros(max(1, len(c)), dtype=np.int32)
+    lib().swe_lpt_partition(c.ctypes.data, len(c), nparts, owner.ctypes.data)
+    return owner[:len(c)]
 
 
 def measure_mix_peak(device: int = 0):

@@ -522,3 +522,38 @@ def test_config2_full_properties_and_sampled_rows(eng):
     rows = list(range(0, 20000, 1999))
     R = O.score_rows(seqs, rows)
     assert np.array_equal(D[rows], R)
+
+
+@pytest.mark.gpu
+def test_partitioned_score_passes_combine_to_the_full_matrix():
+    """Three tile groups scored one after the other on one GPU (as three ranks
+    would), each leaving 0xFF bytes outside its tiles; their bytewise minimum,
+    copied back into the engine, is the whole pass's matrix, and DBSCAN on it
+    matches."""
+    import torch
+    import swgpu
+    seqs, _ = W.config2(n=1500)
+    seqs = list(seqs) + [b"ACGTRYNNNNACGT" * 3, b"", b"A" * 900]  # 32-bit path rows too
+    eng = swgpu.Engine()
+    eng.upload(seqs)
+    eng.score_all_pairs()
+    full = eng.distances()
+    cells_full = eng.stats()["tile_cells"]
+    nbytes = eng.distance_bytes()
+    parts, cells = [], 0.0
+    for p in range(3):
+        eng.set_partition(p, 3)
+        eng.score_all_pairs()
+        cells += eng.stats()["tile_cells"]
+        buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda:0")
+        eng.distance_copy(buf.data_ptr(), to_engine=False)
+        parts.append(buf)
+    assert cells == pytest.approx(cells_full)
+    combined = torch.minimum(torch.minimum(parts[0], parts[1]), parts[2])
+    eng.distance_copy(combined.data_ptr(), to_engine=True)
+    assert np.array_equal(eng.distances(), full)
+    assert eng.dbscan(300.0, 5) == O.dbscan(full, 300.0, 5)
+    eng.set_partition(0, 1)
+    eng.score_all_pairs()
+    assert np.array_equal(eng.distances(), full)
+    eng.close()

@@ -1092,7 +1092,6 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
   const int batch = max_steps > 0 ? std::min(8, max_steps) : 8;
   std::vector<std::unique_ptr<SweepMachine>> m(S);
   std::vector<std::string> logs(S);
-  for (int k = 0; k < S; ++k)
   for (int k = 0; k < S; ++k) {
     m[k].reset(new SweepMachine(ctx->set_first[k + 1] - ctx->set_first[k], eps_start, eps_inc, minpts, max_steps,
                                 batch, true, fixed));

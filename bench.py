@@ -623,7 +623,9 @@ def run_gpu_multi(args):
         torch.cuda.synchronize(dev)
 
     def sweeps():
-        return eng.adaptive_sets(wl["eps_start"], wl["eps_inc"], wl["minpts"], max_steps=wl["max_steps"])
+        # layer counts only: the split sets stay in the library (freed there)
+        return eng.adaptive_sets(wl["eps_start"], wl["eps_inc"], wl["minpts"], max_steps=wl["max_steps"],
+                                 layers=False)
 
     def step():
         eng.timer_start()
@@ -684,7 +686,8 @@ def run_gpu_multi(args):
             t1 = time.perf_counter()
             solo.upload_sets([st])
             solo.score_all_pairs()
-            solo.adaptive_sets(wl["eps_start"], wl["eps_inc"], wl["minpts"], max_steps=wl["max_steps"])
+            solo.adaptive_sets(wl["eps_start"], wl["eps_inc"], wl["minpts"], max_steps=wl["max_steps"],
+                               layers=False)
             per.append(1e3 * (time.perf_counter() - t1))
         total = time.perf_counter() - t0
         solo.close()

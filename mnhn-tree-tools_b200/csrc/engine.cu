@@ -1131,6 +1131,10 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
   double kernel_ms = 0;
   int launches = 0;
   while (!active.empty()) {
+    // largest sets first: their replays start first and their bitmaps are copied first
+    std::stable_sort(active.begin(), active.end(), [&](int x, int y) {
+      return ctx->set_first[x + 1] - ctx->set_first[x] > ctx->set_first[y + 1] - ctx->set_first[y];
+    });
     size_t a = 0;
     while (a < active.size()) {
       // sets [a, b) of the active list share one launch
@@ -1168,20 +1172,41 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
         add_set_groups(ctx, k, launchT.data(), (int)launchT.size(), &groups, &thr, &bw, &ci);
       }
       job_first.push_back(jobs.size());
+      // the bitmaps come back in chunks (in the sets' memory order, largest
+      // first); a replay waits for the chunk that completes its bitmap
+      constexpr int NCH = 16;
+      std::vector<cudaEvent_t> chunk_ev(NCH, nullptr);
+      struct EventGuard {
+        std::vector<cudaEvent_t>& ev;
+        ~EventGuard() {
+          for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+        }
+      } guard{chunk_ev};
+      // the chunk whose range [total*c/NCH, total*(c+1)/NCH) holds pos
+      auto chunk_of = [&](long long pos, long long total) -> int {
+        int c = 0;
+        while (c + 1 < NCH && total * (c + 1) / NCH <= pos) ++c;
+        return c;
+      };
       if (bw > 0) {
         CK(ctx->d_bbits.alloc((size_t)bw));
         CK(ctx->d_bcounts.alloc((size_t)ci));
         CK(ctx->h_bbits.alloc((size_t)bw));
         CK(ctx->h_bcounts.alloc((size_t)ci));
         if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bbits.p, ctx->d_bcounts.p)) return st;
-        CK(cpy(ctx, ctx->h_bbits.p, ctx->d_bbits.p, sizeof(uint64_t) * bw, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cpy(ctx, ctx->h_bcounts.p, ctx->d_bcounts.p, sizeof(int) * ci, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
-        if (swe_status st = thr_status(ctx)) return st;
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
-        kernel_ms += ms;
-        ++launches;
+        for (int c = 0; c < NCH; ++c) {
+          const long long w0 = bw * c / NCH, w1 = bw * (c + 1) / NCH;
+          const long long c0 = ci * c / NCH, c1 = ci * (c + 1) / NCH;
+          if (w1 > w0)
+            CK(cpy(ctx, ctx->h_bbits.p + w0, ctx->d_bbits.p + w0, sizeof(uint64_t) * (w1 - w0),
+                   cudaMemcpyDeviceToHost, ctx->st));
+          if (c1 > c0)
+            CK(cpy(ctx, ctx->h_bcounts.p + c0, ctx->d_bcounts.p + c0, sizeof(int) * (c1 - c0),
+                   cudaMemcpyDeviceToHost, ctx->st));
+          CK(cudaEventCreateWithFlags(&chunk_ev[c], cudaEventDisableTiming));
+          CK(cudaEventRecord(chunk_ev[c], ctx->st));
+        }
       }
       // order-faithful replays, one per (set, distinct threshold), largest sets first
       std::vector<int> order(jobs.size());
@@ -1194,6 +1219,11 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
         SweepJob& j = jobs[order[q]];
         const int ns = ctx->set_first[j.set + 1] - ctx->set_first[j.set], wpr = (ns + 63) / 64;
         if (j.bits_off >= 0) {
+          const int c = std::max(chunk_of(j.bits_off + (long long)ns * wpr - 1, bw), chunk_of(j.count_off + ns - 1, ci));
+          if (cudaEventSynchronize(chunk_ev[c]) != cudaSuccess) {
+            j.rc = SWE_ERR_CUDA;
+            return;
+          }
           j.rc = dbscan_replay_bitmap(ns, ctx->h_bbits.p + j.bits_off, wpr, ctx->h_bcounts.p + j.count_off, mp,
                                       &j.res);
         } else {  // no neighbour at all, not even the point itself
@@ -1202,6 +1232,18 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
           j.rc = dbscan_replay_bitmap(ns, zb.data(), wpr, zc.data(), mp, &j.res);
         }
       });
+      if (bw > 0) {
+        CK(cudaStreamSynchronize(ctx->st));
+        swe_status st = thr_status(ctx);
+        if (st) {
+          for (auto& j : jobs) free_split_set_and_associated_clusters(j.res);
+          return st;
+        }
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        kernel_ms += ms;
+        ++launches;
+      }
       // advance every set of the launch
       parallel_for((int)(b - a), [&](int x) {
         const int k = active[a + x];

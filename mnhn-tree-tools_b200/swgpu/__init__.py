@@ -450,9 +450,10 @@ class Engine:
         return text, kept
 
     def adaptive_sets(self, eps_start: float, eps_inc: float, minpts: int, max_steps: int = 0,
-                      prefix: str | None = None):
+                      prefix: str | None = None, layers: bool = True):
         """Sweeps of every uploaded set at once; one dict per set with its
-        status, truncated flag, steps, log text, kept layers and done_ms."""
+        status, truncated flag, steps, log text, kept layers (their number
+        with layers=False) and done_ms."""
         S = self.set_count()
         res = (SweepResult * max(S, 1))()
         _check(lib().swe_adaptive_sets(self.ctx, C.c_float(eps_start), C.c_float(eps_inc), minpts, max_steps,
@@ -462,7 +463,8 @@ class Engine:
             r = res[k]
             out.append({"status": r.status, "truncated": bool(r.truncated), "steps": r.steps,
                         "log": C.string_at(r.log).decode("latin-1") if r.log else "",
-                        "layers": [split_set_to_lists(r.layers[i]) for i in range(r.n_layers)],
+                        "layers": ([split_set_to_lists(r.layers[i]) for i in range(r.n_layers)] if layers
+                                   else r.n_layers),
                         "done_ms": r.done_ms})
         lib().swe_free_sweep_results(res, S)
         return out

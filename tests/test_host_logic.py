@@ -292,3 +292,59 @@ def test_sweep_speculation_through_halving():
         for batch in (1, 5):
             got = swgpu.adaptive_from_matrix(D, start, 7.0, 4, speculate=True, batch=batch)
             assert got[0] == want[0] and got[1] == want[1], (start, batch)
+
+
+def _load_kmer_file_with_lib(path):
+    import os as _os
+    L = swgpu.lib()
+
+    class Shape(C.Structure):
+        _fields_ = [("n_features", C.c_size_t), ("n_samples", C.c_size_t)]
+
+    L.shape_from_kmer_file.restype = Shape
+    L.shape_from_kmer_file.argtypes = [C.c_int]
+    L.load_kmer_from_file_into_dataset.restype = swgpu.Dataset
+    L.load_kmer_from_file_into_dataset.argtypes = [C.c_void_p, Shape]
+    L.free_values_from_dataset.argtypes = [swgpu.Dataset]
+    libc = C.CDLL(None)
+    libc.fdopen.restype = C.c_void_p
+    libc.fdopen.argtypes = [C.c_int, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    fd = _os.open(str(path), _os.O_RDONLY)
+    shape = L.shape_from_kmer_file(fd)
+    f = libc.fdopen(fd, b"r")
+    ds = L.load_kmer_from_file_into_dataset(f, shape)
+    libc.fclose(f)
+    vals = C.cast(ds.values, C.POINTER(C.POINTER(C.c_float)))
+    V = np.array([[vals[d][i] for i in range(ds.n_values)] for d in range(ds.n_dimensions)], dtype=np.float32)
+    L.free_values_from_dataset(ds)
+    return (shape.n_features, shape.n_samples), V
+
+
+def test_kmer_file_loader_matches_reference_semantics(tmp_path):
+    """shape_from_kmer_file + load_kmer_from_file_into_dataset (dataset.c:
+    346-425) on the reference fasta2kmer's own tables, and on a 3 MB table
+    with scattered whitespace and numbers in several notations (the threaded
+    tokenizer's pieces): the same floats as the reference's fscanf stream."""
+    doc = load_golden("points.json")
+    for k, text in doc["kmer"].items():
+        p = tmp_path / f"k{k}.tsv"
+        p.write_text(text)
+        shape, V = _load_kmer_file_with_lib(p)
+        want = O.load_kmer_text(text)
+        assert shape == (want.shape[0], want.shape[1]) and np.array_equal(V, want), k
+    rng = np.random.default_rng(3)
+    rows = []
+    for i in range(3000):
+        vals = rng.normal(0, 50, size=64)
+        toks = [("%d" % int(v)) if j % 3 == 0 else ("%.6f" % v) if j % 3 == 1 else ("%.3e" % v)
+                for j, v in enumerate(vals)]
+        sep = ["\t" if rng.random() < 0.9 else " \t " for _ in toks]
+        rows.append("sequence_%d\t" % i + "".join(t + s for t, s in zip(toks[:-1], sep)) + toks[-1] + "\n")
+    text = "".join(rows)
+    p = tmp_path / "big.tsv"
+    p.write_text(text)
+    shape, V = _load_kmer_file_with_lib(p)
+    want = O.load_kmer_text(text)
+    assert shape == (want.shape[0], want.shape[1])
+    assert np.array_equal(V, want)

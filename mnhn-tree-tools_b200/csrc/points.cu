@@ -28,26 +28,56 @@ constexpr int PT_TILE = 128;   // points per tile side
 constexpr int PT_KC = 16;      // dimensions per shared-memory stage
 constexpr int PT_THREADS = 256;
 
+// Two float32 values in one 64-bit register (x in the low half) and back.
+__device__ __forceinline__ uint64_t pack2(float x, float y) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void unpack2(uint64_t v, float& x, float& y) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v));
+}
+// Element-wise float32 pairs, each element rounded as its scalar operation.
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // One CTA per upper-triangle tile (bi <= bj) of 128 x 128 pairs; each thread
 // holds 8 x 8 pairs: rows i0 + {ty*4 .. ty*4+3, 64+ty*4 .. 64+ty*4+3}, the
 // same pattern of columns from tx.  Operands stream through shared memory in
 // stages of 16 dimensions, the next stage loaded into registers while the
-// current one is used.
+// current one is used.  L2 works on float32 pairs (sub.f32x2 / fma.f32x2:
+// two columns per instruction, each element rounded exactly as the scalar
+// operation), with the A operand stored twice in shared memory so that a pair
+// (a, a) is one 8-byte load; L1 stays scalar (its |a-b| has no pair form).
 template <int METRIC, bool VEC>
 __global__ void __launch_bounds__(PT_THREADS, 2)
     point_dist_kernel(const float* __restrict__ V, int64_t n_pad, int n, int dims, const int2* __restrict__ tiles,
                       int ntiles, uint32_t* __restrict__ D, unsigned* __restrict__ max_bits) {
-  __shared__ __align__(16) float sA[2][PT_KC][PT_TILE];
+  constexpr bool PAIRS = METRIC == SWE_METRIC_L2;
+  constexpr int AW = PAIRS ? 2 * PT_TILE : PT_TILE;  // floats per A row of a stage
+  __shared__ __align__(16) float sA[2][PT_KC][AW];
   __shared__ __align__(16) float sB[2][PT_KC][PT_TILE];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   unsigned local_max = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int i0 = tiles[t].x * PT_TILE, j0 = tiles[t].y * PT_TILE;
     float acc[8][8];
+    uint64_t acc2[8][4];  // the L2 accumulators as pairs of columns (2cp, 2cp+1)
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
+    for (int r = 0; r < 8; ++r) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
+#pragma unroll
+      for (int cp = 0; cp < 4; ++cp) acc2[r][cp] = 0ull;  // +0.0f in both halves
+    }
     // stage loads: 2 x 512 float4 per stage, 2 + 2 per thread
     float4 ra[2], rb[2];
     auto fetch = [&](int k0) {
@@ -69,7 +99,12 @@ __global__ void __launch_bounds__(PT_THREADS, 2)
       for (int h = 0; h < 2; ++h) {
         const int q = threadIdx.x + h * PT_THREADS;
         const int kk = q >> 5, c4 = (q & 31) * 4;
-        *reinterpret_cast<float4*>(&sA[buf][kk][c4]) = ra[h];
+        if (PAIRS) {  // each A value twice: (a0, a0, a1, a1), (a2, a2, a3, a3)
+          *reinterpret_cast<float4*>(&sA[buf][kk][2 * c4]) = make_float4(ra[h].x, ra[h].x, ra[h].y, ra[h].y);
+          *reinterpret_cast<float4*>(&sA[buf][kk][2 * c4 + 4]) = make_float4(ra[h].z, ra[h].z, ra[h].w, ra[h].w);
+        } else {
+          *reinterpret_cast<float4*>(&sA[buf][kk][c4]) = ra[h];
+        }
         *reinterpret_cast<float4*>(&sB[buf][kk][c4]) = rb[h];
       }
     };
@@ -82,6 +117,26 @@ __global__ void __launch_bounds__(PT_THREADS, 2)
       const bool more = k0 + PT_KC < dims;
       if (more) fetch(k0 + PT_KC);
       const int kc = min(PT_KC, dims - k0);
+      if (PAIRS) {
+        for (int kk = 0; kk < kc; ++kk) {
+          const float4 p0 = *reinterpret_cast<const float4*>(&sA[buf][kk][2 * (ty * 4)]);
+          const float4 p1 = *reinterpret_cast<const float4*>(&sA[buf][kk][2 * (ty * 4) + 4]);
+          const float4 p2 = *reinterpret_cast<const float4*>(&sA[buf][kk][2 * (64 + ty * 4)]);
+          const float4 p3 = *reinterpret_cast<const float4*>(&sA[buf][kk][2 * (64 + ty * 4) + 4]);
+          const float4 b0 = *reinterpret_cast<const float4*>(&sB[buf][kk][tx * 4]);
+          const float4 b1 = *reinterpret_cast<const float4*>(&sB[buf][kk][64 + tx * 4]);
+          const uint64_t ap[8] = {pack2(p0.x, p0.y), pack2(p0.z, p0.w), pack2(p1.x, p1.y), pack2(p1.z, p1.w),
+                                  pack2(p2.x, p2.y), pack2(p2.z, p2.w), pack2(p3.x, p3.y), pack2(p3.z, p3.w)};
+          const uint64_t bp[4] = {pack2(b0.x, b0.y), pack2(b0.z, b0.w), pack2(b1.x, b1.y), pack2(b1.z, b1.w)};
+#pragma unroll
+          for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int cp = 0; cp < 4; ++cp) {
+              const uint64_t d = sub2(ap[r], bp[cp]);
+              acc2[r][cp] = fma2(d, d, acc2[r][cp]);
+            }
+        }
+      } else
       for (int kk = 0; kk < kc; ++kk) {
         const float4 a0 = *reinterpret_cast<const float4*>(&sA[buf][kk][ty * 4]);
         const float4 a1 = *reinterpret_cast<const float4*>(&sA[buf][kk][64 + ty * 4]);
@@ -102,6 +157,12 @@ __global__ void __launch_bounds__(PT_THREADS, 2)
         __syncthreads();
         buf ^= 1;
       }
+    }
+    if (PAIRS) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int cp = 0; cp < 4; ++cp) unpack2(acc2[r][cp], acc[r][2 * cp], acc[r][2 * cp + 1]);
     }
     // both halves of the matrix
 #pragma unroll

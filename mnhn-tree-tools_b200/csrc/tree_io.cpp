@@ -132,6 +132,10 @@ double* densities_from_epsilons(int type, int dimensions, double* epsilons, int 
 }
 
 tree_node* generate_tree(int n_layers, cluster_connections** c, split_set* sets, double* tree_lengths) {
+  if (n_layers < 1 || !sets || sets[n_layers - 1].n_clusters < 1) {  // no root (the reference reads past its arrays)
+    fail_status(SWE_ERR_INVALID);
+    return nullptr;
+  }
   tree_node** nodes = (tree_node**)malloc(sizeof(tree_node*) * (size_t)n_layers);
   for (int i = 0; i < n_layers; i++) {
     nodes[i] = (tree_node*)malloc(sizeof(tree_node) * (size_t)(sets[i].n_clusters > 0 ? sets[i].n_clusters : 1));
@@ -185,12 +189,14 @@ split_set filtered_split_set_by_min_size(split_set s_in, int min_size) {
 }
 
 void print_tree(FILE* f, tree_node* root) {
+  if (!root) return;
   print_tree_worker(f, root);
   fprintf(f, ";");
 }
 
 int pureness_from_tree(int n_layers, tree_node* root, split_set* s, split_set target, double** pureness_values,
                        int** inpure_clusters) {
+  if (!root) return 1;
   double* pureness = (double*)calloc((size_t)(n_layers > 0 ? n_layers : 1), sizeof(double));
   int* inpures = (int*)calloc((size_t)(n_layers > 0 ? n_layers : 1), sizeof(int));
   if (!pureness || !inpures) {

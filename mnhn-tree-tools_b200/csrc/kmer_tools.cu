@@ -339,6 +339,17 @@ swe_status staging_ready(swe_ctx* ctx, size_t chunk, Staging** out) {
 
 namespace {
 
+// Device buffers above 1 GB (very long k-mers, very many rows) are given back
+// after a call instead of being kept for the next one.
+void trim_kmer_state(KmerState* km) {
+  constexpr size_t KEEP = size_t(1) << 30;
+  if (km->d_out.n * sizeof(int16_t) > KEEP) km->d_out.release();
+  if (km->d_cnt.n * sizeof(int16_t) > KEEP) km->d_cnt.release();
+  if (km->d_text.n > KEEP) km->d_text.release();
+  if (km->d_wide.n * sizeof(uint32_t) > KEEP) km->d_wide.release();
+  if (km->d_seq.n > KEEP) km->d_seq.release();
+}
+
 // The context's k-mer buffers and its staging chunks.
 swe_status kmer_state(swe_ctx* ctx, size_t chunk, KmerState** out, Staging** sg) {
   if (!ctx->km) {
@@ -487,6 +498,7 @@ swe_status swe_kmer_counts(swe_ctx* ctx, const char* const* seqs, const int64_t*
     if (st) return st;
   }
   CK(cudaStreamSynchronize(ctx->st));
+  trim_kmer_state(km);
   return SWE_OK;
 }
 
@@ -554,6 +566,7 @@ swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int
     if (st) return st;
   }
   CK(cudaStreamSynchronize(ctx->st));
+  trim_kmer_state(km);
   return SWE_OK;
 }
 

@@ -61,13 +61,21 @@ int dbscan_replay_bitmap(int n, const uint64_t* bits, int wpr, const int* counts
         visited[q] = 1;
         if (counts[q] >= minpts) {
           const uint64_t* rq = bits + (size_t)q * (size_t)wpr;
-          for (int w = 0; w < wpr; ++w) {
-            uint64_t fresh = rq[w] & ~queued[w];
-            if (!fresh) continue;
-            queued[w] |= fresh;
-            while (fresh) {
-              frontier.push_back(w * 64 + __builtin_ctzll(fresh));
-              fresh &= fresh - 1;
+          // blocks of 8 words: most rows add nothing new once the cluster's
+          // core is queued, so a branch-free test of the block comes first
+          for (int w0 = 0; w0 < wpr; w0 += 8) {
+            const int w1 = w0 + 8 < wpr ? w0 + 8 : wpr;
+            uint64_t any = 0;
+            for (int w = w0; w < w1; ++w) any |= rq[w] & ~queued[w];
+            if (!any) continue;
+            for (int w = w0; w < w1; ++w) {
+              uint64_t fresh = rq[w] & ~queued[w];
+              if (!fresh) continue;
+              queued[w] |= fresh;
+              while (fresh) {
+                frontier.push_back(w * 64 + __builtin_ctzll(fresh));
+                fresh &= fresh - 1;
+              }
             }
           }
         }

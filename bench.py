@@ -276,6 +276,105 @@ def kmer_dbscan_leg(eng, seqs, dev, k: int = 5, cpu: bool = True, reps: int = 3)
     return out
 
 
+def kmer2pca_leg(eng, seqs, dev, k: int = 5, dims: int = 7, cpu: bool = True, reps: int = 3):
+    """kmer2pca (kmer2pca.c) on the k-mer table of the same reads: through the
+    C ABI with host buffers (kmer2pca's float64 table in; every eigenvalue and
+    the projections onto the `dims` leading eigenvectors out), median of
+    `reps` after one warm-up, and the drop-in tool on the table's text file.
+    The Gram kernel's CUDA-event time gives its roofline: n4 nf (nf + 1) / 2
+    multiply-adds (the lower triangle of X4^T X4, n4 = n - n % 4 samples)
+    against 148 SMs x 64 FP64 FMA per clock x 2 at 1,965 MHz.  With cpu, the
+    reference's own kmer2pca (oracle/_ref, LAPACK from scipy's OpenBLAS) on
+    the same file with all host threads, on the first m rows when the whole
+    table would take more than about 20 s."""
+    import subprocess
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import swgpu
+    table = eng.kmer_counts(seqs, k)
+    X = table.astype(np.float64)
+    n, nf = X.shape
+    n4 = n - n % 4
+    e2e, gram, cov_ms, eig, proj, up = [], [], [], [], [], []
+    for r in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        w, P, info = eng.pca(X, dims)
+        t1 = time.perf_counter()
+        if r:
+            e2e.append(1e3 * (t1 - t0))
+            gram.append(info["ms_gram"])
+            cov_ms.append(info["ms_covariance"])
+            eig.append(info["ms_eigen"])
+            proj.append(info["ms_project"])
+            up.append(info["ms_upload"])
+    gms = statistics.median(gram)
+    fmas = n4 * nf * (nf + 1) / 2
+    props = torch.cuda.get_device_properties(dev)
+    peak = props.multi_processor_count * 64 * 2 * 1.965e9
+    achieved = 2 * fmas / (gms * 1e-3)
+    out = {"workload": f"kmer2pca ({dims} dimensions) of the {k}-mer table of the same {n} reads ({nf} features), "
+                       f"host float64 table in, eigenvalues and projections out",
+           "e2e_ms": round(statistics.median(e2e), 2), "upload_ms": round(statistics.median(up), 2),
+           "covariance_ms": round(statistics.median(cov_ms), 3), "eigen_ms": round(statistics.median(eig), 1),
+           "project_ms": round(statistics.median(proj), 3), "exact_route": bool(info["exact"]),
+           "top_eigenvalue": round(float(w[-1]), 6),
+           "kernel": {"name": "pca_gram_kernel", "ms": round(gms, 3), "bound": "fp64",
+                      "achieved": round(achieved / 1e12, 3), "peak": round(peak / 1e12, 2), "unit": "TFLOP/s",
+                      "frac": round(achieved / peak, 4),
+                      "peak_source": "SMs x 64 FP64 FMA/clock x 2 x 1,965 MHz (clocks.max.sm); nominal, not "
+                                     "measured"},
+           "tool_ms": None, "cpu_baseline": None}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "table.tsv")
+        with open(path, "wb") as f:
+            eng_text = eng.kmer_tsv(table)
+            f.write(eng_text)
+        t0 = time.perf_counter()
+        r = subprocess.run([str(swgpu.BIN_DIR / "kmer2pca"), path, os.path.join(td, "p"), os.path.join(td, "e"),
+                            str(dims), "1"], capture_output=True, timeout=600)
+        if r.returncode == 0:
+            out["tool_ms"] = round(1e3 * (time.perf_counter() - t0), 1)
+        if cpu:
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import oracle as O
+            ref = O.REF_DIR / "kmer2pca"
+            if ref.exists():
+                threads = os.cpu_count() or 1
+
+                def ref_run(rows):
+                    src = path
+                    if rows < n:
+                        src = os.path.join(td, f"head{rows}.tsv")
+                        with open(src, "wb") as f:
+                            f.write(b"".join(eng_text.splitlines(keepends=True)[:rows]))
+                    t0 = time.perf_counter()
+                    rr = subprocess.run([str(ref), src, os.path.join(td, "rp"), os.path.join(td, "re"), str(dims),
+                                         str(threads)], capture_output=True, timeout=900)
+                    return time.perf_counter() - t0, rr.returncode
+
+                m = min(n, 1000)
+                dt, rc = ref_run(m)
+                if rc == 0:
+                    if m < n and dt * n / m <= 20.0:
+                        m = n
+                    elif m < n:
+                        m = int(min(n, max(m, m * 20.0 / max(dt, 1e-3))))
+                    dt, rc = ref_run(m)
+                if rc == 0:
+                    out["cpu_baseline"] = {
+                        "kind": "reference", "cores": threads, "seconds": round(dt, 3),
+                        "rows_per_s": round(m / dt, 1),
+                        "sample": f"the reference's kmer2pca tool (file in, files out; LAPACK dsyev from scipy's "
+                                  f"OpenBLAS) on the first {m} of the {n} rows, {threads} threads"}
+                    if out["tool_ms"]:
+                        out["tool_vs_cpu"] = round((n * dt / m) / (out["tool_ms"] * 1e-3), 1)
+    return out
+
+
 def run_leg(args):
     """One side leg alone (profiling a small case of its kernels)."""
     import swgpu
@@ -287,7 +386,8 @@ def run_leg(args):
         out = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
     else:
         eng = swgpu.Engine(device=0)
-        out = kmer_dbscan_leg(eng, seqs, 0, cpu=not args.no_cpu_baseline)
+        leg = kmer2pca_leg if args.leg == "kmer2pca" else kmer_dbscan_leg
+        out = leg(eng, seqs, 0, cpu=not args.no_cpu_baseline)
         eng.close()
     print(json.dumps({"leg": args.leg, **out}), flush=True)
     return 0
@@ -571,6 +671,7 @@ def run_gpu(args):
         if world == 1 and wl["gen"] == "config2" and not args.no_kmer:
             line["fasta2kmer"] = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
             line["kmer_dbscan"] = kmer_dbscan_leg(eng, seqs, dev, cpu=not args.no_cpu_baseline)
+            line["kmer2pca"] = kmer2pca_leg(eng, seqs, dev, cpu=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     eng.close()
     del flush
@@ -936,8 +1037,8 @@ def main():
     ap.add_argument("--split", action="store_true",
                     help="config 2/3: one data set split over all ranks (strong scaling: tile groups and one "
                          "all-reduce of the matrix) instead of one data set per rank")
-    ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer and k-mer DBSCAN legs")
-    ap.add_argument("--leg", choices=["fasta2kmer", "kmer_dbscan"],
+    ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer, k-mer DBSCAN and kmer2pca legs")
+    ap.add_argument("--leg", choices=["fasta2kmer", "kmer_dbscan", "kmer2pca"],
                     help="run one side leg alone on the config-2 reads (the first --n) and print its object")
     ap.add_argument("--weight-decay", type=float, default=0.0, help="config 4: decoupled weight decay of Adam")
     args = ap.parse_args()

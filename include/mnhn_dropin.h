@@ -131,6 +131,11 @@ data_shape shape_from_kmer_file(int infile);
 /* dataset.c:384-425: a label then n_features numbers per sample into
    values[feature][sample] (32-byte aligned rows); other fields zeroed. */
 dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape);
+/* kmer2pca.c:255-268 (data_from_file): the same token stream read as doubles
+   ("%lf") into data[sample * n_features + feature], kmer2pca's row-major
+   in_data.  Returns 0, or an swe_status when a value is not a number or the
+   file ends early (where the reference leaves values unset). */
+int swe_read_feature_table(FILE* in_file, data_shape shape, double* data);
 /* dataset.c:629-635, 646-649. */
 void free_values_from_dataset(dataset ds);
 void free_dataset(dataset ds);

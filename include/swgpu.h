@@ -399,6 +399,56 @@ typedef int (*swe_text_sink)(const char* data, size_t size, void* user);
 swe_status swe_kmer_tsv(swe_ctx* ctx, const int16_t* const* rows, int64_t n, int64_t nk, swe_text_sink sink,
                         void* user);
 
+/* ---- kmer2pca: principal components of a sample x feature table ----------
+   `data` is n_samples rows of n_features doubles, row-major (kmer2pca.c's
+   in_data, filled by data_from_file, kmer2pca.c:255-268).  The covariance is
+   the reference's (kmer2pca.c:337-481): means over all samples, sums over the
+   first n_samples - n_samples % 4 samples (its AVX loop never adds the last
+   n_samples % 4), divided by n_samples.  Tables of integers in the int16
+   range (every fasta2kmer table) are kept as int16 on the GPU and their
+   covariance is the exact value rounded (see csrc/pca.cu); other tables are
+   centred and summed in float64. */
+typedef struct {
+  int exact;            /* 1: integer table, covariance from exact integer sums */
+  int64_t h2d_bytes;    /* table bytes copied to the GPU */
+  double ms_upload;     /* host time of the table check, conversion and copy */
+  double ms_covariance; /* device time of the covariance kernels */
+  double ms_gram;       /* device time of the Gram tile kernel inside it */
+  double ms_eigen;      /* host time of the eigen-decomposition (swe_pca) */
+  double ms_project;    /* device time of the projection kernel */
+} swe_pca_info;
+
+/* means_from_data + feature_covariance_matrix (kmer2pca.c:286-481): cov gets
+   the n_features x n_features covariance matrix (row-major, symmetric).  The
+   table stays on the GPU for a following swe_pca_project with data == NULL.
+   info may be NULL. */
+swe_status swe_pca_covariance(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, double* cov,
+                              swe_pca_info* info);
+
+/* eigen_from_corr (kmer2pca.c:107-138, LAPACK dsyev): every eigenvalue of the
+   symmetric cov in ascending order into eigenvalues[n_features], and the unit
+   eigenvectors of the n_vectors largest ones, largest first, into
+   vectors[n_vectors][n_features] (n_vectors may be 0, vectors then unused).
+   An eigenvector's sign is not defined by the problem; each is returned with
+   its largest-magnitude entry positive.  Host code, no context. */
+swe_status swe_pca_eigen(const double* cov, int64_t n_features, int64_t n_vectors, double* eigenvalues,
+                         double* vectors);
+
+/* obtain_projections (kmer2pca.c:141-211): projections[j][i] = sum over k of
+   data[j][k] * vectors[i][k] in the order of k (one fused multiply-add per
+   term) for the `dimensions` vectors given (1 <= dimensions <= n_features).
+   data == NULL projects the table left on the GPU by the previous
+   swe_pca_covariance / swe_pca call of this context (same shape). */
+swe_status swe_pca_project(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features,
+                           const double* vectors, int64_t dimensions, double* projections, swe_pca_info* info);
+
+/* The whole of kmer2pca after reading its file (kmer2pca.c:540-586): one
+   table upload, the covariance, the eigen-decomposition and the projections
+   onto the eigenvectors of the `dimensions` largest eigenvalues.
+   eigenvalues[n_features] ascending, projections[n_samples][dimensions]. */
+swe_status swe_pca(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, int64_t dimensions,
+                   double* eigenvalues, double* projections, swe_pca_info* info);
+
 void swe_free(void* p);
 
 #ifdef __cplusplus

@@ -65,6 +65,8 @@ struct PrefilterState;
 void prefilter_destroy(PrefilterState* pf);
 struct KmerState;
 void kmer_state_destroy(KmerState* km);
+struct PcaState;
+void pca_state_destroy(PcaState* ps);
 struct Staging;
 void staging_destroy(Staging* sg);
 
@@ -186,6 +188,8 @@ struct swe_ctx {
   swgpu::PrefilterState* pf = nullptr;
   // k-mer tables: device buffers and pinned staging (null until first used)
   swgpu::KmerState* km = nullptr;
+  // kmer2pca: the resident table and its buffers (null until first used)
+  swgpu::PcaState* pca = nullptr;
   // pinned staging chunks of the chunked transfers (null until first used)
   swgpu::Staging* stage = nullptr;
 
@@ -193,6 +197,7 @@ struct swe_ctx {
     cudaSetDevice(device);
     swgpu::prefilter_destroy(pf);
     swgpu::kmer_state_destroy(km);
+    swgpu::pca_state_destroy(pca);
     swgpu::staging_destroy(stage);
     if (graph) cudaGraphExecDestroy(graph);
     for (auto& e : ev)

@@ -1,7 +1,8 @@
 // Point-dataset files of the k-mer / PCA DBSCAN tools (cluster_dbscan_kmer.c,
 // cluster_dbscan_pca.c, adaptive_clustering.c): the k-mer table loader of
 // dataset.c:346-425, the value frees of dataset.c:629-649 and the cluster
-// files with values of cluster_io.c:343-379.
+// files with values of cluster_io.c:343-379, and kmer2pca's table reader
+// (kmer2pca.c:255-268).
 //
 // load_kmer_from_file_into_dataset reads the reference's token stream (a
 // label, then n_features numbers, per sample, whitespace anywhere) with strtof
@@ -10,11 +11,14 @@
 // t / (n_features + 1), which is what the reference's fscanf("%s") /
 // fscanf("%f") sequence assigns.  strtof gives the same float as fscanf("%f")
 // for every number; a token that is not a number reads as 0 (the reference
-// leaves the value unset and stops advancing).
+// leaves the value unset and stops advancing).  swe_read_feature_table reads
+// the same stream with strtod (fscanf("%lf")) into kmer2pca's row-major
+// doubles and reports such a token, or a short file, as an error.
 #include <fcntl.h>
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -33,6 +37,78 @@ float* alloc_values(size_t n) {
   if (posix_memalign(&p, 32, sizeof(float) * std::max<size_t>(padded, 8)) != 0) return nullptr;
   memset(p, 0, sizeof(float) * std::max<size_t>(padded, 8));
   return static_cast<float*>(p);
+}
+
+
+// Reads the token stream of a table file (a label, then n_features numbers,
+// per sample, whitespace anywhere) on host threads and hands each number token
+// to on_value(sample, feature, token) as a NUL-terminated string; returns the
+// number of tokens found (at most (n_features + 1) * n_samples are used).
+template <class F>
+uint64_t read_fields(FILE* in_file, data_shape shape, F&& on_value) {
+  rewind(in_file);
+  std::vector<char> text;
+  {
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = fread(chunk, 1, sizeof chunk, in_file)) > 0) text.insert(text.end(), chunk, chunk + got);
+  }
+  text.push_back('\0');
+  const size_t len = text.size() - 1;
+  const size_t fields = shape.n_features + 1;
+  const uint64_t want = (uint64_t)fields * shape.n_samples;
+  if (want == 0) return 0;
+  // pieces cut at whitespace
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int T = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(hw, 16), len >> 20));
+  std::vector<size_t> cut(T + 1, len);
+  cut[0] = 0;
+  for (int t = 1; t < T; ++t) {
+    size_t p = std::max(cut[t - 1], len * t / T);
+    while (p < len && !is_space(text[p])) ++p;
+    cut[t] = p;
+  }
+  auto tokens = [&](size_t a, size_t b, auto&& on_token) {
+    size_t p = a;
+    uint64_t k = 0;
+    while (p < b) {
+      while (p < b && is_space(text[p])) ++p;
+      if (p >= b) break;
+      const size_t q0 = p;
+      while (p < b && !is_space(text[p])) ++p;
+      if (!on_token(k++, q0, p)) break;
+    }
+    return k;
+  };
+  std::vector<uint64_t> count(T, 0), first(T + 1, 0);
+  {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t)
+      th.emplace_back([&, t]() { count[t] = tokens(cut[t], cut[t + 1], [](uint64_t, size_t, size_t) { return true; }); });
+    for (auto& x : th) x.join();
+  }
+  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; ++t)
+    th.emplace_back([&, t]() {
+      char tmp[128];
+      tokens(cut[t], cut[t + 1], [&](uint64_t k, size_t q0, size_t q1) {
+        const uint64_t g = first[t] + k;
+        if (g >= want) return false;
+        const uint64_t sample = g / fields, field = g % fields;
+        if (field == 0) return true;  // the label, read with "%s"
+        const size_t L = q1 - q0;
+        if (L < sizeof tmp) {
+          memcpy(tmp, text.data() + q0, L);
+          tmp[L] = '\0';
+          return on_value(sample, field - 1, (const char*)tmp);
+        }
+        std::string s(text.data() + q0, L);
+        return on_value(sample, field - 1, s.c_str());
+      });
+    });
+  for (auto& x : th) x.join();
+  return first[T];
 }
 
 }  // namespace
@@ -74,72 +150,28 @@ dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape) {
       return ds;
     }
   }
-  rewind(in_file);
-  std::vector<char> text;
-  {
-    char chunk[1 << 16];
-    size_t got;
-    while ((got = fread(chunk, 1, sizeof chunk, in_file)) > 0) text.insert(text.end(), chunk, chunk + got);
-  }
-  text.push_back('\0');
-  const size_t len = text.size() - 1;
-  const size_t fields = shape.n_features + 1;
-  const uint64_t want = (uint64_t)fields * shape.n_samples;
-  if (want == 0) return ds;
-  // pieces cut at whitespace
-  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-  const int T = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(hw, 16), len >> 20));
-  std::vector<size_t> cut(T + 1, len);
-  cut[0] = 0;
-  for (int t = 1; t < T; ++t) {
-    size_t p = std::max(cut[t - 1], len * t / T);
-    while (p < len && !is_space(text[p])) ++p;
-    cut[t] = p;
-  }
-  auto tokens = [&](size_t a, size_t b, auto&& on_token) {
-    size_t p = a;
-    uint64_t k = 0;
-    while (p < b) {
-      while (p < b && is_space(text[p])) ++p;
-      if (p >= b) break;
-      const size_t q0 = p;
-      while (p < b && !is_space(text[p])) ++p;
-      on_token(k++, q0, p);
-    }
-    return k;
-  };
-  std::vector<uint64_t> count(T, 0), first(T + 1, 0);
-  {
-    std::vector<std::thread> th;
-    for (int t = 0; t < T; ++t)
-      th.emplace_back([&, t]() { count[t] = tokens(cut[t], cut[t + 1], [](uint64_t, size_t, size_t) {}); });
-    for (auto& x : th) x.join();
-  }
-  for (int t = 0; t < T; ++t) first[t + 1] = first[t] + count[t];
-  std::vector<std::thread> th;
-  for (int t = 0; t < T; ++t)
-    th.emplace_back([&, t]() {
-      char tmp[128];
-      tokens(cut[t], cut[t + 1], [&](uint64_t k, size_t q0, size_t q1) {
-        const uint64_t g = first[t] + k;
-        if (g >= want) return;
-        const uint64_t sample = g / fields, field = g % fields;
-        if (field == 0) return;  // the label, read with "%s"
-        const size_t L = q1 - q0;
-        float v = 0.0f;
-        if (L < sizeof tmp) {
-          memcpy(tmp, text.data() + q0, L);
-          tmp[L] = '\0';
-          v = strtof(tmp, nullptr);
-        } else {
-          std::string s(text.data() + q0, L);
-          v = strtof(s.c_str(), nullptr);
-        }
-        ds.values[field - 1][sample] = v;
-      });
-    });
-  for (auto& x : th) x.join();
+  read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
+    ds.values[field][sample] = strtof(tok, nullptr);
+    return true;
+  });
   return ds;
+}
+
+int swe_read_feature_table(FILE* in_file, data_shape shape, double* data) {
+  if (!in_file || (!data && shape.n_features * shape.n_samples > 0)) return SWE_ERR_INVALID;
+  std::atomic<int> bad{0};
+  const uint64_t got = read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
+    char* end = nullptr;
+    const double v = strtod(tok, &end);
+    if (end == tok) {
+      bad.store(1, std::memory_order_relaxed);
+      return false;
+    }
+    data[sample * shape.n_features + field] = v;
+    return true;
+  });
+  if (bad.load() || got < (uint64_t)(shape.n_features + 1) * shape.n_samples) return SWE_ERR_IO;
+  return SWE_OK;
 }
 
 void free_values_from_dataset(dataset ds) {

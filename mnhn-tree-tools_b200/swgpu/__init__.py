@@ -115,6 +115,21 @@ class KmerFrequencies(C.Structure):
     _fields_ = [("frequencies", C.POINTER(C.POINTER(C.c_short))), ("n_kmers", C.c_size_t),
                 ("n_seq", C.c_size_t)]
 
+class DataShape(C.Structure):
+    # dataset.h:37-40 (kmer2pca.c:20-23 declares the same struct)
+    _fields_ = [("n_features", C.c_size_t), ("n_samples", C.c_size_t)]
+
+
+class PcaInfo(C.Structure):
+    # swgpu.h: swe_pca_info
+    _fields_ = [("exact", C.c_int), ("h2d_bytes", C.c_int64), ("ms_upload", C.c_double),
+                ("ms_covariance", C.c_double), ("ms_gram", C.c_double), ("ms_eigen", C.c_double),
+                ("ms_project", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # Every symbol the public headers declare (checked by the CPU test suite).
 EXPORTS = [
     # include/swgpu.h
@@ -129,6 +144,7 @@ EXPORTS = [
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
     "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition",
+    "swe_pca_covariance", "swe_pca_eigen", "swe_pca_project", "swe_pca",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -136,7 +152,7 @@ EXPORTS = [
     "free_split_set_and_associated_clusters", "swgpu_last_dropin_status",
     "frequencies_from_dataset", "write_kmer_base", "free_kmer_frequencies", "dbscan_L1", "dbscan_L2",
     "shape_from_kmer_file", "load_kmer_from_file_into_dataset", "free_values_from_dataset", "free_dataset",
-    "create_single_cluster_file_with_values", "create_cluster_files_with_values",
+    "create_single_cluster_file_with_values", "create_cluster_files_with_values", "swe_read_feature_table",
 ]
 
 _lib = None
@@ -268,6 +284,17 @@ def lib():
         L.write_kmer_base.argtypes = [C.c_void_p, KmerFrequencies]
         L.free_kmer_frequencies.restype = None
         L.free_kmer_frequencies.argtypes = [KmerFrequencies]
+        L.swe_pca_covariance.restype = C.c_int
+        L.swe_pca_covariance.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                                         C.POINTER(PcaInfo)]
+        L.swe_pca_eigen.restype = C.c_int
+        L.swe_pca_eigen.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
+        L.swe_pca_project.restype = C.c_int
+        L.swe_pca_project.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
+                                      C.c_void_p, C.POINTER(PcaInfo)]
+        L.swe_pca.restype = C.c_int
+        L.swe_pca.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                              C.POINTER(PcaInfo)]
         _lib = L
     return _lib
 
@@ -503,6 +530,48 @@ class Engine:
         _check(lib().swe_kmer_tsv(self.ctx, self._row_ptrs(t), t.shape[0], t.shape[1], sink, None), self.ctx)
         return b"".join(chunks)
 
+    # ---------------------------------------------------------------- kmer2pca
+    def pca_covariance(self, table) -> tuple[np.ndarray, dict]:
+        """means_from_data + feature_covariance_matrix (kmer2pca.c:286-481) of
+        a (samples, features) table on the GPU: the covariance matrix and the
+        call's swe_pca_info.  The table stays on the GPU for pca_project(None, ...)."""
+        X = np.ascontiguousarray(table, dtype=np.float64)
+        n, nf = X.shape
+        cov = np.zeros((nf, nf))
+        info = PcaInfo()
+        _check(lib().swe_pca_covariance(self.ctx, X.ctypes.data, n, nf, cov.ctypes.data, C.byref(info)), self.ctx)
+        self._pca_rows = n
+        return cov, info.as_dict()
+
+    def pca_project(self, table, vectors) -> np.ndarray:
+        """obtain_projections (kmer2pca.c:141-211): (samples, len(vectors)) sums
+        of table row x vector in the order of the features; table None projects
+        the table of the last pca_covariance / pca call."""
+        V = np.ascontiguousarray(vectors, dtype=np.float64)
+        d, nf = V.shape
+        if table is None:
+            ptr, n = None, getattr(self, "_pca_rows", 0)
+        else:
+            X = np.ascontiguousarray(table, dtype=np.float64)
+            ptr, n = X.ctypes.data, X.shape[0]
+        out = np.zeros((n, d))
+        _check(lib().swe_pca_project(self.ctx, ptr, n, nf, V.ctypes.data, d, out.ctypes.data, None), self.ctx)
+        return out
+
+    def pca(self, table, dimensions: int) -> tuple[np.ndarray, np.ndarray, dict]:
+        """kmer2pca after its file is read (kmer2pca.c:540-586): every
+        eigenvalue (ascending), the projections onto the `dimensions` leading
+        eigenvectors, and the call's swe_pca_info."""
+        X = np.ascontiguousarray(table, dtype=np.float64)
+        n, nf = X.shape
+        w = np.zeros(nf)
+        P = np.zeros((n, dimensions))
+        info = PcaInfo()
+        _check(lib().swe_pca(self.ctx, X.ctypes.data, n, nf, dimensions, w.ctypes.data, P.ctypes.data,
+                             C.byref(info)), self.ctx)
+        self._pca_rows = n
+        return w, P, info.as_dict()
+
     # ---------------------------------------------------------------- prefilter
     def kmer_features(self, k: int = 5) -> np.ndarray:
         out = np.zeros((self.n, 4 ** k), dtype=np.float32)
@@ -649,6 +718,19 @@ def adaptive_from_matrix(D: np.ndarray, eps_start: float, eps_inc: float, minpts
         lib().free_split_set_and_associated_clusters(sets[k])
     lib().swe_free(sets)
     return text, kept
+
+
+def pca_eigen(cov, n_vectors: int) -> tuple[np.ndarray, np.ndarray]:
+    """eigen_from_corr (kmer2pca.c:107-138) on the host: every eigenvalue of
+    the symmetric matrix, ascending, and the unit eigenvectors of the
+    n_vectors largest ones, largest first (rows; sign: largest-magnitude entry
+    positive)."""
+    A = np.ascontiguousarray(cov, dtype=np.float64)
+    n = A.shape[0]
+    w = np.zeros(n)
+    V = np.zeros((max(n_vectors, 1), n))
+    _check(lib().swe_pca_eigen(A.ctypes.data, n, n_vectors, w.ctypes.data, V.ctypes.data))
+    return w, V[:n_vectors]
 
 
 def lpt_partition(cost, nparts: int) -> np.ndarray:

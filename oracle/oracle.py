@@ -7,11 +7,13 @@ engine.  Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline leg of
 Two kinds of checker live here:
 
 * ``liboracle.so`` - the plain-C restatement in ``sw_oracle.c`` (score,
-  all-pairs, DBSCAN, FASTA loader, k-mer counts), wrapped with ctypes;
+  all-pairs, DBSCAN, FASTA loader, k-mer counts, point distances, kmer2pca's
+  projections), wrapped with ctypes;
 * the reference itself, compiled from its own sources into ``_ref/`` by
   ``make -C oracle ref`` (``libref.so`` and the reference command-line tools,
   plus ``*_subst`` builds whose score() reads a precomputed matrix, see
-  ``score_subst.c``).
+  ``score_subst.c``, and kmer2pca linked to scipy's OpenBLAS LAPACK through
+  ``lapack_shim.c``).
 
 The adaptive-eps driver and the split-set helpers are restated below in
 Python (small inputs only); each cites the reference lines it follows.
@@ -68,6 +70,7 @@ def lib():
         L.orc_dbscan_points.restype = C.c_int
         L.orc_dbscan_points.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_int, C.c_void_p,
                                         C.c_void_p]
+        L.orc_pca_project.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
         _lib = L
     return _lib
 
@@ -261,6 +264,100 @@ def kmer_tsv(table: np.ndarray) -> bytes:
     for i, row in enumerate(np.asarray(table, dtype=np.int16)):
         lines.append("sequence_%d\t" % i + "\t".join(str(int(v)) for v in row) + "\n")
     return "".join(lines).encode()
+
+
+# --------------------------------------------------------------------------
+# kmer2pca (kmer2pca.c)
+# --------------------------------------------------------------------------
+
+def read_feature_table(text: str) -> np.ndarray:
+    """shape_from_input_file + data_from_file (kmer2pca.c:43-89, 255-268):
+    n_features = tabs of the first line, n_samples = newlines from the end of
+    the first line on, then per sample a label and n_features numbers of the
+    whitespace token stream ("%lf").  Returns (samples, features) float64."""
+    first_nl = text.index("\n") if "\n" in text else len(text)
+    nf = text[:first_nl].count("\t")
+    ns = text[first_nl:].count("\n")
+    toks = text.split()
+    X = np.zeros((ns, nf))
+    for s in range(ns):
+        X[s] = [float(t) for t in toks[s * (nf + 1) + 1:(s + 1) * (nf + 1)]]
+    return X
+
+
+def pca_covariance(X: np.ndarray) -> np.ndarray:
+    """means_from_data + feature_covariance_matrix (kmer2pca.c:466-481,
+    337-463) in float64: means over all n samples; the centred products summed
+    over the first n - n % 4 samples only (the AVX loop's scalar tail is
+    guarded by `!n_samples%4`, which is 0 for n > 0); divided by n.  The sums
+    run in numpy's order, the reference's are 4-lane Kahan sums: equal up to
+    rounding."""
+    X = np.asarray(X, dtype=np.float64)
+    n = X.shape[0]
+    m = X.sum(0) / n
+    n4 = n - n % 4
+    Xc = X[:n4] - m
+    return Xc.T @ Xc / n
+
+
+def pca_covariance_exact(table: np.ndarray) -> np.ndarray:
+    """The quantity pca_covariance estimates, computed exactly for an integer
+    table and rounded as the GPU's integer route does: with P = X4^T X4, T the
+    column sums of X4 (X4 = the first n4 = n - n % 4 rows) and S those of X,
+    C = float(n^2 P - n (S T^T + T S^T) + n4 S S^T) / n / n / n, the numerator
+    an exact (Python) integer converted to the nearest double."""
+    X = np.asarray(table, dtype=np.int64)
+    n, nf = X.shape
+    n4 = n - n % 4
+    P = (X[:n4].T @ X[:n4]).astype(object)
+    T = X[:n4].sum(0).astype(object)
+    S = X.sum(0).astype(object)
+    Q = n * n * P - n * (np.outer(S, T) + np.outer(T, S)) + n4 * np.outer(S, S)
+    out = np.empty((nf, nf))
+    for i in range(nf):
+        for j in range(nf):
+            out[i, j] = float(Q[i, j]) / n / n / n
+    return out
+
+
+def pca_eigen(cov: np.ndarray, n_vectors: int):
+    """eigen_from_corr (kmer2pca.c:107-138): numpy's LAPACK symmetric solver
+    in place of the reference's dsyev: every eigenvalue ascending, and the
+    eigenvectors of the n_vectors largest as rows, largest first, each signed
+    so that its largest-magnitude entry is positive."""
+    w, V = np.linalg.eigh(np.asarray(cov, dtype=np.float64))
+    vec = V[:, ::-1][:, :n_vectors].T.copy()
+    for v in vec:
+        if v[np.argmax(np.abs(v))] < 0:
+            v *= -1
+    return w, vec
+
+
+def pca_project(X: np.ndarray, vectors: np.ndarray) -> np.ndarray:
+    """obtain_projections (kmer2pca.c:141-168) through orc_pca_project: one
+    fused multiply-add per feature, in order."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    V = np.ascontiguousarray(vectors, dtype=np.float64)
+    n, nf = X.shape
+    d = V.shape[0]
+    P = np.zeros((n, d))
+    lib().orc_pca_project(X.ctypes.data, n, nf, V.ctypes.data, d, P.ctypes.data)
+    return P
+
+
+def kmer2pca(X: np.ndarray, dimensions: int):
+    """kmer2pca's computation after reading its file (kmer2pca.c:540-586):
+    eigenvalues ascending and the (samples, dimensions) projections."""
+    w, V = pca_eigen(pca_covariance(X), dimensions)
+    return w, pca_project(X, V)
+
+
+def kmer2pca_texts(eigenvalues, projections) -> tuple[str, str]:
+    """print_eigenvalues / print_projections (kmer2pca.c:226-253): "%lf" per
+    line, and "%lf" tab separated per sample."""
+    ev = "".join("%f\n" % v for v in eigenvalues)
+    pr = "".join("\t".join("%f" % v for v in row) + "\n" for row in np.asarray(projections))
+    return ev, pr
 
 
 # --------------------------------------------------------------------------

@@ -432,3 +432,16 @@ void orc_kmer_frequencies(const char* s, int k, int protein, int16_t* out) {
     if (ok) out[idx] = (int16_t)(uint16_t)((uint16_t)out[idx] + 1u);
   }
 }
+
+/* obtain_projections (kmer2pca.c:141-168): p[j][i] = sum over k of
+   data[j][k] * v[i][k], accumulated in the order of k with one fused
+   multiply-add per term (the reference's loop as an FMA build compiles it).
+   v holds the wanted eigenvectors as rows, largest eigenvalue first. */
+void orc_pca_project(const double* data, int64_t n, int64_t nf, const double* v, int64_t dims, double* p) {
+  for (int64_t j = 0; j < n; j++)
+    for (int64_t i = 0; i < dims; i++) {
+      double acc = 0;
+      for (int64_t k = 0; k < nf; k++) acc = fma(data[j * nf + k], v[i * nf + k], acc);
+      p[j * dims + i] = acc;
+    }
+}

@@ -504,11 +504,54 @@ def score_callers_golden():
     (OUT / "score_callers.json").write_text(json.dumps(doc))
 
 
+def kmer2pca_tables():
+    """The seeded input tables of kmer2pca.json, as the text kmer2pca reads:
+    5-mer, 3-mer and 2-mer tables of random reads (fasta2kmer's format, made by
+    the oracle's frequencies_from_dataset restatement), a table of fractions
+    with spaces, tabs and exponents in its token stream, and tables of fewer
+    than four samples (no sample enters the reference's covariance sums)."""
+    rng = np.random.default_rng(2024)
+    out = []
+
+    def reads(n, lo, hi):
+        return [rand_seq(rng, int(rng.integers(lo, hi + 1))) for _ in range(n)]
+
+    out.append(("k3_n203", O.kmer_tsv(O.kmer_table(reads(203, 50, 400), 3)).decode(), 5))
+    out.append(("k2_n50", O.kmer_tsv(O.kmer_table(reads(50, 20, 120), 2)).decode(), 16))
+    out.append(("k4_n97", O.kmer_tsv(O.kmer_table(reads(97, 100, 300), 4)).decode(), 7))
+    lines = []
+    for i in range(41):
+        vals = rng.normal(size=6) * np.array([5.0, 3.0, 2.0, 1.0, 0.5, 0.25]) + 10.0
+        sep = "\t" if i == 0 else ("  " if i % 3 == 0 else "\t")
+        toks = ["%.6f" % v if i % 5 else "%.6e" % v for v in vals]
+        lines.append(f"row_{i}" + "\t" + sep.join(toks) + "\n")
+    out.append(("fractions_n41", "".join(lines), 3))
+    out.append(("k2_n3", O.kmer_tsv(O.kmer_table(reads(3, 30, 60), 2)).decode(), 16))
+    out.append(("k1_n1", O.kmer_tsv(O.kmer_table(reads(1, 30, 60), 1)).decode(), 2))
+    return out
+
+
+def kmer2pca_golden():
+    """Eigenvalue and projection files and stdout of the reference's own
+    kmer2pca.c (built into oracle/_ref and linked, through oracle/lapack_shim.c,
+    to the LAPACK dsyev inside scipy's OpenBLAS) on kmer2pca_tables()."""
+    cases = []
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        for name, text, dims in kmer2pca_tables():
+            (d / "in.tsv").write_text(text)
+            r = O.run_ref_tool("kmer2pca", ["in.tsv", "proj.txt", "ev.txt", str(dims), "4"], d)
+            assert r.returncode == 0, r.stdout[-400:]
+            cases.append({"name": name, "table": text, "dims": dims, "stdout": r.stdout.decode(),
+                          "ev": (d / "ev.txt").read_text(), "proj": (d / "proj.txt").read_text()})
+    (OUT / "kmer2pca.json").write_text(json.dumps({"cases": cases}))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         O.build()
     which = sys.argv[1:] or ["score", "fasta", "dbscan", "adaptive", "cluster", "closest", "config1", "subsets",
-                             "kmer", "callers", "fasta2kmer", "points", "trees"]
+                             "kmer", "callers", "fasta2kmer", "points", "trees", "kmer2pca"]
     if "score" in which:
         score_pairs()
     if "fasta" in which:
@@ -535,3 +578,5 @@ if __name__ == "__main__":
         points_golden()
     if "trees" in which:
         tree_golden()
+    if "kmer2pca" in which:
+        kmer2pca_golden()

@@ -50,7 +50,7 @@ def test_cli_tools_built():
     for t in ("cluster_dbscan_SW", "adaptive_clustering_SW", "find_closest_sequence_SW", "fasta2kmer",
               "cluster_dbscan_kmerL1", "cluster_dbscan_kmerL2", "cluster_dbscan_pca", "adaptive_clustering_kmer_L1",
               "adaptive_clustering_kmer_L2", "adaptive_clustering_PCA", "split_sets_to_newick", "tree_pureness",
-              "filter_split_sets_by_min", "split_set_to_fasta"):
+              "filter_split_sets_by_min", "split_set_to_fasta", "kmer2pca"):
         assert (swgpu.BIN_DIR / t).exists()
 
 

@@ -414,7 +414,7 @@ typedef struct {
   double ms_upload;     /* host time of the table check, conversion and copy */
   double ms_covariance; /* device time of the covariance kernels */
   double ms_gram;       /* device time of the Gram tile kernel inside it */
-  double ms_eigen;      /* host time of the eigen-decomposition (swe_pca) */
+  double ms_eigen;      /* host time of the eigen-decomposition call (swe_pca) */
   double ms_project;    /* device time of the projection kernel */
 } swe_pca_info;
 
@@ -434,6 +434,15 @@ swe_status swe_pca_covariance(swe_ctx* ctx, const double* data, int64_t n_sample
 swe_status swe_pca_eigen(const double* cov, int64_t n_features, int64_t n_vectors, double* eigenvalues,
                          double* vectors);
 
+/* swe_pca_eigen with the O(n_features^3) part on the GPU: the Householder
+   reduction (three launches per column, the matrix in device memory) and the
+   bisection of every eigenvalue; inverse iteration for the n_vectors wanted
+   vectors and their back-transformation on the host.  Same outputs and sign
+   rule as swe_pca_eigen, equal to it up to rounding; matrices below 64 x 64
+   and diagonal ones are solved on the host. */
+swe_status swe_pca_eigen_gpu(swe_ctx* ctx, const double* cov, int64_t n_features, int64_t n_vectors,
+                             double* eigenvalues, double* vectors);
+
 /* obtain_projections (kmer2pca.c:141-211): projections[j][i] = sum over k of
    data[j][k] * vectors[i][k] in the order of k (one fused multiply-add per
    term) for the `dimensions` vectors given (1 <= dimensions <= n_features).
@@ -443,8 +452,9 @@ swe_status swe_pca_project(swe_ctx* ctx, const double* data, int64_t n_samples, 
                            const double* vectors, int64_t dimensions, double* projections, swe_pca_info* info);
 
 /* The whole of kmer2pca after reading its file (kmer2pca.c:540-586): one
-   table upload, the covariance, the eigen-decomposition and the projections
-   onto the eigenvectors of the `dimensions` largest eigenvalues.
+   table upload, the covariance, the eigen-decomposition (swe_pca_eigen_gpu)
+   and the projections onto the eigenvectors of the `dimensions` largest
+   eigenvalues.
    eigenvalues[n_features] ascending, projections[n_samples][dimensions]. */
 swe_status swe_pca(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, int64_t dimensions,
                    double* eigenvalues, double* projections, swe_pca_info* info);

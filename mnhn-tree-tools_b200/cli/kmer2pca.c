@@ -6,21 +6,37 @@
  * The eigenvalue file gets every eigenvalue of the covariance matrix in
  * ascending order, one "%lf" per line; the projection file gets, per sample,
  * its raw counts projected onto the eigenvectors of the `dimensions` largest
- * eigenvalues, "%lf" tab separated.  Covariance and projections run on the
- * GPU through libswgpu (the table is uploaded once), the eigen-decomposition
- * on the host; n_threads is accepted and ignored.  Exits 1 on a missing
- * argument, a file that cannot be opened or read, dimensions outside
- * 1 .. n_features, or a GPU error (the reference reads past its arguments or
- * arrays there).
+ * eigenvalues, "%lf" tab separated.  Covariance, projections and the
+ * reduction and bisection of the eigen-decomposition run on the GPU through
+ * libswgpu (the table is uploaded once); n_threads is accepted and ignored.
+ * Exits 1 on a missing argument, a file that cannot be opened or read,
+ * dimensions outside 1 .. n_features, or a GPU error (the reference reads past
+ * its arguments or arrays there).
  */
 #define _POSIX_C_SOURCE 200809L
 #include <fcntl.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <unistd.h>
 
 #include "mnhn_dropin.h"
 #include "swgpu.h"
+
+/* The GPU context is opened on a second thread while the table is read. */
+typedef struct {
+  swe_ctx* ctx;
+  int status;
+} context_job;
+
+static void* open_context(void* arg) {
+  context_job* job = (context_job*)arg;
+  swe_opts opts = {0};
+  const char* dev = getenv("SWGPU_DEVICE");
+  opts.device = dev ? atoi(dev) : 0;
+  job->status = swe_create(&job->ctx, &opts);
+  return NULL;
+}
 
 static int failed(const char* what, swe_ctx* ctx, int st) {
   printf("%s failed: %s %s\n", what, swe_strerror(st), ctx ? swe_last_error(ctx) : "");
@@ -53,19 +69,21 @@ int main(int argc, char** argv) {
     printf("dimensions must lie in 1 .. %zu (features) and the table must hold samples\n", nf);
     return 1;
   }
+  context_job job = {NULL, 0};
+  pthread_t opener;
+  const int threaded = pthread_create(&opener, NULL, open_context, &job) == 0;
+  if (!threaded) open_context(&job);
   double* data = malloc(sizeof(double) * nf * n);
   FILE* infilep = fdopen(infile, "r");
-  if (!data || !infilep || swe_read_feature_table(infilep, shape, data) != 0) {
+  const int read_ok = data && infilep && swe_read_feature_table(infilep, shape, data) == 0;
+  if (threaded) pthread_join(opener, NULL);
+  if (!read_ok) {
     printf("Could not read the table in %s\n", argv[1]);
     return 1;
   }
   printf("Read in data complete: shape: features %lu samples %lu\n", (unsigned long)nf, (unsigned long)n);
-
-  swe_ctx* ctx = NULL;
-  swe_opts opts = {0};
-  const char* dev = getenv("SWGPU_DEVICE");
-  opts.device = dev ? atoi(dev) : 0;
-  int st = swe_create(&ctx, &opts);
+  swe_ctx* ctx = job.ctx;
+  int st = job.status;
   if (st) return failed("swe_create", NULL, st);
   double* cov = malloc(sizeof(double) * nf * nf);
   double* eigenvalues = malloc(sizeof(double) * nf);
@@ -76,8 +94,8 @@ int main(int argc, char** argv) {
   if (st) return failed("covariance", ctx, st);
   printf("Means complete \n");
   printf("Covariance complete\n");
-  st = swe_pca_eigen(cov, (int64_t)nf, (int64_t)dimensions, eigenvalues, vectors);
-  if (st) return failed("eigen-decomposition", NULL, st);
+  st = swe_pca_eigen_gpu(ctx, cov, (int64_t)nf, (int64_t)dimensions, eigenvalues, vectors);
+  if (st) return failed("eigen-decomposition", ctx, st);
   printf("Eigenspace obtained\n");
   st = swe_pca_project(ctx, NULL, (int64_t)n, (int64_t)nf, vectors, (int64_t)dimensions, projections, NULL);
   if (st) return failed("projection", ctx, st);

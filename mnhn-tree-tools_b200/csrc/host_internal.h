@@ -13,6 +13,18 @@
 
 namespace swgpu {
 
+// kmer2pca's eigen-decomposition pieces (pca_eigen.cpp).  A diagonal matrix is
+// solved directly, with dsyev's order of equal eigenvalues (false if A is not
+// diagonal).  pca_vectors_from_tridiagonal: the unit eigenvectors of the
+// n_vectors largest eigenvalues (eigenvalues: all of them, ascending) of the
+// tridiagonal T (d, e) of a Householder reduction whose reflector k
+// (k = 0 .. n-3) acts on indices k+1 .. n-1 and is stored in A[k][k+1 ..]
+// (first entry 1) with factor tau[k]; largest first, each signed so that its
+// largest-magnitude entry is positive.
+bool pca_eigen_diagonal(const double* A, int64_t n, int64_t n_vectors, double* eigenvalues, double* vectors);
+void pca_vectors_from_tridiagonal(const double* A, const double* tau, const double* d, const double* e, int64_t n,
+                                  const double* eigenvalues, int64_t n_vectors, double* vectors);
+
 // Integer form of the reference's neighbour test (float)d <= eps
 // (dbscan.c:548-551): d <= T with T = floor(eps) for eps >= 0, and no
 // neighbour at all (T = -1) for negative or NaN eps.  Exact while d < 2^24.

@@ -1,7 +1,9 @@
 // kmer2pca on the GPU (kmer2pca.c:286-597): the sample table resident in HBM,
 // the feature sums and the covariance matrix from one tiled pass over it, and
-// the projections of every sample onto the leading eigenvectors.  The
-// eigen-decomposition between them is host code (pca_eigen.cpp).
+// the projections of every sample onto the leading eigenvectors, and between
+// them the Householder reduction and the bisection of the eigen-decomposition
+// (the inverse iteration for the few wanted vectors is host code,
+// pca_eigen.cpp).
 //
 // What the reference computes (kmer2pca.c):
 //   means       m_i = (sum of x_ki over all n samples) / n              (466-481)
@@ -32,6 +34,7 @@
 #include <algorithm>
 #include <chrono>
 #include <climits>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -43,6 +46,7 @@ namespace swgpu {
 struct PcaState {
   DevBuf<int16_t> d_x16;
   DevBuf<double> d_x64, d_part, d_gram, d_colpart, d_shift, d_vec, d_proj;
+  DevBuf<double> d_eig, d_tri;  // eigen-decomposition: the matrix, then per-column vectors
   int64_t n = 0, nf = 0;
   bool resident = false;  // a table is on the device
   bool int16 = false;     // held as int16 (integral values in the int16 range)
@@ -172,6 +176,128 @@ __global__ void __launch_bounds__(256) pca_project_kernel(const T* __restrict__ 
   double acc = 0.0;
   for (int64_t k = 0; k < nf; ++k) acc = __fma_rn(val(x[k]), v[k], acc);
   P[idx] = acc;
+}
+
+// ---- eigen-decomposition of the covariance matrix ------------------------
+// The Householder reduction of the host solver (pca_eigen.cpp) with the matrix
+// in device memory (n_features^2 doubles, L2-resident for 5-mers), three
+// launches per column k: the reflector from row k (one CTA), p = tau A22 u
+// (a warp per row of the trailing block), and the rank-2 update
+// A22 -= u w^T + w u^T, w = p - (tau/2)(p.u) u, of the whole trailing block
+// (every CTA forms p.u itself).  Then every eigenvalue of the tridiagonal by
+// bisection on Sturm counts, a thread per eigenvalue.  The few wanted
+// eigenvectors come from inverse iteration and the stored reflectors on the
+// host.
+
+// Sum of v over the CTA (blockDim.x a multiple of 32), returned to every thread.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();  // sh may still be read by a previous call
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+  return t;
+}
+
+// Reflector of step k from x = A[k][k+1 .. n-1] (the column below the
+// diagonal): u (u[0] = 1) to `u` and into row k, tau[k], d[k] = A[k][k] and
+// e[k] = beta.  One CTA.
+__global__ void __launch_bounds__(1024) tri_reflector_kernel(double* __restrict__ A, int64_t n, int64_t k,
+                                                             double* __restrict__ u, double* __restrict__ tau,
+                                                             double* __restrict__ dd, double* __restrict__ ee) {
+  __shared__ double sh[32];
+  const int64_t m = n - k - 1;
+  double* x = A + k * n + k + 1;
+  const double alpha = x[0];
+  double s = 0.0;
+  for (int64_t i = 1 + threadIdx.x; i < m; i += blockDim.x) s = __fma_rn(x[i], x[i], s);
+  const double sigma = block_sum(s, sh);  // every read of x above happens before the writes below
+  double t = 0.0, beta = alpha, scale = 0.0;
+  if (sigma != 0.0) {
+    const double norm = sqrt(alpha * alpha + sigma);
+    beta = alpha <= 0.0 ? norm : -norm;
+    scale = 1.0 / (alpha - beta);
+    t = (beta - alpha) / beta;
+  }
+  for (int64_t i = threadIdx.x; i < m; i += blockDim.x) {
+    const double ui = i == 0 ? 1.0 : x[i] * scale;
+    u[i] = ui;
+    x[i] = ui;
+  }
+  if (threadIdx.x == 0) {
+    tau[k] = t;
+    dd[k] = A[k * n + k];
+    ee[k] = beta;
+  }
+}
+
+// p[i] = tau[k] * sum over j of A[k+1+i][k+1+j] u[j], a warp per row.
+__global__ void __launch_bounds__(256) tri_symv_kernel(const double* __restrict__ A, int64_t n, int64_t k,
+                                                       const double* __restrict__ u, const double* __restrict__ tau,
+                                                       double* __restrict__ p) {
+  const double t = tau[k];
+  if (t == 0.0) return;
+  const int64_t m = n - k - 1;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < m; i += warps) {
+    const double* row = A + (k + 1 + i) * n + k + 1;
+    double s = 0.0;
+    for (int64_t j = lane; j < m; j += 32) s = __fma_rn(row[j], u[j], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) p[i] = t * s;
+  }
+}
+
+// A22 -= u w^T + w u^T over the whole trailing block, rows spread over CTAs.
+__global__ void __launch_bounds__(256) tri_update_kernel(double* __restrict__ A, int64_t n, int64_t k,
+                                                         const double* __restrict__ u, const double* __restrict__ tau,
+                                                         const double* __restrict__ p) {
+  __shared__ double sh[32];
+  const double t = tau[k];
+  if (t == 0.0) return;
+  const int64_t m = n - k - 1;
+  double s = 0.0;
+  for (int64_t j = threadIdx.x; j < m; j += blockDim.x) s = __fma_rn(p[j], u[j], s);
+  const double K = 0.5 * t * block_sum(s, sh);
+  for (int64_t i = blockIdx.x; i < m; i += gridDim.x) {
+    const double ui = u[i], wi = p[i] - K * ui;
+    double* row = A + (k + 1 + i) * n + k + 1;
+    for (int64_t j = threadIdx.x; j < m; j += blockDim.x) {
+      const double uj = u[j], wj = p[j] - K * uj;
+      row[j] -= ui * wj + wi * uj;
+    }
+  }
+}
+
+// Eigenvalue j of the tridiagonal (d, e2 = e^2): the point where the Sturm
+// count passes from j to j + 1, bisected from [lo, hi] to a few ulps.
+__global__ void __launch_bounds__(128) tri_bisect_kernel(const double* __restrict__ d, const double* __restrict__ e2,
+                                                         int64_t n, double lo, double hi, double pivmin, double tnorm,
+                                                         double* __restrict__ lam) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double l = lo, u = hi;
+  for (int it = 0; it < 200; ++it) {
+    const double tol = 2 * DBL_EPSILON * fmax(fabs(l), fabs(u)) + DBL_EPSILON * tnorm + pivmin;
+    const double mid = l + 0.5 * (u - l);
+    if (u - l <= tol || mid <= l || mid >= u) break;
+    int64_t c = 0;
+    double q = d[0] - mid;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q <= 0.0;
+    for (int64_t i = 1; i < n; ++i) {
+      q = d[i] - mid - e2[i - 1] / q;
+      if (fabs(q) < pivmin) q = -pivmin;
+      c += q <= 0.0;
+    }
+    if (c > j) u = mid;
+    else l = mid;
+  }
+  lam[j] = l + 0.5 * (u - l);
 }
 
 double ms_since(std::chrono::steady_clock::time_point t0) {
@@ -417,6 +543,74 @@ swe_status pca_project(swe_ctx* ctx, PcaState* ps, const double* vectors, int64_
   return SWE_OK;
 }
 
+// Eigenvalues (ascending) and the eigenvectors of the n_vectors largest ones
+// of the symmetric host matrix cov, reduced and bisected on the GPU.  Diagonal
+// and small matrices go to the host solver.
+swe_status pca_eigen_device(swe_ctx* ctx, const double* cov, int64_t n, int64_t n_vectors, double* eigenvalues,
+                            double* vectors, double* ms_out) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int64_t i = 0; i < n * n; ++i)
+    if (!std::isfinite(cov[i])) return fail(ctx, SWE_ERR_INVALID, "pca: matrix entry not finite");
+  if (n < 64 || pca_eigen_diagonal(cov, n, n_vectors, eigenvalues, vectors)) {
+    swe_status s = n < 64 ? swe_pca_eigen(cov, n, n_vectors, eigenvalues, vectors) : SWE_OK;
+    if (ms_out) *ms_out = ms_since(t0);
+    return s ? fail(ctx, s, "pca: eigen-decomposition failed") : SWE_OK;
+  }
+  if (swe_status s = select_device(ctx)) return s;
+  PcaState* ps = nullptr;
+  if (swe_status s = pca_state(ctx, &ps)) return s;
+  cudaStream_t st = ctx->st;
+  CK(ps->d_eig.alloc((size_t)(n * n)));
+  CK(ps->d_tri.alloc((size_t)(6 * n)));  // u, p, tau, d, e, then d, e^2 / eigenvalues
+  double* A = ps->d_eig.p;
+  double *u = ps->d_tri.p, *p = u + n, *tau = p + n, *dd = tau + n, *ee = dd + n, *lam = ee + n;
+  CK(cpy(ctx, A, cov, sizeof(double) * (size_t)(n * n), cudaMemcpyHostToDevice, st));
+  const int sms = ctx->num_sms;
+  for (int64_t k = 0; k + 2 < n; ++k) {
+    const int64_t m = n - k - 1;
+    tri_reflector_kernel<<<1, 1024, 0, st>>>(A, n, k, u, tau, dd, ee);
+    tri_symv_kernel<<<(unsigned)std::min<int64_t>((m + 7) / 8, 8 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau, p);
+    tri_update_kernel<<<(unsigned)std::min<int64_t>(m, 4 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau, p);
+  }
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches += 3 * (n - 2);
+  std::vector<double> Ah((size_t)(n * n)), tau_h(n), d(n), e(n), e2(n);
+  CK(cpy(ctx, tau_h.data(), tau, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cpy(ctx, d.data(), dd, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cpy(ctx, e.data(), ee, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cpy(ctx, Ah.data(), A, sizeof(double) * (size_t)(n * n), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  d[n - 2] = Ah[(n - 2) * n + n - 2];
+  d[n - 1] = Ah[(n - 1) * n + n - 1];
+  e[n - 2] = Ah[(n - 2) * n + n - 1];
+  // Gershgorin bounds and the pivot floor, as the host bisection takes them
+  double lo = d[0], hi = d[0], emax2 = 0.0, tnorm = 0.0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double r = (i > 0 ? std::fabs(e[i - 1]) : 0) + (i + 1 < n ? std::fabs(e[i]) : 0);
+    lo = std::min(lo, d[i] - r);
+    hi = std::max(hi, d[i] + r);
+    if (i + 1 < n) {
+      e2[i] = e[i] * e[i];
+      emax2 = std::max(emax2, e2[i]);
+    }
+  }
+  tnorm = std::max(std::fabs(lo), std::fabs(hi));
+  const double pivmin = DBL_MIN * std::max(1.0, emax2);
+  const double pad = 2 * DBL_EPSILON * tnorm + 2 * pivmin;
+  // d and e^2 into the device scratch (over u and p), eigenvalues into lam
+  CK(cpy(ctx, u, d.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  CK(cpy(ctx, p, e2.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  tri_bisect_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(u, p, n, lo - pad, hi + pad, pivmin, tnorm, lam);
+  CK(cudaGetLastError());
+  ctx->stats.kernel_launches += 1;
+  CK(cpy(ctx, eigenvalues, lam, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  pca_vectors_from_tridiagonal(Ah.data(), tau_h.data(), d.data(), e.data(), n, eigenvalues, n_vectors, vectors);
+  if (n * n * sizeof(double) > (size_t(1) << 30)) ps->d_eig.release();
+  if (ms_out) *ms_out = ms_since(t0);
+  return SWE_OK;
+}
+
 }  // namespace
 }  // namespace swgpu
 
@@ -454,6 +648,17 @@ swe_status swe_pca_project(swe_ctx* ctx, const double* data, int64_t n_samples, 
   return s;
 }
 
+swe_status swe_pca_eigen_gpu(swe_ctx* ctx, const double* cov, int64_t n_features, int64_t n_vectors,
+                             double* eigenvalues, double* vectors) {
+  if (!ctx) return SWE_ERR_INVALID;
+  const int64_t n = n_features;
+  if (n < 0 || n_vectors < 0 || n_vectors > n || (n > 0 && (!cov || !eigenvalues)) || (n_vectors > 0 && !vectors) ||
+      n > 65536)
+    return fail(ctx, SWE_ERR_INVALID, "pca: bad eigen-decomposition arguments");
+  if (n == 0) return SWE_OK;
+  return pca_eigen_device(ctx, cov, n, n_vectors, eigenvalues, vectors, nullptr);
+}
+
 swe_status swe_pca(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, int64_t dimensions,
                    double* eigenvalues, double* projections, swe_pca_info* info) {
   if (!ctx) return SWE_ERR_INVALID;
@@ -469,10 +674,10 @@ swe_status swe_pca(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t 
     return fail(ctx, SWE_ERR_OOM, "pca: host matrices");
   }
   if (swe_status s = pca_covariance(ctx, ps, cov.data(), info)) return s;
-  const auto t0 = std::chrono::steady_clock::now();
-  if (swe_status s = swe_pca_eigen(cov.data(), n_features, dimensions, eigenvalues, vec.data()))
-    return fail(ctx, s, "pca: eigen-decomposition failed");
-  if (info) info->ms_eigen = ms_since(t0);
+  double ms_eigen = 0.0;
+  if (swe_status s = pca_eigen_device(ctx, cov.data(), n_features, dimensions, eigenvalues, vec.data(), &ms_eigen))
+    return s;
+  if (info) info->ms_eigen = ms_eigen;
   swe_status s = pca_project(ctx, ps, vec.data(), dimensions, projections, info);
   trim_pca_state(ps);
   return s;

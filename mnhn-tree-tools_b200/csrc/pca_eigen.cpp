@@ -332,6 +332,86 @@ void inverse_iteration(const double* d, const double* e, int64_t n, double lam, 
 
 }  // namespace
 
+namespace swgpu {
+
+bool pca_eigen_diagonal(const double* A, int64_t n, int64_t n_vectors, double* eigenvalues, double* vectors) {
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t j = 0; j < n; ++j)
+      if (j != i && A[i * n + j] != 0.0) return false;
+  // A diagonal matrix (the zero matrix of fewer than four samples among
+  // them) has the unit vectors as eigenvectors.  Equal eigenvalues leave the
+  // basis open; this takes the one dsyev returns, whose tridiagonal QL ends
+  // with a selection sort: for each position in turn the first strictly
+  // smallest value of the rest is swapped in.
+  std::vector<double> dv(n);
+  std::vector<int64_t> id(n);
+  for (int64_t i = 0; i < n; ++i) {
+    dv[i] = A[i * n + i];
+    id[i] = i;
+  }
+  for (int64_t i = 0; i + 1 < n; ++i) {
+    int64_t k = i;
+    for (int64_t j = i + 1; j < n; ++j)
+      if (dv[j] < dv[k]) k = j;
+    if (k != i) {
+      std::swap(dv[i], dv[k]);
+      std::swap(id[i], id[k]);
+    }
+  }
+  std::copy(dv.begin(), dv.end(), eigenvalues);
+  for (int64_t v = 0; v < n_vectors; ++v) {
+    double* y = vectors + v * n;
+    std::fill(y, y + n, 0.0);
+    y[id[n - 1 - v]] = 1.0;
+  }
+  return true;
+}
+
+void pca_vectors_from_tridiagonal(const double* A, const double* tau, const double* d, const double* e, int64_t n,
+                                  const double* eigenvalues, int64_t n_vectors, double* vectors) {
+  if (n_vectors == 0) return;
+  double tnorm = 0;
+  for (int64_t i = 0; i < n; ++i)
+    tnorm = std::max(tnorm, std::fabs(d[i]) + (i > 0 ? std::fabs(e[i - 1]) : 0) + (i + 1 < n ? std::fabs(e[i]) : 0));
+  // wanted eigenvalues, largest first; clusters (gaps below 1e-3 ||T||) are
+  // separated by a few ulps and orthogonalised against each other
+  const double cluster_gap = 1e-3 * tnorm, sep = 10 * DBL_EPSILON * std::max(tnorm, DBL_MIN);
+  std::vector<double> lam(n_vectors);
+  for (int64_t v = 0; v < n_vectors; ++v) {
+    lam[v] = eigenvalues[n - 1 - v];
+    if (v > 0 && lam[v] >= lam[v - 1] - sep) lam[v] = lam[v - 1] - sep;
+  }
+  for (int64_t v = 0; v < n_vectors; ++v) {
+    std::vector<const double*> others;
+    for (int64_t o = v - 1; o >= 0 && lam[o] - lam[v] < cluster_gap; --o) others.push_back(vectors + o * n);
+    double* y = vectors + v * n;
+    inverse_iteration(d, e, n, lam[v], tnorm, others, (uint64_t)v + 1, y);
+  }
+  // back to the basis of the covariance matrix: v = H_0 H_1 ... H_{n-3} y
+  RowPool pool(n >= 256 ? (int)std::min<int64_t>(host_threads(), n_vectors) : 1);
+  pool.run(0, n_vectors, [&](int64_t a, int64_t b) {
+    for (int64_t v = a; v < b; ++v) {
+      double* y = vectors + v * n;
+      for (int64_t k = n - 3; k >= 0; --k) {
+        if (tau[k] == 0.0) continue;
+        const double* u = A + k * n + k + 1;
+        const int64_t m = n - k - 1;
+        double s = 0;
+        for (int64_t j = 0; j < m; ++j) s += u[j] * y[k + 1 + j];
+        s *= tau[k];
+        for (int64_t j = 0; j < m; ++j) y[k + 1 + j] -= s * u[j];
+      }
+      int64_t big = 0;
+      for (int64_t i = 1; i < n; ++i)
+        if (std::fabs(y[i]) > std::fabs(y[big])) big = i;
+      if (y[big] < 0)
+        for (int64_t i = 0; i < n; ++i) y[i] = -y[i];
+    }
+  });
+}
+
+}  // namespace swgpu
+
 extern "C" swe_status swe_pca_eigen(const double* cov, int64_t n_features, int64_t n_vectors, double* eigenvalues,
                                     double* vectors) {
   const int64_t n = n_features;
@@ -348,84 +428,13 @@ extern "C" swe_status swe_pca_eigen(const double* cov, int64_t n_features, int64
   }
   for (double v : A)
     if (!std::isfinite(v)) return SWE_ERR_INVALID;
-  bool diagonal = true;
-  for (int64_t i = 0; i < n && diagonal; ++i)
-    for (int64_t j = 0; j < n; ++j)
-      if (j != i && A[i * n + j] != 0.0) {
-        diagonal = false;
-        break;
-      }
-  if (diagonal) {
-    // A diagonal matrix (the zero matrix of fewer than four samples among
-    // them) has the unit vectors as eigenvectors.  Equal eigenvalues leave
-    // the basis open; this takes the one dsyev returns, whose tridiagonal QL
-    // ends with a selection sort: for each position in turn the first
-    // strictly smallest value of the rest is swapped in.
-    std::vector<double> dv(n);
-    std::vector<int64_t> id(n);
-    for (int64_t i = 0; i < n; ++i) {
-      dv[i] = A[i * n + i];
-      id[i] = i;
-    }
-    for (int64_t i = 0; i + 1 < n; ++i) {
-      int64_t k = i;
-      for (int64_t j = i + 1; j < n; ++j)
-        if (dv[j] < dv[k]) k = j;
-      if (k != i) {
-        std::swap(dv[i], dv[k]);
-        std::swap(id[i], id[k]);
-      }
-    }
-    std::copy(dv.begin(), dv.end(), eigenvalues);
-    for (int64_t v = 0; v < n_vectors; ++v) {
-      double* y = vectors + v * n;
-      std::fill(y, y + n, 0.0);
-      y[id[n - 1 - v]] = 1.0;
-    }
-    return SWE_OK;
-  }
-  RowPool pool(n >= 256 ? host_threads() : 1);
+  if (swgpu::pca_eigen_diagonal(A.data(), n, n_vectors, eigenvalues, vectors)) return SWE_OK;
   std::vector<double> d(n), e(std::max<int64_t>(n - 1, 1), 0.0), tau(std::max<int64_t>(n - 2, 1), 0.0);
-  tridiagonalize(A.data(), n, d.data(), e.data(), tau.data(), pool);
-  eigenvalues_bisect(d.data(), e.data(), n, eigenvalues, pool);
-  if (n_vectors == 0) return SWE_OK;
-
-  double tnorm = 0;
-  for (int64_t i = 0; i < n; ++i)
-    tnorm = std::max(tnorm, std::fabs(d[i]) + (i > 0 ? std::fabs(e[i - 1]) : 0) + (i + 1 < n ? std::fabs(e[i]) : 0));
-  // wanted eigenvalues, largest first; clusters (gaps below 1e-3 ||T||) are
-  // separated by a few ulps and orthogonalised against each other
-  const double cluster_gap = 1e-3 * tnorm, sep = 10 * DBL_EPSILON * std::max(tnorm, DBL_MIN);
-  std::vector<double> lam(n_vectors);
-  for (int64_t v = 0; v < n_vectors; ++v) {
-    lam[v] = eigenvalues[n - 1 - v];
-    if (v > 0 && lam[v] >= lam[v - 1] - sep) lam[v] = lam[v - 1] - sep;
+  {
+    RowPool pool(n >= 256 ? host_threads() : 1);
+    tridiagonalize(A.data(), n, d.data(), e.data(), tau.data(), pool);
+    eigenvalues_bisect(d.data(), e.data(), n, eigenvalues, pool);
   }
-  for (int64_t v = 0; v < n_vectors; ++v) {
-    std::vector<const double*> others;
-    for (int64_t o = v - 1; o >= 0 && lam[o] - lam[v] < cluster_gap; --o) others.push_back(vectors + o * n);
-    double* y = vectors + v * n;
-    inverse_iteration(d.data(), e.data(), n, lam[v], tnorm, others, (uint64_t)v + 1, y);
-  }
-  // back to the basis of the covariance matrix: v = H_0 H_1 ... H_{n-3} y
-  pool.run(0, n_vectors, [&](int64_t a, int64_t b) {
-    for (int64_t v = a; v < b; ++v) {
-      double* y = vectors + v * n;
-      for (int64_t k = n - 3; k >= 0; --k) {
-        if (tau[k] == 0.0) continue;
-        const double* u = A.data() + k * n + k + 1;
-        const int64_t m = n - k - 1;
-        double s = 0;
-        for (int64_t j = 0; j < m; ++j) s += u[j] * y[k + 1 + j];
-        s *= tau[k];
-        for (int64_t j = 0; j < m; ++j) y[k + 1 + j] -= s * u[j];
-      }
-      int64_t big = 0;
-      for (int64_t i = 1; i < n; ++i)
-        if (std::fabs(y[i]) > std::fabs(y[big])) big = i;
-      if (y[big] < 0)
-        for (int64_t i = 0; i < n; ++i) y[i] = -y[i];
-    }
-  });
+  swgpu::pca_vectors_from_tridiagonal(A.data(), tau.data(), d.data(), e.data(), n, eigenvalues, n_vectors, vectors);
   return SWE_OK;
 }

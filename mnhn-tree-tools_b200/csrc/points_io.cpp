@@ -31,6 +31,25 @@ namespace {
 
 inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
 
+// A token that is an optional '-' and 1 .. max_digits decimal digits (every
+// count of a k-mer table) as its integer value: what strtod / strtof return
+// for it whenever the value is exactly representable (max_digits 15 for
+// double, 7 for float).  False for any other token.
+inline bool small_integer(const char* tok, int max_digits, long long* out) {
+  const char* c = tok;
+  const bool neg = *c == '-';
+  if (neg) ++c;
+  long long v = 0;
+  int nd = 0;
+  for (; *c >= '0' && *c <= '9'; ++c, ++nd) {
+    if (nd == max_digits) return false;
+    v = v * 10 + (*c - '0');
+  }
+  if (nd == 0 || *c != '\0' || (neg && v == 0)) return false;  // "-0" is -0.0: left to strtod
+  *out = neg ? -v : v;
+  return true;
+}
+
 float* alloc_values(size_t n) {
   void* p = nullptr;
   const size_t padded = (n + 8) & ~size_t(7);  // whole 8-float vectors, as the reference's AVX loop reads
@@ -151,7 +170,8 @@ dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape) {
     }
   }
   read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
-    ds.values[field][sample] = strtof(tok, nullptr);
+    long long v;
+    ds.values[field][sample] = small_integer(tok, 7, &v) ? (float)v : strtof(tok, nullptr);
     return true;
   });
   return ds;
@@ -161,6 +181,11 @@ int swe_read_feature_table(FILE* in_file, data_shape shape, double* data) {
   if (!in_file || (!data && shape.n_features * shape.n_samples > 0)) return SWE_ERR_INVALID;
   std::atomic<int> bad{0};
   const uint64_t got = read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
+    long long iv;
+    if (small_integer(tok, 15, &iv)) {
+      data[sample * shape.n_features + field] = (double)iv;
+      return true;
+    }
     char* end = nullptr;
     const double v = strtod(tok, &end);
     if (end == tok) {

@@ -144,7 +144,7 @@ EXPORTS = [
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
     "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition",
-    "swe_pca_covariance", "swe_pca_eigen", "swe_pca_project", "swe_pca",
+    "swe_pca_covariance", "swe_pca_eigen", "swe_pca_eigen_gpu", "swe_pca_project", "swe_pca",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -289,6 +289,8 @@ def lib():
                                          C.POINTER(PcaInfo)]
         L.swe_pca_eigen.restype = C.c_int
         L.swe_pca_eigen.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
+        L.swe_pca_eigen_gpu.restype = C.c_int
+        L.swe_pca_eigen_gpu.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
         L.swe_pca_project.restype = C.c_int
         L.swe_pca_project.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
                                       C.c_void_p, C.POINTER(PcaInfo)]
@@ -542,6 +544,17 @@ class Engine:
         _check(lib().swe_pca_covariance(self.ctx, X.ctypes.data, n, nf, cov.ctypes.data, C.byref(info)), self.ctx)
         self._pca_rows = n
         return cov, info.as_dict()
+
+    def pca_eigen(self, cov, n_vectors: int) -> tuple[np.ndarray, np.ndarray]:
+        """swgpu.pca_eigen with the reduction and the bisection on the GPU
+        (swe_pca_eigen_gpu)."""
+        A = np.ascontiguousarray(cov, dtype=np.float64)
+        n = A.shape[0]
+        w = np.zeros(n)
+        V = np.zeros((max(n_vectors, 1), n))
+        _check(lib().swe_pca_eigen_gpu(self.ctx, A.ctypes.data, n, n_vectors, w.ctypes.data, V.ctypes.data),
+               self.ctx)
+        return w, V[:n_vectors]
 
     def pca_project(self, table, vectors) -> np.ndarray:
         """obtain_projections (kmer2pca.c:141-211): (samples, len(vectors)) sums

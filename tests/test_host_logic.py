@@ -348,3 +348,8 @@ def test_kmer_file_loader_matches_reference_semantics(tmp_path):
     want = O.load_kmer_text(text)
     assert shape == (want.shape[0], want.shape[1])
     assert np.array_equal(V, want)
+    # integer tokens take a shortcut: the same float bits, signed zero included
+    text = "a\t-0\t+5\t1234567\t16777217\t-007\nb\t0\t-1\t9999999\t12345678\t3\n"
+    p.write_text(text)
+    _, V = _load_kmer_file_with_lib(p)
+    assert np.array_equal(V.view(np.uint32), O.load_kmer_text(text).view(np.uint32))

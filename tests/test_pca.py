@@ -167,6 +167,9 @@ def test_read_feature_table_matches_oracle(tmp_path):
     for case in load_golden("kmer2pca.json")["cases"]:
         st, X = _read_with_lib(tmp_path, case["table"])
         assert st == 0 and np.array_equal(X, O.read_feature_table(case["table"])), case["name"]
+    text = "a\t-0\t+5\t007\nb 1e3 3.5 -12\nc\t-0.0\t123456789012345\t1234567890123456789\n"
+    st, X = _read_with_lib(tmp_path, text)
+    assert st == 0 and np.array_equal(X.view(np.uint64), O.read_feature_table(text).view(np.uint64))
     st, _ = _read_with_lib(tmp_path, "a\t1\t2\nb\t3\n")  # file ends early
     assert st != 0
     st, _ = _read_with_lib(tmp_path, "a\t1\t2\nb\t3\tx\n")  # not a number
@@ -257,6 +260,39 @@ def test_pca_matches_oracle(eng):
         if len(T) < 4:  # zero covariance: dsyev's unit vectors, projections are raw columns
             assert np.array_equal(P, T[:, ::-1][:, :d].astype(float)), name
         assert info["ms_gram"] >= 0 and info["ms_project"] >= 0
+
+
+@pytest.mark.gpu
+def test_gpu_eigen_matches_host_eigen(eng):
+    """swe_pca_eigen_gpu (reduction and bisection on the GPU) against the host
+    solver and numpy: eigenvalues to 1e-12 of the largest, eigenvectors where
+    eigenvalues are apart, eigen-residuals and orthonormality everywhere."""
+    rng = np.random.default_rng(21)
+    mats = []
+    for n, rows in [(64, 300), (65, 40), (256, 97), (300, 2000), (1024, 3000)]:
+        X = rng.poisson(1.5, size=(rows, n)).astype(float)
+        X[:, : n // 10] = 0  # features that never occur: exact zero rows and columns
+        mats.append(O.pca_covariance(X))
+    Q, _ = np.linalg.qr(rng.normal(size=(80, 80)))
+    lam = np.concatenate([np.linspace(0.1, 1.0, 77), [5.0, 5.0, 5.0]])
+    mats.append((Q * lam) @ Q.T)
+    mats[-1] = (mats[-1] + mats[-1].T) / 2
+    mats.append(np.diag(rng.normal(size=70)))
+    for A in mats:
+        n = A.shape[0]
+        d = min(7, n)
+        w, V = eng.pca_eigen(A, d)
+        wh, Vh = swgpu.pca_eigen(A, d)
+        scale = np.abs(wh).max()
+        assert np.abs(w - wh).max() <= 1e-12 * scale, n
+        assert np.abs(w - np.linalg.eigvalsh(A)).max() <= 1e-12 * scale, n
+        assert np.abs(V @ V.T - np.eye(d)).max() <= 1e-10, n
+        assert np.abs(A @ V.T - V.T * w[::-1][:d]).max() <= 1e-10 * scale, n
+        top = np.sort(wh)[::-1][:d + 1]
+        for i in range(d):
+            gaps = [abs(top[i] - top[j]) for j in (i - 1, i + 1) if 0 <= j < len(top)]
+            if min(gaps) > 1e-6 * scale:
+                assert np.abs(V[i] - Vh[i]).max() <= 1e-9, (n, i)
 
 
 @pytest.mark.gpu

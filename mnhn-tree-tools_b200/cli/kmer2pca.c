@@ -15,28 +15,12 @@
  */
 #define _POSIX_C_SOURCE 200809L
 #include <fcntl.h>
-#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <unistd.h>
 
 #include "mnhn_dropin.h"
 #include "swgpu.h"
-
-/* The GPU context is opened on a second thread while the table is read. */
-typedef struct {
-  swe_ctx* ctx;
-  int status;
-} context_job;
-
-static void* open_context(void* arg) {
-  context_job* job = (context_job*)arg;
-  swe_opts opts = {0};
-  const char* dev = getenv("SWGPU_DEVICE");
-  opts.device = dev ? atoi(dev) : 0;
-  job->status = swe_create(&job->ctx, &opts);
-  return NULL;
-}
 
 static int failed(const char* what, swe_ctx* ctx, int st) {
   printf("%s failed: %s %s\n", what, swe_strerror(st), ctx ? swe_last_error(ctx) : "");
@@ -69,21 +53,19 @@ int main(int argc, char** argv) {
     printf("dimensions must lie in 1 .. %zu (features) and the table must hold samples\n", nf);
     return 1;
   }
-  context_job job = {NULL, 0};
-  pthread_t opener;
-  const int threaded = pthread_create(&opener, NULL, open_context, &job) == 0;
-  if (!threaded) open_context(&job);
   double* data = malloc(sizeof(double) * nf * n);
   FILE* infilep = fdopen(infile, "r");
-  const int read_ok = data && infilep && swe_read_feature_table(infilep, shape, data) == 0;
-  if (threaded) pthread_join(opener, NULL);
-  if (!read_ok) {
+  if (!data || !infilep || swe_read_feature_table(infilep, shape, data) != 0) {
     printf("Could not read the table in %s\n", argv[1]);
     return 1;
   }
   printf("Read in data complete: shape: features %lu samples %lu\n", (unsigned long)nf, (unsigned long)n);
-  swe_ctx* ctx = job.ctx;
-  int st = job.status;
+
+  swe_ctx* ctx = NULL;
+  swe_opts opts = {0};
+  const char* dev = getenv("SWGPU_DEVICE");
+  opts.device = dev ? atoi(dev) : 0;
+  int st = swe_create(&ctx, &opts);
   if (st) return failed("swe_create", NULL, st);
   double* cov = malloc(sizeof(double) * nf * nf);
   double* eigenvalues = malloc(sizeof(double) * nf);

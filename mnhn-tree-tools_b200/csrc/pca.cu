@@ -616,71 +616,86 @@ swe_status pca_eigen_device(swe_ctx* ctx, const double* cov, int64_t n, int64_t 
 
 using namespace swgpu;
 
+namespace {
+
+// Runs a call's body with host allocation failures turned into SWE_ERR_OOM
+// (nothing is thrown across the C ABI) and the call's info cleared first.
+template <class F>
+swe_status pca_call(swe_ctx* ctx, swe_pca_info* info, F&& body) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (info) *info = swe_pca_info{};
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, SWE_ERR_OOM, "pca: host allocation failed");
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 swe_status swe_pca_covariance(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, double* cov,
                               swe_pca_info* info) {
-  if (!ctx) return SWE_ERR_INVALID;
-  if (!cov) return fail(ctx, SWE_ERR_INVALID, "pca: no covariance buffer");
-  PcaState* ps = nullptr;
-  if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
-  swe_status s = pca_covariance(ctx, ps, cov, info);
-  trim_pca_state(ps);
-  return s;
+  return pca_call(ctx, info, [&]() -> swe_status {
+    if (!cov) return fail(ctx, SWE_ERR_INVALID, "pca: no covariance buffer");
+    PcaState* ps = nullptr;
+    if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
+    swe_status s = pca_covariance(ctx, ps, cov, info);
+    trim_pca_state(ps);
+    return s;
+  });
 }
 
 swe_status swe_pca_project(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features,
                            const double* vectors, int64_t dimensions, double* projections, swe_pca_info* info) {
-  if (!ctx) return SWE_ERR_INVALID;
-  if (dimensions < 1 || dimensions > n_features || !vectors || !projections)
-    return fail(ctx, SWE_ERR_INVALID, "pca: bad projection arguments");
-  PcaState* ps = nullptr;
-  if (data) {
-    if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
-  } else {
-    ps = ctx->pca;
-    if (!ps || !ps->resident || ps->n != n_samples || ps->nf != n_features)
-      return fail(ctx, SWE_ERR_STATE, "pca: no resident table of this shape");
-    if (swe_status s = select_device(ctx)) return s;
-  }
-  swe_status s = pca_project(ctx, ps, vectors, dimensions, projections, info);
-  trim_pca_state(ps);
-  return s;
+  return pca_call(ctx, info, [&]() -> swe_status {
+    if (dimensions < 1 || dimensions > n_features || !vectors || !projections)
+      return fail(ctx, SWE_ERR_INVALID, "pca: bad projection arguments");
+    PcaState* ps = nullptr;
+    if (data) {
+      if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
+    } else {
+      ps = ctx->pca;
+      if (!ps || !ps->resident || ps->n != n_samples || ps->nf != n_features)
+        return fail(ctx, SWE_ERR_STATE, "pca: no resident table of this shape");
+      if (swe_status s = select_device(ctx)) return s;
+    }
+    swe_status s = pca_project(ctx, ps, vectors, dimensions, projections, info);
+    trim_pca_state(ps);
+    return s;
+  });
 }
 
 swe_status swe_pca_eigen_gpu(swe_ctx* ctx, const double* cov, int64_t n_features, int64_t n_vectors,
                              double* eigenvalues, double* vectors) {
-  if (!ctx) return SWE_ERR_INVALID;
-  const int64_t n = n_features;
-  if (n < 0 || n_vectors < 0 || n_vectors > n || (n > 0 && (!cov || !eigenvalues)) || (n_vectors > 0 && !vectors) ||
-      n > 65536)
-    return fail(ctx, SWE_ERR_INVALID, "pca: bad eigen-decomposition arguments");
-  if (n == 0) return SWE_OK;
-  return pca_eigen_device(ctx, cov, n, n_vectors, eigenvalues, vectors, nullptr);
+  return pca_call(ctx, nullptr, [&]() -> swe_status {
+    const int64_t n = n_features;
+    if (n < 0 || n_vectors < 0 || n_vectors > n || (n > 0 && (!cov || !eigenvalues)) ||
+        (n_vectors > 0 && !vectors) || n > 65536)
+      return fail(ctx, SWE_ERR_INVALID, "pca: bad eigen-decomposition arguments");
+    if (n == 0) return SWE_OK;
+    return pca_eigen_device(ctx, cov, n, n_vectors, eigenvalues, vectors, nullptr);
+  });
 }
 
 swe_status swe_pca(swe_ctx* ctx, const double* data, int64_t n_samples, int64_t n_features, int64_t dimensions,
                    double* eigenvalues, double* projections, swe_pca_info* info) {
-  if (!ctx) return SWE_ERR_INVALID;
-  if (dimensions < 1 || dimensions > n_features || !eigenvalues || !projections)
-    return fail(ctx, SWE_ERR_INVALID, "pca: bad arguments");
-  PcaState* ps = nullptr;
-  if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
-  std::vector<double> cov, vec;
-  try {
-    cov.resize((size_t)(n_features * n_features));
-    vec.resize((size_t)(dimensions * n_features));
-  } catch (const std::bad_alloc&) {
-    return fail(ctx, SWE_ERR_OOM, "pca: host matrices");
-  }
-  if (swe_status s = pca_covariance(ctx, ps, cov.data(), info)) return s;
-  double ms_eigen = 0.0;
-  if (swe_status s = pca_eigen_device(ctx, cov.data(), n_features, dimensions, eigenvalues, vec.data(), &ms_eigen))
+  return pca_call(ctx, info, [&]() -> swe_status {
+    if (dimensions < 1 || dimensions > n_features || !eigenvalues || !projections)
+      return fail(ctx, SWE_ERR_INVALID, "pca: bad arguments");
+    PcaState* ps = nullptr;
+    if (swe_status s = pca_upload(ctx, data, n_samples, n_features, &ps, info)) return s;
+    std::vector<double> cov((size_t)(n_features * n_features)), vec((size_t)(dimensions * n_features));
+    if (swe_status s = pca_covariance(ctx, ps, cov.data(), info)) return s;
+    double ms_eigen = 0.0;
+    if (swe_status s = pca_eigen_device(ctx, cov.data(), n_features, dimensions, eigenvalues, vec.data(), &ms_eigen))
+      return s;
+    if (info) info->ms_eigen = ms_eigen;
+    swe_status s = pca_project(ctx, ps, vec.data(), dimensions, projections, info);
+    trim_pca_state(ps);
     return s;
-  if (info) info->ms_eigen = ms_eigen;
-  swe_status s = pca_project(ctx, ps, vec.data(), dimensions, projections, info);
-  trim_pca_state(ps);
-  return s;
+  });
 }
 
 }  // extern "C"

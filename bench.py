@@ -375,6 +375,15 @@ def kmer2pca_leg(eng, seqs, dev, k: int = 5, dims: int = 7, cpu: bool = True, re
     return out
 
 
+def side_leg(fn, *args, **kw):
+    """A side leg's object; a leg that fails reports its error in place of its
+    numbers instead of taking the main line down with it."""
+    try:
+        return fn(*args, **kw)
+    except Exception as e:  # noqa: BLE001 - any failure of a side measurement
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def run_leg(args):
     """One side leg alone (profiling a small case of its kernels)."""
     import swgpu
@@ -669,9 +678,10 @@ def run_gpu(args):
             "prefilter_speedup": None,
         }
         if world == 1 and wl["gen"] == "config2" and not args.no_kmer:
-            line["fasta2kmer"] = fasta2kmer_leg(seqs, cpu=not args.no_cpu_baseline)
-            line["kmer_dbscan"] = kmer_dbscan_leg(eng, seqs, dev, cpu=not args.no_cpu_baseline)
-            line["kmer2pca"] = kmer2pca_leg(eng, seqs, dev, cpu=not args.no_cpu_baseline)
+            cpu_leg = not args.no_cpu_baseline
+            line["fasta2kmer"] = side_leg(fasta2kmer_leg, seqs, cpu=cpu_leg)
+            line["kmer_dbscan"] = side_leg(kmer_dbscan_leg, eng, seqs, dev, cpu=cpu_leg)
+            line["kmer2pca"] = side_leg(kmer2pca_leg, eng, seqs, dev, cpu=cpu_leg)
         print(json.dumps(line), flush=True)
     eng.close()
     del flush

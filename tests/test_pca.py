@@ -346,3 +346,21 @@ def test_kmer2pca_tool_matches_reference(tmp_path, build):
         assert _columns_match_up_to_sign(got, _proj(proj, dims), PRINT_TOL), name
         if name.endswith(("_n3", "_n1")):  # no sample in the sums: the same files byte for byte
             assert (tmp_path / "ev.txt").read_text() == ev and (tmp_path / "proj.txt").read_text() == proj
+
+
+def test_kmer2pca_tool_rejects_bad_arguments_before_the_gpu(tmp_path):
+    """The CLI's argument and file errors come before it opens the GPU: usage
+    text for fewer than five arguments (the reference reads argv[5] with
+    four), exit 1 for dimensions outside 1 .. n_features, a missing or
+    unreadable table."""
+    exe = swgpu.BIN_DIR / "kmer2pca"
+    (tmp_path / "t.tsv").write_text("s0\t1\t2\t3\ns1\t4\t5\t6\n")
+    (tmp_path / "bad.tsv").write_text("s0\t1\t2\t3\ns1\t4\tx\t6\n")
+    runs = [["t.tsv", "p", "e", "2"], ["t.tsv", "p", "e", "0", "1"], ["t.tsv", "p", "e", "4", "1"],
+            ["missing.tsv", "p", "e", "1", "1"], ["bad.tsv", "p", "e", "1", "1"]]
+    for args in runs:
+        r = subprocess.run([str(exe), *args], cwd=tmp_path, capture_output=True, timeout=60)
+        assert r.returncode == 1, args
+    r = subprocess.run([str(exe), "t.tsv"], cwd=tmp_path, capture_output=True, timeout=60)
+    assert r.stdout.decode().startswith("Arguments are: \n [FILE-in ] kmer file to apply PCA on")
+    assert not (tmp_path / "p").exists() and not (tmp_path / "e").exists()

@@ -70,6 +70,37 @@ def test_reference_skips_the_last_samples():
     assert np.abs(np.linalg.eigvalsh(O.pca_covariance(X)) - ev).max() <= PRINT_TOL
 
 
+def test_reference_tool_matches_oracle_on_more_tables(tmp_path):
+    """The reference's kmer2pca (oracle/_ref, run here on the host) against the
+    oracle on tables the golden file does not hold: a protein 2-mer table
+    (400 features), a DNA 5-mer table (1,024 features, 1,203 reads) and a
+    table of negative and large counts with n % 4 == 2."""
+    ref = O.REF_DIR / "kmer2pca"
+    if not ref.exists():
+        pytest.skip("reference kmer2pca not built")
+    rng = np.random.default_rng(8)
+    dna = np.frombuffer(b"ACGT", dtype=np.uint8)
+    aa = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", dtype=np.uint8)
+    prot = [aa[rng.integers(0, 20, size=int(rng.integers(200, 600)))].tobytes() for _ in range(450)]
+    reads = [dna[rng.integers(0, 4, size=int(rng.integers(80, 300)))].tobytes() for _ in range(1203)]
+    wide = rng.integers(-3000, 30000, size=(130, 12))
+    tables = [("protein_k2", O.kmer_tsv(O.kmer_table(prot, 2, True)).decode(), 6),
+              ("dna_k5", O.kmer_tsv(O.kmer_table(reads, 5)).decode(), 7),
+              ("wide_n130", "".join("r%d\t" % i + "\t".join(str(v) for v in row) + "\n"
+                                     for i, row in enumerate(wide)), 4)]
+    for name, text, dims in tables:
+        (tmp_path / "in.tsv").write_text(text)
+        r = subprocess.run([str(ref), "in.tsv", "p.txt", "e.txt", str(dims), "4"], cwd=tmp_path,
+                           capture_output=True, timeout=600)
+        assert r.returncode == 0, name
+        X = O.read_feature_table(text)
+        w, P = O.kmer2pca(X, dims)
+        ev = np.array([float(t) for t in (tmp_path / "e.txt").read_text().split()])
+        assert np.abs(w - ev).max() <= PRINT_TOL * max(1.0, np.abs(w).max() / 1e6), name
+        tol = PRINT_TOL * max(1.0, np.abs(P).max() / 1e6)
+        assert _columns_match_up_to_sign(P, _proj((tmp_path / "p.txt").read_text(), dims), tol), name
+
+
 def test_exact_covariance_is_the_reference_sum():
     rng = np.random.default_rng(3)
     for n, nf in [(1, 3), (4, 2), (7, 5), (64, 9), (203, 16)]:

@@ -14,6 +14,7 @@
 // leaves the value unset and stops advancing).  swe_read_feature_table reads
 // the same stream with strtod (fscanf("%lf")) into kmer2pca's row-major
 // doubles and reports such a token, or a short file, as an error.
+#include <errno.h>
 #include <fcntl.h>
 #include <unistd.h>
 
@@ -31,21 +32,23 @@ namespace {
 
 inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
 
-// A token that is an optional '-' and 1 .. max_digits decimal digits (every
-// count of a k-mer table) as its integer value: what strtod / strtof return
-// for it whenever the value is exactly representable (max_digits 15 for
-// double, 7 for float).  False for any other token.
-inline bool small_integer(const char* tok, int max_digits, long long* out) {
+// A token of `len` bytes that is an optional '-' and 1 .. max_digits decimal
+// digits (every count of a k-mer table) as its integer value: what strtod /
+// strtof return for it whenever the value is exactly representable
+// (max_digits 15 for double, 7 for float).  False for any other token.
+inline bool small_integer(const char* tok, size_t len, int max_digits, long long* out) {
   const char* c = tok;
-  const bool neg = *c == '-';
+  const char* end = tok + len;
+  const bool neg = c < end && *c == '-';
   if (neg) ++c;
+  const size_t nd = (size_t)(end - c);
+  if (nd == 0 || nd > (size_t)max_digits) return false;
   long long v = 0;
-  int nd = 0;
-  for (; *c >= '0' && *c <= '9'; ++c, ++nd) {
-    if (nd == max_digits) return false;
+  for (; c < end; ++c) {
+    if (*c < '0' || *c > '9') return false;
     v = v * 10 + (*c - '0');
   }
-  if (nd == 0 || *c != '\0' || (neg && v == 0)) return false;  // "-0" is -0.0: left to strtod
+  if (neg && v == 0) return false;  // "-0" is -0.0: left to strtod
   *out = neg ? -v : v;
   return true;
 }
@@ -61,16 +64,30 @@ float* alloc_values(size_t n) {
 
 // Reads the token stream of a table file (a label, then n_features numbers,
 // per sample, whitespace anywhere) on host threads and hands each number token
-// to on_value(sample, feature, token) as a NUL-terminated string; returns the
-// number of tokens found (at most (n_features + 1) * n_samples are used).
+// to on_value(sample, feature, token, length); the token lies in a buffer
+// where whitespace or a NUL follows it, so strtod / strtof can read it in
+// place.  Returns the number of tokens found (at most (n_features + 1) *
+// n_samples are used).
 template <class F>
 uint64_t read_fields(FILE* in_file, data_shape shape, F&& on_value) {
   rewind(in_file);
   std::vector<char> text;
   {
-    char chunk[1 << 16];
-    size_t got;
-    while ((got = fread(chunk, 1, sizeof chunk, in_file)) > 0) text.insert(text.end(), chunk, chunk + got);
+    // the whole file in one buffer: sized from the stream's length when it has
+    // one, grown chunk by chunk otherwise (a pipe)
+    size_t have = 0;
+    if (fseeko(in_file, 0, SEEK_END) == 0) {
+      const off_t size = ftello(in_file);
+      if (size > 0) text.resize((size_t)size);
+    }
+    rewind(in_file);
+    for (;;) {
+      if (have == text.size()) text.resize(std::max<size_t>(text.size() * 2, size_t(1) << 16));
+      const size_t got = fread(text.data() + have, 1, text.size() - have, in_file);
+      have += got;
+      if (got == 0) break;
+    }
+    text.resize(have);
   }
   text.push_back('\0');
   const size_t len = text.size() - 1;
@@ -110,20 +127,19 @@ uint64_t read_fields(FILE* in_file, data_shape shape, F&& on_value) {
   std::vector<std::thread> th;
   for (int t = 0; t < T; ++t)
     th.emplace_back([&, t]() {
-      char tmp[128];
-      tokens(cut[t], cut[t + 1], [&](uint64_t k, size_t q0, size_t q1) {
-        const uint64_t g = first[t] + k;
+      // token g of the stream is field g % fields of sample g / fields
+      uint64_t g = first[t], sample = g / fields, field = g % fields;
+      tokens(cut[t], cut[t + 1], [&](uint64_t, size_t q0, size_t q1) {
         if (g >= want) return false;
-        const uint64_t sample = g / fields, field = g % fields;
-        if (field == 0) return true;  // the label, read with "%s"
-        const size_t L = q1 - q0;
-        if (L < sizeof tmp) {
-          memcpy(tmp, text.data() + q0, L);
-          tmp[L] = '\0';
-          return on_value(sample, field - 1, (const char*)tmp);
+        bool go = true;
+        if (field != 0)  // field 0 is the label, read with "%s"
+          go = on_value(sample, field - 1, (const char*)text.data() + q0, q1 - q0);
+        ++g;
+        if (++field == fields) {
+          field = 0;
+          ++sample;
         }
-        std::string s(text.data() + q0, L);
-        return on_value(sample, field - 1, s.c_str());
+        return go;
       });
     });
   for (auto& x : th) x.join();
@@ -136,22 +152,34 @@ extern "C" {
 
 data_shape shape_from_kmer_file(int infile) {
   data_shape s{0, 0};
-  const off_t size = lseek(infile, 0, SEEK_END);
   lseek(infile, 0, SEEK_SET);
-  if (size <= 0) return s;
-  std::vector<char> buf((size_t)size);
-  if (read(infile, buf.data(), (size_t)size) != (ssize_t)size) {
-    printf("Could not read file in order to read obtain data shape\n");
-    swgpu::dropin_set_status(SWE_ERR_IO);
-    return s;
+  // dataset.c:370-378: the tabs of the first line, then the newlines from
+  // the end of the first line on; read in 8 MB pieces
+  std::vector<char> buf(size_t(8) << 20);
+  bool first_line = true;
+  for (;;) {
+    const ssize_t got = read(infile, buf.data(), buf.size());
+    if (got < 0) {
+      if (errno == EINTR) continue;
+      printf("Could not read file in order to read obtain data shape\n");
+      swgpu::dropin_set_status(SWE_ERR_IO);
+      return data_shape{0, 0};
+    }
+    if (got == 0) break;
+    const char* p = buf.data();
+    const char* end = p + got;
+    if (first_line) {
+      const char* nl = static_cast<const char*>(memchr(p, '\n', (size_t)(end - p)));
+      s.n_features += (size_t)std::count(p, nl ? nl : end, '\t');
+      if (!nl) continue;
+      first_line = false;
+      p = nl;
+    }
+    while ((p = static_cast<const char*>(memchr(p, '\n', (size_t)(end - p)))) != nullptr) {
+      s.n_samples++;
+      ++p;
+    }
   }
-  size_t i = 0;
-  while (i < buf.size() && buf[i] != '\n') {  // dataset.c:370-373: tabs of the first line
-    if (buf[i] == '\t') s.n_features++;
-    i++;
-  }
-  for (; i < buf.size(); i++)  // dataset.c:375-378: newlines from the first one on
-    if (buf[i] == '\n') s.n_samples++;
   return s;
 }
 
@@ -169,9 +197,9 @@ dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape) {
       return ds;
     }
   }
-  read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
+  read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok, size_t len) {
     long long v;
-    ds.values[field][sample] = small_integer(tok, 7, &v) ? (float)v : strtof(tok, nullptr);
+    ds.values[field][sample] = small_integer(tok, len, 7, &v) ? (float)v : strtof(tok, nullptr);
     return true;
   });
   return ds;
@@ -180,9 +208,9 @@ dataset load_kmer_from_file_into_dataset(FILE* in_file, data_shape shape) {
 int swe_read_feature_table(FILE* in_file, data_shape shape, double* data) {
   if (!in_file || (!data && shape.n_features * shape.n_samples > 0)) return SWE_ERR_INVALID;
   std::atomic<int> bad{0};
-  const uint64_t got = read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok) {
+  const uint64_t got = read_fields(in_file, shape, [&](uint64_t sample, uint64_t field, const char* tok, size_t len) {
     long long iv;
-    if (small_integer(tok, 15, &iv)) {
+    if (small_integer(tok, len, 15, &iv)) {
       data[sample * shape.n_features + field] = (double)iv;
       return true;
     }

@@ -217,6 +217,18 @@ def test_replay_random_graphs():
         assert swgpu.dbscan_from_matrix(D, eps, mp) == O.dbscan(D, eps, mp), (trial, n, eps, mp)
 
 
+def test_replay_rows_of_many_words():
+    """Rows of more than 8 bitmap words (n > 512): the replay tests words in
+    blocks of 8 before walking them; clusters spread over every block."""
+    rng = np.random.default_rng(12)
+    for n in (513, 777, 1600, 2100):
+        centres = rng.normal(size=(int(rng.integers(3, 9)), 2)) * 20
+        pts = centres[rng.integers(0, len(centres), size=n)] + rng.normal(size=(n, 2)) * 2
+        D = np.round(np.sqrt(((pts[:, None] - pts[None]) ** 2).sum(-1)) * 10).astype(np.uint32)
+        for eps, mp in ((15.0, 4), (40.0, 10), (4.0, 2)):
+            assert swgpu.dbscan_from_matrix(D, eps, mp) == O.dbscan(D, eps, mp), (n, eps, mp)
+
+
 @pytest.fixture(scope="module")
 def host_driver(tmp_path_factory):
     exe = tmp_path_factory.mktemp("drv") / "adaptive_host_driver"

@@ -58,6 +58,19 @@ def test_golden_reference_outputs_match_oracle():
                                   "Covariance complete\nEigenspace obtained\n" % (X.shape[1], X.shape[0]))
 
 
+def test_host_eigen_on_golden_tables():
+    """The library's host solver (swe_pca_eigen) on the oracle's covariance of
+    each golden table prints the reference's eigenvalue file and projections
+    (through the oracle's FMA projection) to the last printed digit."""
+    for case in load_golden("kmer2pca.json")["cases"]:
+        X = O.read_feature_table(case["table"])
+        w, V = swgpu.pca_eigen(O.pca_covariance(X), case["dims"])
+        ev = np.array([float(t) for t in case["ev"].split()])
+        assert np.abs(w - ev).max() <= PRINT_TOL, case["name"]
+        P = O.pca_project(X, V)
+        assert _columns_match_up_to_sign(P, _proj(case["proj"], case["dims"]), PRINT_TOL), case["name"]
+
+
 def test_reference_skips_the_last_samples():
     """The reference's covariance leaves out the last n % 4 samples: with all
     samples summed the golden eigenvalues are not reproduced."""

@@ -104,12 +104,15 @@ def config2(seed: int = 2, n: int = 20000, n_fam: int = 200, n_frac: float = 0.0
 
 
 def config3(seed: int = 3, n: int = 100000, n_fam: int = 50, mono: int = 171,
-            min_len: int = 150, max_len: int = 342):
+            min_len: int = 150, max_len: int = 342, with_rc: bool = False):
+    """Returns (reads, family of each read), plus with_rc a boolean array
+    marking the reverse-complemented reads."""
     rng = np.random.default_rng(seed)
     monos = [_random_seq(rng, mono) for _ in range(n_fam)]
     fam = rng.integers(0, n_fam, size=n)
     seqs = []
-    for f in fam:
+    rc = np.zeros(n, dtype=bool)
+    for k, f in enumerate(fam):
         arr = np.concatenate([monos[f], monos[f]])
         L = int(rng.integers(min_len, max_len + 1))
         st = int(rng.integers(0, 2 * mono - L + 1))
@@ -117,7 +120,10 @@ def config3(seed: int = 3, n: int = 100000, n_fam: int = 50, mono: int = 171,
         s = _mutate(rng, s, rng.uniform(0.02, 0.15), 0.0)
         if rng.random() < 0.5:
             s = COMP[s[::-1]]
+            rc[k] = True
         seqs.append(s)
+    if with_rc:
+        return _to_bytes(seqs), fam, rc
     return _to_bytes(seqs), fam
 
 

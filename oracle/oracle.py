@@ -38,10 +38,16 @@ _ref = None
 # loading
 # --------------------------------------------------------------------------
 
+def reference_dir() -> str:
+    """The reference's source tree: $MNHN_REFERENCE_DIR, else the default
+    mount point /root/reference."""
+    return os.environ.get("MNHN_REFERENCE_DIR") or "/root/reference"
+
+
 def build(ref_src: str | None = None) -> None:
     """Compile liboracle.so (and the reference into _ref/ when its sources exist)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    src = ref_src or "/root/reference"
+    src = ref_src or reference_dir()
     if os.path.isdir(src):
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={src}"], check=True)
 
@@ -397,6 +403,12 @@ def ref_harness():
         H.refh_score_rows.restype = C.c_int
         H.refh_score_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                       C.c_int]
+        H.refh_score_block.restype = C.c_int
+        H.refh_score_block.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.c_int, C.c_void_p, C.c_int]
+        H.refh_score_pairs.restype = C.c_int
+        H.refh_score_pairs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong,
+                                       C.c_void_p, C.c_int]
         _harness = H
     return _harness
 
@@ -434,6 +446,71 @@ def ref_dbscan(seqs, eps: float, minpts: int):
                   sa.n, None, 0, mx)
     s = R.dbscan_SW(ds, C.c_float(eps), minpts)
     return [[s.clusters[c].members[k] for k in range(s.clusters[c].n_members)] for c in range(s.n_clusters)]
+
+
+def ref_score_block(seqs, rows, cols, threads: int = 0) -> np.ndarray:
+    """Reference score() on rows x cols (D[r][c] = score(seq[cols[c]],
+    seq[rows[r]]), region_query's argument order) on all host cores."""
+    sa = _SeqArray(seqs)
+    rows_arr = np.ascontiguousarray(rows, dtype=np.int32)
+    cols_arr = np.ascontiguousarray(cols, dtype=np.int32)
+    out = np.zeros((len(rows_arr), len(cols_arr)), dtype=np.uint32)
+    ref_harness().refh_score_block(sa.ptrs, sa.lens, sa.n, rows_arr.ctypes.data, len(rows_arr),
+                                   cols_arr.ctypes.data, len(cols_arr), out.ctypes.data,
+                                   threads or os.cpu_count())
+    return out
+
+
+def ref_score_pairs(seqs, a, b, threads: int = 0) -> np.ndarray:
+    """Reference score(seq[a[k]], seq[b[k]]) for every k, on all host cores."""
+    sa = _SeqArray(seqs)
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    out = np.zeros(len(a), dtype=np.uint32)
+    ref_harness().refh_score_pairs(sa.ptrs, sa.lens, sa.n, a.ctypes.data, b.ctypes.data, len(a),
+                                   out.ctypes.data, threads or os.cpu_count())
+    return out
+
+
+def write_neighbor_bitmap_file(path, n: int, row_blocks, eps: float) -> int:
+    """Neighbour bits of one eps in the "SWB1" form score_subst.c reads: bit j
+    of row i is (float)D[i][j] <= eps, the test of region_query
+    (dbscan.c:548-551), evaluated here in float32 on the distances of each
+    (row0, uint32 rows) block that `row_blocks` yields in row order.  Returns
+    the number of neighbour pairs (ordered, self included)."""
+    words = (n + 63) // 64
+    e = np.float32(eps)
+    total = 0
+    nxt = 0
+    with open(path, "wb") as f:
+        f.write(b"SWB1" + struct.pack("<II", n, words))
+        for r0, block in row_blocks:
+            assert r0 == nxt and block.shape[1] == n
+            bits = block.astype(np.float32) <= e
+            total += int(bits.sum())
+            packed = np.packbits(bits, axis=1, bitorder="little")
+            out = np.zeros((block.shape[0], words * 8), dtype=np.uint8)
+            out[:, :packed.shape[1]] = packed
+            f.write(out.tobytes())
+            nxt += block.shape[0]
+    assert nxt == n
+    return total
+
+
+def read_split_set_file(path) -> list[list[int]]:
+    """Clusters (member lists in stored order) of a split-set file
+    (cluster_io.c:638-669: "SPLIT_SET", int32 count, per cluster int32
+    n_members, int32 id, members)."""
+    b = Path(path).read_bytes()
+    assert b[:9] == b"SPLIT_SET"
+    (nc,) = struct.unpack_from("<i", b, 9)
+    pos, out = 13, []
+    for _ in range(nc):
+        nm, _cid = struct.unpack_from("<ii", b, pos)
+        pos += 8
+        out.append(list(struct.unpack_from(f"<{nm}i", b, pos)))
+        pos += 4 * nm
+    return out
 
 
 def write_dist_file(path, D: np.ndarray) -> None:

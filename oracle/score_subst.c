@@ -13,11 +13,23 @@
  * dataset_from_fasta (dataset.c:264-344) with `ld --wrap`: the real loader
  * runs, then its pointer table is recorded and sorted.
  *
- * The distance matrix comes from the file named by $SWGPU_SUBST_DIST:
- *   bytes 0..3   "SWD1"
- *   bytes 4..7   uint32 n
- *   bytes 8..11  uint32 element size (2 or 4)
- *   bytes 12..   n*n little-endian unsigned distances, row-major
+ * The distances come from the file named by $SWGPU_SUBST_DIST, in one of two
+ * forms:
+ *   "SWD1"  uint32 n, uint32 element size (2 or 4), then n*n little-endian
+ *           unsigned distances, row-major (a symmetric matrix)
+ *   "SWB1"  uint32 n, uint32 words per row w, then n rows of w little-endian
+ *           uint64 words: bit (j % 64) of word j / 64 of row i is set when
+ *           pair (i, j) is an eps-neighbour pair of the one eps the tool is
+ *           run with.  score() answers 0 for a set bit and 0xFFFFFFFF
+ *           otherwise, so region_query's (float)d <= eps test (dbscan.c:548)
+ *           selects exactly the set bits.  This form serves single-eps
+ *           DBSCAN runs whose full matrix would not fit in memory.
+ *
+ * region_query calls score(seq[i], seq[point]) for i = 0 .. n-1 in order
+ * (dbscan.c:546-551).  The shim answers from row `point` (the distance is
+ * symmetric, smith-waterman.c:16-80 being a transposed DP), so the reads
+ * are sequential, and it remembers the last two indices it resolved, so a
+ * call costs O(1) instead of a binary search.
  */
 #define _GNU_SOURCE
 #include <fcntl.h>
@@ -50,7 +62,10 @@ typedef struct {
 static ptr_entry* g_map = NULL;
 static int g_n = 0;
 static const unsigned char* g_data = NULL;
-static unsigned g_elem = 0;
+static unsigned g_elem = 0;      /* 2 or 4 (distances), 0 (neighbour bits) */
+static size_t g_row_words = 0;   /* uint64 words per bitmap row */
+static const char* const* g_seq = NULL;  /* dataset order, for the O(1) hits */
+static int g_last_a = -1, g_last_b = -1;
 
 static int cmp_ptr(const void* a, const void* b) {
   const char* pa = ((const ptr_entry*)a)->ptr;
@@ -74,15 +89,24 @@ static void load_matrix(int n) {
   close(fd);
   if (m == MAP_FAILED) die("cannot map distance file");
   const unsigned char* b = (const unsigned char*)m;
-  if (st.st_size < 12 || memcmp(b, "SWD1", 4) != 0) die("bad magic");
+  if (st.st_size < 12) die("bad magic");
   uint32_t fn, fe;
   memcpy(&fn, b + 4, 4);
   memcpy(&fe, b + 8, 4);
   if ((int)fn != n) die("matrix size does not match the FASTA record count");
-  if (fe != 2 && fe != 4) die("element size must be 2 or 4");
-  if ((size_t)st.st_size != 12 + (size_t)fn * fn * fe) die("truncated matrix");
+  if (memcmp(b, "SWD1", 4) == 0) {
+    if (fe != 2 && fe != 4) die("element size must be 2 or 4");
+    if ((size_t)st.st_size != 12 + (size_t)fn * fn * fe) die("truncated matrix");
+    g_elem = fe;
+  } else if (memcmp(b, "SWB1", 4) == 0) {
+    if ((size_t)fe != ((size_t)fn + 63) / 64) die("bitmap rows must hold ceil(n/64) words");
+    if ((size_t)st.st_size != 12 + (size_t)fn * fe * 8) die("truncated bitmap");
+    g_elem = 0;
+    g_row_words = fe;
+  } else {
+    die("bad magic");
+  }
   g_data = b + 12;
-  g_elem = fe;
 }
 
 dataset __wrap_dataset_from_fasta(FILE* in) {
@@ -95,6 +119,7 @@ dataset __wrap_dataset_from_fasta(FILE* in) {
       g_map[i].idx = i;
     }
     qsort(g_map, (size_t)g_n, sizeof(ptr_entry), cmp_ptr);
+    g_seq = (const char* const*)ds.sequences;
     load_matrix(g_n);
   }
   return ds;
@@ -112,13 +137,27 @@ static int index_of(const char* p) {
   return -1;
 }
 
+/* index of p, trying the last index `*last` and its successor first */
+static int index_near(const char* p, int* last) {
+  int k = *last;
+  if (k >= 0 && g_seq[k] == p) return k;
+  if (k + 1 < g_n && g_seq[k + 1] == p) return (*last = k + 1);
+  return (*last = index_of(p));
+}
+
 unsigned int score(char* A, char* B, size_t len_a, size_t len_b, int* work) {
   (void)len_a;
   (void)len_b;
   (void)work;
   if (!g_data) die("score() called before the dataset was loaded");
-  size_t i = (size_t)index_of(A), j = (size_t)index_of(B);
-  size_t k = i * (size_t)g_n + j;
+  const size_t i = (size_t)index_near(A, &g_last_a);
+  const size_t j = (size_t)index_near(B, &g_last_b);
+  if (g_elem == 0) {
+    uint64_t w;
+    memcpy(&w, g_data + 8 * (j * g_row_words + i / 64), 8);
+    return ((w >> (i % 64)) & 1u) ? 0u : 0xFFFFFFFFu;
+  }
+  const size_t k = j * (size_t)g_n + i;  /* row of B: D is symmetric */
   if (g_elem == 2) {
     uint16_t v;
     memcpy(&v, g_data + 2 * k, 2);

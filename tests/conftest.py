@@ -34,7 +34,7 @@ def _ensure_built():
     import swgpu
     if not (ROOT / "oracle" / "liboracle.so").exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
-    if os.path.isdir("/root/reference") and not O.ref_available():
+    if os.path.isdir(O.reference_dir()) and not O.ref_available():
         O.build()
     swgpu.build()
 

@@ -106,6 +106,41 @@ def test_config1_rows_match_reference_golden():
         assert zlib.crc32(R[k].tobytes()) == g["row_crc32"][r], r
 
 
+def test_score_substitution_forms_match_reference_tool(tmp_path):
+    """The score-substitution build of cluster_dbscan_SW (oracle/score_subst.c)
+    answers score() from a file.  Given the distances of 200 config-1 reads,
+    as a matrix ("SWD1") and as the neighbour bits of the one eps ("SWB1"), it
+    prints and writes byte for byte what the real reference tool does."""
+    if not (O.REF_DIR / "cluster_dbscan_SW_subst").exists():
+        pytest.skip("reference build (oracle/_ref) not present")
+    from swgpu import workloads as W
+    seqs, _ = W.config1()
+    seqs = seqs[::10][:200]
+    D = O.all_pairs(seqs)
+    eps, minpts = 200.0, 5
+    runs = {}
+    for name in ("real", "matrix", "bits"):
+        d = tmp_path / name
+        d.mkdir()
+        W.write_fasta(d / "r.fa", seqs)
+        env = None
+        if name == "matrix":
+            O.write_dist_file(d / "d.bin", D)
+            env = {"SWGPU_SUBST_DIST": str(d / "d.bin")}
+        elif name == "bits":
+            n = O.write_neighbor_bitmap_file(d / "d.bin", len(seqs), [(0, D)], eps)
+            assert n == int((D <= eps).sum())
+            env = {"SWGPU_SUBST_DIST": str(d / "d.bin")}
+        tool = "cluster_dbscan_SW" if name == "real" else "cluster_dbscan_SW_subst"
+        p = O.run_ref_tool(tool, ["r.fa", eps, minpts, "c"], d, env)
+        assert p.returncode == 0, p.stderr
+        files = {f.name: f.read_bytes() for f in sorted(d.glob("c-*"))}
+        runs[name] = (p.stdout, files)
+    assert runs["real"][0].startswith(b"16 clusters")
+    assert runs["matrix"] == runs["real"]
+    assert runs["bits"] == runs["real"]
+
+
 def test_kmer_table_oracle_matches_reference_fasta2kmer(tmp_path):
     """The oracle's frequency table + text (kmers.c:157-389) reproduces the
     reference fasta2kmer's stdout byte for byte (sha256) on every golden run:

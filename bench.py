@@ -1,29 +1,35 @@
 """Benchmark of the all-pairs Smith-Waterman neighbourhood engine on B200.
 
-One step = one all-pairs score pass over the config-2 workload (20,000 reads,
-lognormal 100-600 bp, median 220, 200 families, 2% 'N' runs) followed by the
-adaptive DBSCAN sweep (minpts 5) that the one score pass serves; the sweep's
-layers and log are produced exactly as the reference tool would.
+Default workload (config 3): 100,000 satellite-like reads (50 tandem-repeat
+monomer families of 171 bp, reads of 150-342 bp, 2-15% substitution, half
+reverse-complemented).  One step = one all-pairs score pass (5e9 unique
+pairs, 3.0e14 DP cells) followed by the DBSCAN it serves (eps 400, minpts 10),
+labels produced exactly as the reference's cluster_dbscan_SW would.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl swgpu|reference]
+                    [--config 2|3|4|5]
 
 Under torchrun each rank drives its own GPU on its own independently seeded
-config-2 dataset (independent objects, no data-path collective: weak
-scaling); the step time is the max over ranks.
+dataset of the same configuration (independent objects, no data-path
+collective: weak scaling); the step time is the max over ranks.
 
 Printed value: exact SW GCUPS = unique-pair DP cells (sum over i<j of
-len_i*len_j) / seconds of the whole step (score pass + sweep), inputs already
-resident on the device.  `e2e` is the same metric through the C ABI with host
-buffers (upload, score pass, sweep, results back on the host) every step.
+len_i*len_j) / seconds of the whole step (score pass + clustering), inputs
+already resident on the device.  `e2e` is the same metric through the C ABI
+with host buffers (upload, score pass, clustering, results back on the host),
+repeated --e2e-reps times (default 2).
+
+On one GPU the config-3 line carries the other workloads as side legs, each
+with --leg-warmup / --leg-steps steps: `sweep_config2` (20,000 reads, one
+score pass + the 8-eps adaptive sweep), `config5` (500 split sets in one
+score launch + every set's sweep, against the sets one by one) and `config4`
+(the learned prefilter against the exact step: speed-up, eps-neighbour
+recall, adjusted Rand, the same recipe without the network);
+`prefilter_speedup` is config 4's headline speed-up.
 
 `--impl reference` times the reference's own CPU score() (compiled from its
 sources into oracle/_ref) on all host cores on a bounded row sample of the
 same workload and prints the same metric from it.
-
-On config 2 the line also carries `fasta2kmer`: the k-mer table and its text
-(fasta2kmer's frequencies_from_dataset + write_kmer_base, k = 5) for the same
-reads through the drop-in C ABI, beside the reference's own two functions on
-all host cores.
 """
 from __future__ import annotations
 
@@ -89,10 +95,16 @@ def env_rank():
 # ---------------------------------------------------------------------------
 # reference CPU arm / baseline
 # ---------------------------------------------------------------------------
+_REF_PROBE = {}
+
+
 def reference_sample(seqs, target_s: float = 12.0, threads: int = 0):
     """Times the reference score() (or, without oracle/_ref, the oracle's C
     restatement) on all host cores over a bounded sample of query rows x all
-    sequences.  Returns (GCUPS, info dict)."""
+    sequences.  Returns (GCUPS, info dict).  The first call on a data set
+    times a probe of one row per thread to size the sample; later calls on
+    the same data set reuse that rate (the sample is the same seeded row
+    choice every time)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
 
@@ -102,14 +114,16 @@ def reference_sample(seqs, target_s: float = 12.0, threads: int = 0):
     fn = O.ref_score_rows if kind == "reference" else O.score_rows
     L = np.array([len(s) for s in seqs], dtype=np.float64)
     rng = np.random.default_rng(0)
-    rows = [int(r) for r in rng.choice(len(seqs), size=max(threads, 8), replace=False)]
-    t0 = time.perf_counter()
-    fn(seqs, rows, threads)
-    dt = time.perf_counter() - t0
-    cells = float(L[rows].sum() * L.sum())
-    rate = cells / dt
+    key = (id(seqs), len(seqs), threads)
+    if key not in _REF_PROBE:
+        rows = [int(r) for r in rng.choice(len(seqs), size=max(threads, 8), replace=False)]
+        t0 = time.perf_counter()
+        fn(seqs, rows, threads)
+        dt = time.perf_counter() - t0
+        _REF_PROBE[key] = (len(rows), dt)
+    probe_rows, probe_dt = _REF_PROBE[key]
     # grow the sample to about target_s seconds of CPU work
-    n_rows = int(min(len(seqs), max(len(rows), len(rows) * target_s / max(dt, 1e-3))))
+    n_rows = int(min(len(seqs), max(threads, probe_rows * target_s / max(probe_dt, 1e-3))))
     rows = [int(r) for r in rng.choice(len(seqs), size=n_rows, replace=False)]
     t0 = time.perf_counter()
     fn(seqs, rows, threads)
@@ -517,27 +531,84 @@ def hbm_peak_gbs():
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def run_gpu(args):
-    import torch
+class Run:
+    """One bench process: its rank and GPU, the process group (N > 1), the
+    L2-flush buffer, the barrier and the max over ranks.  Every rank takes the
+    same collective steps in the same order."""
 
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.rank, self.local, self.world = env_rank()
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+        self.dev = self.local
+        torch.cuda.set_device(self.dev)
+        self.flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{self.dev}")
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+        self.torch.cuda.synchronize(self.dev)
+
+    def flush_l2(self):
+        """Writes 256 MB (more than the 126 MB L2) between timed steps."""
+        self.flush.fill_(1)
+        self.torch.cuda.synchronize(self.dev)
+
+    def max(self, x: float) -> float:
+        return max_over_ranks(x, self.dist, f"cuda:{self.dev}")
+
+    def close(self):
+        del self.flush
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def fast_roofline(eng_cells: float, kernel_ms: float, dev: int, traffic=None) -> dict:
+    """The hot kernel against the integer roofline R = 2*P_int/K (P_int measured
+    on this GPU by the instruction-mix probe)."""
+    import swgpu
+    fast_gcups = eng_cells / (kernel_ms * 1e-3) / 1e9
+    _, peak_instr = swgpu.measure_mix_peak(dev)
+    # R = 2 * P_int / K: P_int = lane instructions/s of the per-cell mix at full
+    # issue on this GPU, K = 4.5 instructions per packed cell pair in that mix
+    roof_peak = 2.0 * peak_instr / 4.5 / 1e9
+    return {"bound": "int", "kernel": "fast_all_pairs_kernel", "achieved": round(fast_gcups, 1),
+            "peak": round(roof_peak, 1), "unit": "Gcell/s", "frac": round(fast_gcups / roof_peak, 4),
+            "peak_source": "measured on this GPU: issue rate of the kernel's per-cell 16x2 "
+                           "instruction mix on independent chains, R = 2*P_int/4.5",
+            "peak_k4": round(roof_peak * 4.5 / 4.0, 1),
+            "frac_k4": round(fast_gcups / (roof_peak * 4.5 / 4.0), 4),
+            "k4_note": "R = 2*P_int/4: the recurrence's minimum of 4 packed instructions per cell pair",
+            "ms_per_launch": round(kernel_ms, 2),
+            "traffic": traffic,
+            "traffic_source": ("DRAM read+write bytes per launch from one ncu capture, stored in "
+                               "profiles/fast_all_pairs_kernel_traffic.txt" if traffic else None)}
+
+
+def measure_single(run: Run, config: str, args, steps: int, warmup: int, e2e_reps: int, cpu: bool,
+                   kmer_legs: bool = False):
+    """One data set: `warmup` untimed and `steps` timed steps of one all-pairs
+    score pass + the DBSCAN (config 3) or adaptive sweep (config 2) it serves,
+    then `e2e_reps` host-to-host repetitions through the C ABI.  Returns the
+    line (rank 0) or None."""
     import swgpu
     from swgpu import workloads as W
 
-    rank, local, world = env_rank()
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = local
-    torch.cuda.set_device(dev)
-
-    wl = WORKLOADS[args.config]
+    torch = run.torch
+    rank, world, dev = run.rank, run.world, run.dev
+    wl = WORKLOADS[config]
     gen = getattr(W, wl["gen"])
     split = bool(args.split)  # one data set over all ranks (strong scaling) instead of one per rank
-    seqs, _ = gen(seed=dataset_seed(args.config, 0 if split else rank))
+    seqs, _ = gen(seed=dataset_seed(config, 0 if split else rank))
     if args.n:
         seqs = seqs[:args.n]
     cells = W.cells(seqs)
@@ -545,18 +616,17 @@ def run_gpu(args):
     if split:
         from swgpu import split_pass
         eng.set_partition(rank, world)
+    # tile plan of the 16x2 kernel from the autotuner (every rank of a split
+    # pass must lay out the same tiles, so that mode keeps the default plan)
+    tune = None if (split or args.no_autotune) else eng.autotune(seqs)
     eng.upload(seqs)
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    exch = []
 
     def score():
         eng.score_all_pairs()
         if split and world > 1:  # the one exchange: bytewise minimum of the ranks' matrices
-            split_pass.combine_parts(eng, dist, f"cuda:{dev}")
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
+            exch.append(split_pass.exchange_tiles(eng, run.dist, f"cuda:{dev}"))
 
     def cluster():
         # the number of kept layers / clusters; the split sets stay in the library
@@ -571,123 +641,154 @@ def run_gpu(args):
         kept = cluster()
         return eng.timer_stop(), kept
 
-    for _ in range(args.warmup):
-        flush.fill_(1)
-        torch.cuda.synchronize(dev)
+    for _ in range(warmup):
+        run.flush_l2()
         step()
 
     st0 = eng.stats()
-    barrier()
+    run.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
     step_ms, kernel_ms, score_ms = [], [], []
     kept = None
-    for _ in range(args.steps):
-        flush.fill_(1)  # L2 flush between timed steps (256 MB > 126 MB L2)
-        torch.cuda.synchronize(dev)
+    for _ in range(steps):
+        run.flush_l2()  # L2 flush between timed steps (256 MB > 126 MB L2)
         ms, kept = step()
         s = eng.stats()
         step_ms.append(ms)
         kernel_ms.append(s["ms_fast_kernel"])
         score_ms.append(s["ms_score_pass"])
-    barrier()
+    run.barrier()
     clk = clocks.stop()
     st1 = eng.stats()
-    total_ms = sum(step_ms)
-    total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
-    ms_per_step = total_ms / args.steps
+    total_ms = run.max(sum(step_ms))
+    ms_per_step = total_ms / steps
     value = cells * (1 if split else world) / (ms_per_step * 1e-3) / 1e9
-    launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
+    launches = (st1["kernel_launches"] - st0["kernel_launches"]) // steps
 
     # the eps threshold kernel alone (HBM-bound): one launch per distinct
     # threshold, timed by the engine's CUDA events around the launch
     thr_ms = []
     for k in range(3):
-        eng.dbscan((wl.get("eps") or wl["eps_start"]) + k, wl["minpts"])
+        eng.dbscan((wl.get("eps") or wl["eps_start"]) + k, wl["minpts"], lists=False)
         thr_ms.append(eng.stats()["ms_last_neighbors"])
     thr_ms = statistics.median(thr_ms)
 
-    # e2e through the C ABI with host buffers: upload + score + sweep + results on the host
+    # e2e through the C ABI with host buffers: upload + score + clustering + results on the host
     e2e_ms = []
-    b0 = eng.stats()
-    for _ in range(max(1, args.steps)):
-        barrier()
+    for _ in range(max(1, e2e_reps)):
+        run.barrier()
         t0 = time.perf_counter()
         eng.upload(seqs)
         score()
         cluster()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     b1 = eng.stats()
-    e2e_total = sum(e2e_ms)
-    e2e_total = max_over_ranks(e2e_total, dist, f"cuda:{dev}")
+    e2e_total = run.max(sum(e2e_ms))
     e2e_value = cells * (1 if split else world) / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
-    # upload() resets the counters, so the last step's totals are the per-step figures
+    # upload() resets the counters, so the last repetition's totals are the per-step figures
     h2d = b1["h2d_bytes"]
     d2h = b1["d2h_bytes"]
 
+    line = None
     if rank == 0:
         kms = statistics.median(kernel_ms)
-        fast_gcups = st1["cells"] / (world if split else 1) / (kms * 1e-3) / 1e9
-        peak_cells, peak_instr = swgpu.measure_mix_peak(dev)
-        # R = 2 * P_int / K: P_int = lane instructions/s of the per-cell mix at full
-        # issue on this GPU, K = 4.5 instructions per packed cell pair in that mix
-        roof_peak = 2.0 * peak_instr / 4.5 / 1e9
-        traffic = measured_traffic("fast_all_pairs_kernel", f"config{args.config}") if not args.n else None
+        traffic = measured_traffic("fast_all_pairs_kernel", f"config{config}") if not args.n else None
+        roof = fast_roofline(st1["cells"] / (world if split else 1), kms, dev, traffic)
         n = len(seqs)
         dist_bytes = st1["dist_bytes"]
         thr_bytes = n * n * dist_bytes + n * ((n + 63) // 64) * 8 + n * 4
         hbm_peak = hbm_peak_gbs()
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        cpu_line = None
+        if world == 1 and cpu:
             g, info = reference_sample(seqs, target_s=args.ref_seconds)
-            cpu = dict(info, value=round(g, 3), unit="GCUPS")
+            cpu_line = dict(info, value=round(g, 3), unit="GCUPS")
         sweep_s = (statistics.median(step_ms) - statistics.median(score_ms)) * 1e-3
+        mat_gb = n * n * dist_bytes / 1e9
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 2), "higher_is_better": True,
+            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": round(ms_per_step, 2), "higher_is_better": True,
             "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "s16x2", "data": "synthetic",
-            "config": {"workload": wl["text"], "n_sequences": len(seqs), "cells_per_gpu": cells,
-                       "pairs_per_gpu": len(seqs) * (len(seqs) - 1) // 2,
-                       "kept_layers" if wl["mode"] == "adaptive" else "clusters":
-                           kept,
-                       "parallelism": (f"one dataset split over {world} GPUs (cost-balanced tile groups, one all-reduce)" if split else f"{world} independent datasets (one per GPU)"),
-                       "l2": "256 MB buffer written between timed steps (L2 flush); distance matrix 800 MB"},
+            "config": {"workload": wl["text"], "n_sequences": n, "cells_per_gpu": cells,
+                       "pairs_per_gpu": n * (n - 1) // 2,
+                       "kept_layers" if wl["mode"] == "adaptive" else "clusters": kept,
+                       "parallelism": (f"one dataset split over {world} GPUs (cost-balanced tile groups; each "
+                                       f"rank all-gathers the others' tile rectangles)" if split
+                                       else f"{world} independent datasets (one per GPU)"),
+                       "l2": f"256 MB buffer written between timed steps (L2 flush); distance matrix "
+                             f"{mat_gb:.1f} GB"},
             "dbscan_sec": round(ms_per_step * 1e-3, 4),
             "rerun_pairs": int(st1["reruns"]),
-            "rerun_fraction": st1["reruns"] / max(len(seqs) * (len(seqs) - 1) // 2, 1),
+            "rerun_fraction": st1["reruns"] / max(n * (n - 1) // 2, 1),
             "score_pass_ms": round(statistics.median(score_ms), 2),
-            "sweep_ms": round(sweep_s * 1e3, 2),
-            "roofline": {"bound": "int", "kernel": "fast_all_pairs_kernel", "achieved": round(fast_gcups, 1),
-                         "peak": round(roof_peak, 1), "unit": "Gcell/s", "frac": round(fast_gcups / roof_peak, 4),
-                         "peak_source": "measured on this GPU: issue rate of the kernel's per-cell 16x2 "
-                                        "instruction mix on independent chains, R = 2*P_int/4.5",
-                         "peak_k4": round(roof_peak * 4.5 / 4.0, 1),
-                         "frac_k4": round(fast_gcups / (roof_peak * 4.5 / 4.0), 4),
-                         "k4_note": "R = 2*P_int/4: the recurrence's minimum of 4 packed instructions per "
-                                    "cell pair",
-                         "traffic": traffic},
+            ("sweep_ms" if wl["mode"] == "adaptive" else "dbscan_ms"): round(sweep_s * 1e3, 2),
+            "roofline": roof,
             "threshold_roofline": {"bound": "hbm", "kernel": "threshold_bulk_kernel", "achieved": round(
                 thr_bytes / (thr_ms * 1e-3) / 1e9, 1), "peak": hbm_peak[0], "unit": "GB/s",
                 "frac": round(thr_bytes / (thr_ms * 1e-3) / 1e9 / hbm_peak[0], 4), "peak_source": hbm_peak[1],
                 "bytes_per_launch": thr_bytes, "ms_per_launch": round(thr_ms, 4)},
-            "cpu_baseline": cpu,
+            "cpu_baseline": cpu_line,
             "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "reps": len(e2e_ms),
+                    "note": "upload from host buffers + score pass + clustering + results on the host, "
+                            "wall clock per repetition"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "prefilter_speedup": None,
+            "tile_plan": _plan(tune),
         }
-        if world == 1 and wl["gen"] == "config2" and not args.no_kmer:
+        if exch:
+            line["split_exchange"] = dict(exch[-1], matrix_bytes=int(eng.distance_bytes()))
+        if world == 1 and kmer_legs:
             cpu_leg = not args.no_cpu_baseline
             line["fasta2kmer"] = side_leg(fasta2kmer_leg, seqs, cpu=cpu_leg)
             line["kmer_dbscan"] = side_leg(kmer_dbscan_leg, eng, seqs, dev, cpu=cpu_leg)
             line["kmer2pca"] = side_leg(kmer2pca_leg, eng, seqs, dev, cpu=cpu_leg)
-        print(json.dumps(line), flush=True)
     eng.close()
-    del flush
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return line
+
+
+def _plan(tune):
+    """The autotuner's choice as reported in the line (None: default plan)."""
+    if not tune:
+        return None
+    return {"packs_per_block": tune["packs_per_block"], "threads": tune["threads"], "max_w": tune["max_w"],
+            "from_cache": bool(tune["from_cache"]), "candidates": tune["candidates"],
+            "sample_sequences": tune["sample"], "sample_ms_default": round(tune["ms_default"], 3),
+            "sample_ms_best": round(tune["ms_best"], 3), "key": tune["key"],
+            "note": "16x2 kernel tile plan timed on a length-stratified sample (untimed, before the warm-up); "
+                    "default plan: 32 packs, 256 threads, max_w 24"}
+
+
+# keys of a side leg's line that repeat the main line's
+_LEG_DROP = ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data", "prefilter_speedup")
+
+
+def as_leg(line):
+    if not isinstance(line, dict):
+        return line
+    return {k: v for k, v in line.items() if k not in _LEG_DROP}
+
+
+def run_gpu(args):
+    run = Run()
+    line = measure_single(run, args.config, args, args.steps, args.warmup,
+                          e2e_reps=min(max(args.steps, 1), args.e2e_reps), cpu=not args.no_cpu_baseline,
+                          kmer_legs=(args.config == "2" and not args.no_kmer and not args.n))
+    # the other workloads as side legs of the default line (one GPU; rank 0 alone,
+    # so no rank waits in a collective meanwhile)
+    if run.world == 1 and args.config == "3" and not args.no_legs and not args.n and line is not None:
+        ls, lw = args.leg_steps, args.leg_warmup
+        line["sweep_config2"] = side_leg(lambda: as_leg(measure_single(run, "2", args, ls, lw, e2e_reps=1,
+                                                                       cpu=False)))
+        line["config5"] = side_leg(lambda: as_leg(measure_multi(run, "5", args, ls, lw, e2e_reps=1)))
+        c4 = side_leg(lambda: as_leg(measure_prefilter(run, "4", args, ls, lw, e2e_reps=1)))
+        line["config4"] = c4
+        if isinstance(c4, dict) and "value" in c4:
+            line["prefilter_speedup"] = c4["value"]
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    run.close()
     return 0
 
 
@@ -699,39 +800,24 @@ def _pct(xs, q):
     return round(xs[k], 2)
 
 
-def run_gpu_multi(args):
+def measure_multi(run: Run, config: str, args, steps: int, warmup: int, e2e_reps: int):
     """Many independent split sets: one score pass over every set, then all
     sets' sweeps advanced together (one threshold launch per round), against
-    the same sets run one by one through the same engine."""
-    import torch
-
+    the same sets run one by one through the same engine.  Returns the line
+    (rank 0) or None."""
     import swgpu
     from swgpu import workloads as W
 
-    rank, local, world = env_rank()
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = local
-    torch.cuda.set_device(dev)
-    wl = WORKLOADS[args.config]
-    sets, _ = W.config5(seed=dataset_seed(args.config, rank))
+    rank, world, dev = run.rank, run.world, run.dev
+    wl = WORKLOADS[config]
+    sets, _ = W.config5(seed=dataset_seed(config, rank))
     if args.n:
         sets = sets[:args.n]
     cells = sum(W.cells(st) for st in sets)
     nseq = sum(len(st) for st in sets)
     eng = swgpu.Engine(device=dev)
+    tune = None if args.no_autotune else eng.autotune([q for st in sets for q in st])
     eng.upload_sets(sets)
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
 
     def sweeps():
         # layer counts only: the split sets stay in the library (freed there)
@@ -745,46 +831,42 @@ def run_gpu_multi(args):
         res = sweeps()
         return eng.timer_stop(), score_ms, res
 
-    for _ in range(args.warmup):
-        flush.fill_(1)
-        torch.cuda.synchronize(dev)
+    for _ in range(warmup):
+        run.flush_l2()
         step()
     st0 = eng.stats()
-    barrier()
+    run.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
     step_ms, score_ms, kernel_ms, lat = [], [], [], []
     res = None
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize(dev)
+    for _ in range(steps):
+        run.flush_l2()
         ms, sms, res = step()
         step_ms.append(ms)
         score_ms.append(sms)
         kernel_ms.append(eng.stats()["ms_fast_kernel"])
         lat = [sms + r["done_ms"] for r in res]
-    barrier()
+    run.barrier()
     clk = clocks.stop()
     st1 = eng.stats()
-    total_ms = sum(step_ms)
-    total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
-    ms_per_step = total_ms / args.steps
+    total_ms = run.max(sum(step_ms))
+    ms_per_step = total_ms / steps
     value = cells * world / (ms_per_step * 1e-3) / 1e9
-    launches = (st1["kernel_launches"] - st0["kernel_launches"]) // args.steps
+    launches = (st1["kernel_launches"] - st0["kernel_launches"]) // steps
     bad = [k for k, r in enumerate(res) if r["status"] != 0]
 
     # e2e: host sequences in, every set's layers back on the host
     e2e_ms = []
-    for _ in range(max(1, args.steps)):
-        barrier()
+    for _ in range(max(1, e2e_reps)):
+        run.barrier()
         t0 = time.perf_counter()
         eng.upload_sets(sets)
         eng.score_all_pairs()
         sweeps()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     b1 = eng.stats()
-    e2e_total = sum(e2e_ms)
-    e2e_total = max_over_ranks(e2e_total, dist, f"cuda:{dev}")
+    e2e_total = run.max(sum(e2e_ms))
     e2e_value = cells * world / (e2e_total / len(e2e_ms) * 1e-3) / 1e9
 
     # the same sets one by one (upload, score pass, sweep per set), rank 0 only
@@ -812,14 +894,12 @@ def run_gpu_multi(args):
                "set_ms": {"p50": _pct(per, 50), "p90": _pct(per, 90), "p99": _pct(per, 99)},
                "latency_ms": {"p50": _pct(done, 50), "p90": _pct(done, 90), "p99": _pct(done, 99)}}
 
+    line = None
     if rank == 0:
         kms = statistics.median(kernel_ms)
-        fast_gcups = st1["cells"] / (kms * 1e-3) / 1e9
-        _, peak_instr = swgpu.measure_mix_peak(dev)
-        roof_peak = 2.0 * peak_instr / 4.5 / 1e9
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 2), "higher_is_better": True,
+            "metric": METRIC, "value": round(value, 2), "unit": "GCUPS", "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": round(ms_per_step, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "s16x2", "data": "synthetic",
             "config": {"workload": wl["text"], "n_sets": len(sets), "n_sequences": nseq, "cells_per_gpu": cells,
                        "parallelism": f"{world} independent set collections (one per GPU)",
@@ -833,58 +913,47 @@ def run_gpu_multi(args):
                 "failed_sets": bad[:10], "truncated_sets": sum(r["truncated"] for r in res),
                 "one_by_one": one,
                 "speedup_vs_one_by_one": round(one["total_s"] / (ms_per_step * 1e-3), 2) if one else None},
-            "roofline": {"bound": "int", "kernel": "fast_all_pairs_kernel", "achieved": round(fast_gcups, 1),
-                         "peak": round(roof_peak, 1), "unit": "Gcell/s", "frac": round(fast_gcups / roof_peak, 4),
-                         "peak_source": "measured on this GPU: issue rate of the kernel's per-cell 16x2 "
-                                        "instruction mix on independent chains, R = 2*P_int/4.5",
-                         "peak_k4": round(roof_peak * 4.5 / 4.0, 1),
-                         "frac_k4": round(fast_gcups / (roof_peak * 4.5 / 4.0), 4),
-                         "k4_note": "R = 2*P_int/4: the recurrence's minimum of 4 packed instructions per "
-                                    "cell pair",
-                         "traffic": None},
+            "roofline": fast_roofline(st1["cells"], kms, dev),
             "cpu_baseline": None,
             "e2e": {"value": round(e2e_value, 2), "unit": "GCUPS", "h2d_bytes_per_step": int(b1["h2d_bytes"]),
-                    "d2h_bytes_per_step": int(b1["d2h_bytes"])},
+                    "d2h_bytes_per_step": int(b1["d2h_bytes"]), "reps": len(e2e_ms)},
             "gpu_launches": int(launches),
             "clocks": clk,
             "prefilter_speedup": None,
+            "tile_plan": _plan(tune),
         }
-        print(json.dumps(line), flush=True)
     eng.close()
-    del flush
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return line
+
+
+def run_gpu_multi(args):
+    run = Run()
+    line = measure_multi(run, args.config, args, args.steps, args.warmup,
+                         e2e_reps=min(max(args.steps, 1), args.e2e_reps))
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    run.close()
     return 0
 
 
-def run_gpu_prefilter(args):
+def measure_prefilter(run: Run, config: str, args, steps: int, warmup: int, e2e_reps: int):
     """Learned prefilter (config 4): train on exact-scored pairs of other
     datasets of the distribution, calibrate on a held-out one, then time the
     prefiltered pass + DBSCAN against the exact pass + DBSCAN on the same GPU
-    and report eps-neighbour recall and adjusted Rand of the clusters."""
+    and report eps-neighbour recall and adjusted Rand of the clusters.
+    Returns the line (rank 0) or None."""
     import numpy as np
-    import torch
 
     import swgpu
     from swgpu import prefilter as PF
     from swgpu import workloads as W
 
-    rank, local, world = env_rank()
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = local
-    torch.cuda.set_device(dev)
-    wl = WORKLOADS[args.config]
+    rank, world, dev = run.rank, run.world, run.dev
+    wl = WORKLOADS[config]
     t0 = time.perf_counter()
     train_sets = [W.config2(seed=1000 + k, n=6000, n_fam=60)[0] for k in range(60)]
     cal_seqs, _ = W.config2(seed=101)
-    test, _ = W.config2(seed=dataset_seed(args.config, rank))
+    test, _ = W.config2(seed=dataset_seed(config, rank))
     if args.n:
         test = test[:args.n]
     gen_s = time.perf_counter() - t0
@@ -892,29 +961,21 @@ def run_gpu_prefilter(args):
     eps_list = wl["eps_list"]
     trep = PF.train(eng, train_sets, max(eps_list), seed=0, weight_decay=args.weight_decay)
     cal = {eps: PF.calibrate(eng, cal_seqs, eps, seed=0) for eps in eps_list}
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
     n = len(test)
     cells = W.cells(test)
 
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
     def timed(fn, steps, warmup):
         for _ in range(warmup):
-            flush.fill_(1)
-            torch.cuda.synchronize(dev)
+            run.flush_l2()
             fn()
         out, ms = None, []
-        barrier()
+        run.barrier()
         for _ in range(steps):
-            flush.fill_(1)
-            torch.cuda.synchronize(dev)
+            run.flush_l2()
             eng.timer_start()
             out = fn()
             ms.append(eng.timer_stop())
-        barrier()
+        run.barrier()
         return out, statistics.median(ms)
 
     eng.upload(test)
@@ -933,12 +994,12 @@ def run_gpu_prefilter(args):
             st = eng.score_prefiltered(eps, margins)
             return eng.dbscan(eps, wl["minpts"]), st
 
-        lab_ex, ms_ex = timed(exact_step, args.steps, args.warmup)
+        lab_ex, ms_ex = timed(exact_step, steps, warmup)
         rp, _ = eng.neighbors(eps)
         exact_nbrs = int(rp[-1]) - n
         s0 = eng.stats()["kernel_launches"]
-        (lab_pf, st), ms_pf = timed(pf_step, args.steps, args.warmup)
-        launches_pf = (eng.stats()["kernel_launches"] - s0) // max(args.steps + args.warmup, 1)
+        (lab_pf, st), ms_pf = timed(pf_step, steps, warmup)
+        launches_pf = (eng.stats()["kernel_launches"] - s0) // max(steps + warmup, 1)
         rp, _ = eng.neighbors(eps)
         recall = (int(rp[-1]) - n) / exact_nbrs if exact_nbrs else 1.0
         ari = PF.adjusted_rand(PF.labels_from_split(lab_ex, n), PF.labels_from_split(lab_pf, n))
@@ -958,8 +1019,8 @@ def run_gpu_prefilter(args):
     margins0 = cal[eps_list[0]][0]
     e2e_ms = []
     b0 = eng.stats()
-    for _ in range(max(1, args.steps)):
-        barrier()
+    for _ in range(max(1, e2e_reps)):
+        run.barrier()
         t1 = time.perf_counter()
         eng.upload(test)
         eng.score_prefiltered(eps_list[0], margins0)
@@ -997,11 +1058,12 @@ def run_gpu_prefilter(args):
                 "fallback_full": int(st2["fallback_full"]), "scale": r2.get("scale"),
                 "margins": [[u, round(m, 5)] for u, m in m2]}
 
+    line = None
     if rank == 0:
         sp = per_eps[head]["speedup"]
         line = {
             "metric": METRIC, "value": sp, "unit": "x (prefiltered vs exact step, same GPU)", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_eps[head]["ms_prefilter_step"],
+            "steps": steps, "warmup": warmup, "ms_per_step": per_eps[head]["ms_prefilter_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "s16x2 + bf16",
             "data": "synthetic",
             "config": {"workload": wl["text"], "n_sequences": n, "cells_per_gpu": cells, "eps": eps_list,
@@ -1017,17 +1079,23 @@ def run_gpu_prefilter(args):
             "ablation_without_network": ablation,
             "e2e": {"value": round(per_eps[head]["ms_exact_step"] / statistics.median(e2e_ms), 3),
                     "unit": "x (exact device step / prefiltered host-to-host step)",
-                    "h2d_bytes_per_step": int(b1["h2d_bytes"]), "d2h_bytes_per_step": int(b1["d2h_bytes"])},
+                    "h2d_bytes_per_step": int(b1["h2d_bytes"]), "d2h_bytes_per_step": int(b1["d2h_bytes"]),
+                    "reps": len(e2e_ms)},
             "gpu_launches": int(launches_pf) if launches_pf is not None else None,
             "clocks": clk,
             "prefilter_speedup": sp,
         }
-        print(json.dumps(line), flush=True)
     eng.close()
-    del flush
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return line
+
+
+def run_gpu_prefilter(args):
+    run = Run()
+    line = measure_prefilter(run, args.config, args, args.steps, args.warmup,
+                             e2e_reps=min(max(args.steps, 1), args.e2e_reps))
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    run.close()
     return 0
 
 
@@ -1039,18 +1107,25 @@ def main():
     ap.add_argument("--impl", default="swgpu", choices=["swgpu", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", default="2", choices=sorted(WORKLOADS))
+    ap.add_argument("--config", default="3", choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=0, help="profile a smaller case: the first n reads of the workload "
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
     ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
     ap.add_argument("--split", action="store_true",
-                    help="config 2/3: one data set split over all ranks (strong scaling: tile groups and one "
-                         "all-reduce of the matrix) instead of one data set per rank")
+                    help="config 2/3: one data set split over all ranks (strong scaling: tile groups, then an "
+                         "all-gather of each rank's tile rectangles) instead of one data set per rank")
     ap.add_argument("--no-kmer", action="store_true", help="config 2: skip the fasta2kmer, k-mer DBSCAN and kmer2pca legs")
     ap.add_argument("--leg", choices=["fasta2kmer", "kmer_dbscan", "kmer2pca"],
                     help="run one side leg alone on the config-2 reads (the first --n) and print its object")
     ap.add_argument("--weight-decay", type=float, default=0.0, help="config 4: decoupled weight decay of Adam")
+    ap.add_argument("--e2e-reps", type=int, default=2,
+                    help="host-to-host repetitions of the step for `e2e` (at most --steps)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="config 3: skip the side legs (config-2 sweep, config 5, config 4)")
+    ap.add_argument("--leg-steps", type=int, default=3, help="timed steps of each side leg")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tile plan of the 16x2 kernel")
+    ap.add_argument("--leg-warmup", type=int, default=3, help="warm-up steps of each side leg")
     args = ap.parse_args()
     if args.leg:
         return run_leg(args)

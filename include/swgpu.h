@@ -49,11 +49,19 @@ typedef struct {
                           copy that is never issued, so its bounded wait runs
                           out and the pass returns SWE_ERR_TIMEOUT */
   int threshold_path;  /* test hook for the eps threshold pass: 0 = automatic
-                          (bulk-copied rows, double-buffered), 1 = rows read
-                          from global memory, 2 = positions staged in shared
-                          memory too, 3 = one bulk-copy row buffer */
+                          (transposed two-pass: H-bit words of H sorted rows,
+                          then a gather of those words into original order;
+                          path 4 for sets too large for it), 1 = rows read
+                          from global memory, 2 = bulk-copied rows with the
+                          positions staged in shared memory too, 3 = one
+                          bulk-copy row buffer, 4 = bulk-copied rows,
+                          double-buffered, 5 / 6 = the transposed pass with
+                          blocks of at most 16 / 8 rows */
   int kmer_batch_kb;   /* test hook: device batch of the k-mer calls in KB
                           (0 = 1 GB of counts and 256 MB of text) */
+  int max_w;           /* lane split of the 16x2 kernel: each column sequence
+                          gets the fewest of 8, 16 or 32 lanes that hold at
+                          most max_w columns each (0 = 24, the largest) */
 } swe_opts;
 
 typedef struct {
@@ -138,6 +146,25 @@ swe_status swe_distance_copy(swe_ctx* ctx, void* dev_buf, int to_engine);
 /* The assignment swe_set_partition uses: owner[t] for costs cost[0..n) given
    in descending order. */
 void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
+/* The exchange of a split pass sized to the result (the counterpart of the
+   reference's gather of distance stripes to its master, dbscan.c:374-379,
+   457-458): a group's payload is the distance rectangles of its own tiles,
+   tile after tile in cost order, each row-major, one stored distance
+   (swe_distance_bytes / matrix entries: 2 or 4 bytes) per pair; every
+   process can compute every group's payload size from the shared layout.
+   swe_partition_bytes   bytes of group `part`'s payload (-1: no such group)
+   swe_partition_pack    this context's own payload into dev_buf (after its
+                         partitioned score pass)
+   swe_partition_unpack  bytes [offset, offset + bytes) of group `part`'s
+                         payload, received from its process, written into
+                         both triangles of this context's matrix
+   After every other group's payload is unpacked the matrix equals a whole
+   pass (the pairs of the 32-bit path are scored by every group).  Both calls
+   wait for the context's stream.  bench.py --split and swgpu/split_pass.py
+   exchange payloads in chunks with all-gathers, sizes checked first. */
+int64_t swe_partition_bytes(const swe_ctx* ctx, int part);
+swe_status swe_partition_pack(swe_ctx* ctx, void* dev_buf);
+swe_status swe_partition_unpack(swe_ctx* ctx, int part, const void* dev_buf, int64_t offset, int64_t bytes);
 
 /* Scores every pair of the uploaded sequences into the device distance matrix
    (one pass; later neighbour/DBSCAN calls reuse it). */
@@ -252,34 +279,77 @@ swe_status swe_measure_mix_peak(int device, double* cells_per_s, double* lane_in
 swe_status swe_timer_start(swe_ctx* ctx);
 swe_status swe_timer_stop(swe_ctx* ctx, double* ms);
 
+/* Tile-plan autotuner.  No counterpart in the reference, whose OpenCL launch
+   leaves the work-group size to the driver (dbscan.c:497-501, local size
+   NULL) and whose kernel has no tiles.
+
+   The 16x2 kernel's plan is three knobs: row packs (two sequences each) per
+   tile, threads per CTA, and the lane split (a column sequence gets the
+   fewest of 8, 16 or 32 lanes that hold at most max_w columns each).  Every
+   plan computes the same distances; their speed depends on the device and on
+   the length distribution.  swe_autotune takes a length-stratified sample of
+   up to 4,096 of the given sequences, scores it on a scratch context of the
+   same device with each candidate plan (packs 16 / 32 / 64, threads 128 /
+   256, max_w 16 / 20 / 24), checks that every plan's matrix equals the
+   default plan's, and keeps the fastest unless it is within 2 % of the
+   default, which is then kept.  The plan is
+   set on ctx: it applies to the next upload, and an upload ctx already holds
+   is laid out again (its distances must be scored again).
+
+   cache_path   NULL, or a text file of "key packs threads max_w" lines: a
+                line with this key is used without timing anything
+                (SWE_TUNE_FORCE times anyway); a newly timed plan is appended
+   key          device name, SM count, the sample size class and the length
+                histogram (sixteen 64-symbol bins, in twentieths) */
+#define SWE_TUNE_FORCE 1
+typedef struct {
+  int packs_per_block, threads, max_w;  /* the chosen plan */
+  int from_cache;                       /* 1: read from cache_path, nothing timed */
+  int candidates;                       /* plans timed */
+  int sample;                           /* sequences in the timing sample */
+  double sample_cells;                  /* DP cells of one pass over the sample */
+  double ms_default;                    /* 16x2 kernel time of the default plan (32, 256, 24) */
+  double ms_best;                       /* 16x2 kernel time of the chosen plan */
+  char key[160];
+} swe_tune_result;
+swe_status swe_autotune(swe_ctx* ctx, const char* const* seqs, const size_t* lens, int n, const char* cache_path,
+                        int flags, swe_tune_result* out);
+
 /* Allocation-free scoring of explicit pairs.  No counterpart in the reference
    (which has no device API at all).
 
-   For callers that cannot allocate device memory: code running while a CUDA
-   graph is being captured, real-time or embedded hosts that must not call the
-   device allocator after start-up, and programs whose device memory belongs to
-   a pool this library cannot see.  The caller passes device buffers it already
-   owns; this call calls no cudaMalloc, cudaFree or other allocating routine.
+   For callers that cannot allocate device memory: real-time or embedded hosts
+   that must not call the device allocator once they have started, and programs
+   whose device memory is all owned by their own pooling allocator, which this
+   library can neither see nor grow.  The caller passes device buffers it
+   already owns; this call calls no cudaMalloc, cudaFree or other allocating
+   routine.
 
    seqs         device bytes; sequence i is the C string at seqs + off[i] of
                 length len[i] (readable at [0 .. len[i]], scored like score())
    off, len     device arrays indexed by sequence
    pairs        device int array of 2*npairs indices (a, b)
-   out          device array of npairs distances (0xFFFFFFFF for a pair whose
-                sequence is longer than max_len)
+   out          device array of npairs distances
    max_len      upper bound on every len[i] the pairs reference,
                 at most SWE_NOALLOC_MAX_LEN (larger values: SWE_ERR_INVALID)
-   stream       cudaStream_t to enqueue on (NULL: the default stream)
+   stream       cudaStream_t to run on (NULL: the default stream)
 
-   The work is only enqueued; synchronise the stream before reading `out`.
+   The call waits for `stream` and returns when `out` holds the distances.  A
+   pair that references a sequence longer than max_len is not scored: its
+   distance reads 0xFFFFFFFF and the call returns SWE_ERR_INVALID (every other
+   pair is still scored).  An error that earlier work of the caller left
+   pending in the CUDA runtime is returned as SWE_ERR_CUDA before anything
+   runs, and stays pending for the caller.
+
    Long sequences need scratch, which is one fixed 4 MiB device array per GPU
    (kept until the process exits), so a call runs at most 2^20/(max_len+1)
    warps.  Every call on a device shares that array and it keeps the last
-   call's contents (each call writes every word before reading it): calls that
-   overlap on the GPU - on different streams or threads - race and must be
-   serialised by the caller.  The first call on a device looks up the array's
-   device address with that device current; make that first call before any
-   stream capture. */
+   call's contents (each call writes every word before reading it, and clears
+   its counter of over-length pairs): calls that overlap on the GPU - on
+   different streams or threads - race and must be serialised by the caller.
+   The first call on a device looks up the array's device address with that
+   device current and keeps it; make that first call before any stream
+   capture, and do not call it again after a cudaDeviceReset of the device. */
 #define SWE_NOALLOC_MAX_LEN 65535
 swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* off, const int* len, const int* pairs,
                                    int64_t npairs, unsigned* out, int max_len, void* stream);

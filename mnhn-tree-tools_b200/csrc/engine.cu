@@ -138,8 +138,9 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
     ctx->threads = opts->threads;
   }
   if (opts && opts->inject_timeout) ctx->inject_timeout = 1;
-  if (opts && opts->threshold_path >= 0 && opts->threshold_path <= 3) ctx->threshold_path = opts->threshold_path;
+  if (opts && opts->threshold_path >= 0 && opts->threshold_path <= 6) ctx->threshold_path = opts->threshold_path;
   if (opts && opts->kmer_batch_kb > 0) ctx->kmer_batch_bytes = (size_t)opts->kmer_batch_kb << 10;
+  if (opts && opts->max_w > 0) ctx->max_w = std::min(opts->max_w, FAST_MAX_W);
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
   for (auto& ev : ctx->ev)
@@ -208,6 +209,81 @@ static DistLayout layout(const swe_ctx* ctx) {
   L.D16 = ctx->d_D16.p;
   L.D32 = ctx->d_D32.p;
   return L;
+}
+
+// ---------------------------------------------------------------------------
+// The split pass's exchange: tile rectangles of one group
+// ---------------------------------------------------------------------------
+static void part_tiles(const swe_ctx* ctx, int part, std::vector<TileRect>* rects, std::vector<long long>* pre) {
+  rects->clear();
+  pre->assign(1, 0);
+  for (size_t t = 0; t < ctx->part_rects.size(); ++t)
+    if (ctx->part_owner[t] == part) {
+      const TileRect& R = ctx->part_rects[t];
+      rects->push_back(R);
+      pre->push_back(pre->back() + (long long)R.nra * R.nb);
+    }
+}
+
+extern "C" int64_t swe_partition_bytes(const swe_ctx* ctx, int part) {
+  if (!ctx || part < 0 || part >= ctx->nparts || ctx->metric != 0) return -1;
+  long long entries = 0;
+  for (size_t t = 0; t < ctx->part_rects.size(); ++t)
+    if (ctx->part_owner[t] == part) entries += (long long)ctx->part_rects[t].nra * ctx->part_rects[t].nb;
+  return entries * ctx->dist_bytes;
+}
+
+static swe_status part_upload(swe_ctx* ctx, int part, long long* entries, int* ntiles) {
+  std::vector<TileRect> rects;
+  std::vector<long long> pre;
+  part_tiles(ctx, part, &rects, &pre);
+  CK(ctx->d_part_rects.alloc(std::max<size_t>(rects.size(), 1)));
+  CK(ctx->d_part_pre.alloc(pre.size()));
+  if (!rects.empty())
+    CK(cpy(ctx, ctx->d_part_rects.p, rects.data(), sizeof(TileRect) * rects.size(), cudaMemcpyHostToDevice,
+           ctx->st));
+  CK(cpy(ctx, ctx->d_part_pre.p, pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice, ctx->st));
+  *entries = pre.back();
+  *ntiles = (int)rects.size();
+  return SWE_OK;
+}
+
+extern "C" swe_status swe_partition_pack(swe_ctx* ctx, void* dev_buf) {
+  if (!ctx) return SWE_ERR_INVALID;
+  if (swe_status s = need_sequences(ctx)) return s;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  if (swe_status s = select_device(ctx)) return s;
+  long long entries = 0;
+  int ntiles = 0;
+  if (swe_status s = part_upload(ctx, ctx->part, &entries, &ntiles)) return s;
+  if (entries > 0 && !dev_buf) return SWE_ERR_INVALID;
+  ctx->stats.kernel_launches += ntiles > 0;
+  CK(launch_tile_pack(layout(ctx), ctx->d_part_rects.p, ctx->d_part_pre.p, ntiles, dev_buf, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return SWE_OK;
+}
+
+extern "C" swe_status swe_partition_unpack(swe_ctx* ctx, int part, const void* dev_buf, int64_t offset,
+                                           int64_t bytes) {
+  if (!ctx || part < 0 || part >= ctx->nparts || offset < 0 || bytes < 0) return SWE_ERR_INVALID;
+  if (swe_status s = need_sequences(ctx)) return s;
+  if (!ctx->scored) return fail(ctx, SWE_ERR_STATE, "no scored dataset");
+  const int db = ctx->dist_bytes;
+  if (offset % db || bytes % db) return fail(ctx, SWE_ERR_INVALID, "offset and size must be whole distances");
+  if (offset + bytes > swe_partition_bytes(ctx, part)) return fail(ctx, SWE_ERR_INVALID, "beyond the group's blocks");
+  if (bytes == 0) return SWE_OK;
+  if (!dev_buf) return SWE_ERR_INVALID;
+  if (swe_status s = select_device(ctx)) return s;
+  long long entries = 0;
+  int ntiles = 0;
+  if (swe_status s = part_upload(ctx, part, &entries, &ntiles)) return s;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_tile_unpack(layout(ctx), ctx->d_part_rects.p, ctx->d_part_pre.p, ntiles, dev_buf, offset / db,
+                        (offset + bytes) / db, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->bits_T = LLONG_MIN;  // cached neighbour bitmaps no longer match
+  ctx->bits_set = -1;
+  return SWE_OK;
 }
 
 // Sorted order, packs, row blocks, tiles and every device array that depends
@@ -306,6 +382,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
   const int cta_warps = ctx->threads / 32;
   ctx->tiles.clear();
   std::vector<double> cost;
+  std::vector<swgpu::TileRect> rects;  // each tile's rectangle of the sorted matrix (the split pass's exchange)
   double tile_cells = 0;
   long long tiles_all = 0;
   for (int q0 = 0, k = 0; k < n_sets; ++k) {
@@ -323,7 +400,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
         nb = std::min(nf - b0, cta_warps * (32 / lpb));
         L = 0;
         for (int x = b0; x < b0 + nb; ++x) L = std::max(L, ctx->len[ctx->order[f + x]]);
-        const int need = L <= 8 * FAST_MAX_W ? 8 : (L <= 16 * FAST_MAX_W ? 16 : 32);
+        const int need = L <= 8 * ctx->max_w ? 8 : (L <= 16 * ctx->max_w ? 16 : 32);
         if (need <= lpb) break;
         lpb = need;
       }
@@ -366,6 +443,9 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
           ++tiles_all;
           if (cand && !mark[c * (q1 - q0) + (q - q0)]) continue;
           ctx->tiles.push_back(FastTile{f + cb.b0, cb.nb, q, cb.W | (cb.lpb << 8), k});
+          const int pkl = block_first[q] + block_npacks[q] - 1;
+          rects.push_back(swgpu::TileRect{pack_first[block_first[q]],
+                                          2 * block_npacks[q] - (pack_pair[pkl] ? 0 : 1), f + cb.b0, cb.nb, k});
           const double cc = (double)cb.nb * cb.lpb * cb.W * block_rows[q];
           cost.push_back(cc);
           tile_cells += 2.0 * cc;
@@ -381,15 +461,19 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     std::vector<FastTile> sorted(ctx->tiles.size());
     std::vector<double> sorted_cost(ctx->tiles.size());
-    for (size_t k = 0; k < idx.size(); ++k) sorted[k] = ctx->tiles[idx[k]], sorted_cost[k] = cost[idx[k]];
+    ctx->part_rects.resize(ctx->tiles.size());
+    for (size_t k = 0; k < idx.size(); ++k) {
+      sorted[k] = ctx->tiles[idx[k]], sorted_cost[k] = cost[idx[k]];
+      ctx->part_rects[k] = rects[idx[k]];
+    }
     ctx->tiles.swap(sorted);
+    ctx->part_owner.assign(ctx->tiles.size(), 0);
     if (ctx->nparts > 1) {  // this process's share of the tiles
-      std::vector<int> owner(ctx->tiles.size());
-      lpt_partition(sorted_cost.data(), (int64_t)sorted_cost.size(), ctx->nparts, owner.data());
+      lpt_partition(sorted_cost.data(), (int64_t)sorted_cost.size(), ctx->nparts, ctx->part_owner.data());
       std::vector<FastTile> mine;
       tile_cells = 0;
       for (size_t k = 0; k < ctx->tiles.size(); ++k)
-        if (owner[k] == ctx->part) mine.push_back(ctx->tiles[k]), tile_cells += 2.0 * sorted_cost[k];
+        if (ctx->part_owner[k] == ctx->part) mine.push_back(ctx->tiles[k]), tile_cells += 2.0 * sorted_cost[k];
       ctx->tiles.swap(mine);
     }
   }
@@ -848,9 +932,43 @@ static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& group
     CK(cudaMemsetAsync(ctx->d_thr_status.p, 0, sizeof(unsigned), ctx->st));
     p.status = ctx->d_thr_status.p;
     p.wait_limit = 1u << 22;
+    p.order = ctx->d_order.p;
+    int H = ctx->threshold_path == 0 ? transposed_height(maxn) : 0;
+    if (ctx->threshold_path == 5 || ctx->threshold_path == 6) {  // test hooks: smaller blocks than automatic
+      H = std::min(transposed_height(maxn), ctx->threshold_path == 5 ? 16 : 8);
+      if (H < 8) H = 0;
+    }
+    if (H > 0) {  // transposed two-pass threshold: scratch of H-bit words, item prefix sums
+      std::vector<ThrGroup> tg(groups);
+      std::vector<long long> pre1(groups.size() + 1, 0), pre2(groups.size() + 1, 0);
+      long long tb = 0;
+      for (size_t g = 0; g < tg.size(); ++g) {
+        ThrGroup& G = tg[g];
+        G.nblk = (G.n_s + H - 1) / H;
+        G.blk_stride = transposed_block_stride(G.n_s, H);
+        G.tb_base = tb;
+        tb += (long long)G.nthr * G.nblk * G.blk_stride;
+        pre1[g + 1] = pre1[g] + (long long)G.nblk * ((G.n_s + 255) / 256);
+        pre2[g + 1] = pre2[g] + (long long)G.nthr * G.nblk;
+      }
+      CK(ctx->d_tbits.alloc((size_t)std::max<long long>(tb, 16)));
+      CK(ctx->d_tpre.alloc(2 * pre1.size()));
+      CK(cpy(ctx, ctx->d_groups.p, tg.data(), sizeof(ThrGroup) * tg.size(), cudaMemcpyHostToDevice, ctx->st));
+      CK(cpy(ctx, ctx->d_tpre.p, pre1.data(), sizeof(long long) * pre1.size(), cudaMemcpyHostToDevice, ctx->st));
+      CK(cpy(ctx, ctx->d_tpre.p + pre1.size(), pre2.data(), sizeof(long long) * pre2.size(), cudaMemcpyHostToDevice,
+             ctx->st));
+      p.tbits = ctx->d_tbits.p;
+      CK(cudaEventRecord(ctx->ev[2], ctx->st));
+      ctx->stats.kernel_launches += 2;
+      CK(launch_threshold_transposed(p, H, maxn, ctx->d_tpre.p, pre1.back(), ctx->d_tpre.p + pre1.size(),
+                                     pre2.back(), ctx->st));
+      CK(cudaEventRecord(ctx->ev[3], ctx->st));
+      CK(cpy(ctx, ctx->h_thr_status.p, ctx->d_thr_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+      return SWE_OK;
+    }
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     ctx->stats.kernel_launches += 1;
-    ThrPlan plan = threshold_plan(maxn, ctx->dist_bytes);
+    ThrPlan plan = threshold_plan(maxn, ctx->dist_bytes);  // path 4 (and sets too large for path 0)
     if (ctx->threshold_path == 1) {
       plan.staged = 0, plan.nbuf = 0, plan.stage_pos = 0, plan.block = 256, plan.smem = 0;
     } else if (ctx->threshold_path == 2 && plan.staged) {

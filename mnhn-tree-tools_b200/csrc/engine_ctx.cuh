@@ -81,6 +81,7 @@ struct swe_ctx {
   int pf_packs_per_block = 8;   // the same for candidate-tile layouts (sparser work, finer tiles)
   int layout_pb = 32;           // the value the current layout was built with
   int threads = 256;
+  int max_w = swgpu::FAST_MAX_W;  // lane-split rule: a column sequence gets the fewest lanes holding <= max_w columns each
   int inject_timeout = 0;
   int part = 0, nparts = 1;     // this context scores tile group `part` of `nparts` (swe_set_partition)
   int threshold_path = 0;
@@ -112,6 +113,8 @@ struct swe_ctx {
   size_t smem = 0;
   int fast_grid = 0;
   std::vector<swgpu::FastTile> tiles;
+  std::vector<swgpu::TileRect> part_rects;  // every tile of the layout (all groups), in cost order
+  std::vector<int> part_owner;              // its group under swe_set_partition
   long long tiles_all = 0;  // tiles of the full layout (before a candidate mask)
   bool masked = false;      // only candidate tiles are scored; other pairs read as the largest value
 
@@ -165,6 +168,10 @@ struct swe_ctx {
   swgpu::DevBuf<swgpu::ThrGroup> d_groups;
   swgpu::DevBuf<long long> d_rowpre;
   swgpu::DevBuf<unsigned> d_thr, d_thr_status;
+  swgpu::DevBuf<uint8_t> d_tbits;   // H-bit words of the transposed threshold pass
+  swgpu::DevBuf<swgpu::TileRect> d_part_rects;  // one group's tile rectangles (split-pass exchange)
+  swgpu::DevBuf<long long> d_part_pre;
+  swgpu::DevBuf<long long> d_tpre;  // its two item prefix arrays
   swgpu::HostPinned<unsigned> h_thr_status;
   // batched sweeps: one bitmap slot per distinct threshold
   swgpu::DevBuf<uint64_t> d_bbits;

@@ -91,10 +91,17 @@ __device__ __forceinline__ float gelu_grad(float x) {
 // ---------------------------------------------------------------------------
 // tcgen05 / TMA building blocks (inline PTX)
 // ---------------------------------------------------------------------------
-constexpr int G_BM = 128, G_BN = 128, G_BK = 64, G_STAGES = 4;
-constexpr int G_TILE_BYTES = G_BM * G_BK * 2;  // 16 KB per operand tile (A and B tiles are both 128 x 64)
-constexpr int G_STAGE_BYTES = 2 * G_TILE_BYTES;
-constexpr int G_TMEM_COLS = 128;
+constexpr int G_BM = 128, G_BK = 64, G_STAGES = 4;
+constexpr int G_TILE_BYTES = G_BM * G_BK * 2;  // 16 KB: the A tile (128 x 64)
+// Per tile width BN (128, or 64 when 128-wide tiles would leave SMs idle):
+// the B tile (BN x 64), the stage, the tensor-memory columns of the
+// accumulator and the instruction descriptor.
+template <int BN>
+struct GemmShape {
+  static constexpr int B_BYTES = BN * G_BK * 2;
+  static constexpr int STAGE_BYTES = G_TILE_BYTES + B_BYTES;
+  static constexpr int TMEM_COLS = BN;  // a power of two >= 32
+};
 // 8 warps: warp w drains accumulator rows 32*(w%4) .. +31 (the tensor-memory
 // lanes its quarter may read) and columns 64*(w/4) .. +63
 constexpr int G_THREADS = 256;
@@ -136,9 +143,11 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 }
 
 // Instruction descriptor: fp32 accumulator, bf16 A and B, both K-major,
-// N = 128 (bits 17-22 hold N/8), M = 128 (bits 24-28 hold M/16).
-constexpr uint32_t G_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(G_BN >> 3) << 17) |
-                             ((uint32_t)(G_BM >> 4) << 24);
+// N = BN (bits 17-22 hold N/8), M = 128 (bits 24-28 hold M/16).
+template <int BN>
+__host__ __device__ constexpr uint32_t gemm_idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(G_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile(
@@ -150,19 +159,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// One CTA per 128 x 128 tile of C.  Warp 0 lane 0 feeds the stage ring with
+// One CTA per 128 x BN tile of C.  Warp 0 lane 0 feeds the stage ring with
 // TMA, warp 1 lane 0 issues the MMAs (4 per 64-wide K step) and commits each
 // stage back to the producer; then all eight warps drain the accumulator.
-__global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid_constant__ CUtensorMap ta,
-                                                              const __grid_constant__ CUtensorMap tb, int M, int N,
-                                                              int K, GemmEpi ep) {
+template <int BN>
+__global__ void __launch_bounds__(G_THREADS, BN == 64 ? 2 : 1)
+    gemm_bf16_tn_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int M, int N,
+                        int K, GemmEpi ep) {
+  using S = GemmShape<BN>;
   extern __shared__ uint8_t g_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(g_smem_raw) + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[G_STAGES], empty_bar[G_STAGES], done_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int s_issued, s_consumed;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * G_BM, n0 = blockIdx.x * G_BN;
+  const int m0 = blockIdx.y * G_BM, n0 = blockIdx.x * BN;
   const int nk = K / G_BK;
 
   if (threadIdx.x == 0) {
@@ -176,7 +187,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(G_TMEM_COLS)
+                 "r"(S::TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -193,9 +204,9 @@ __global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid
         atomicOr(ep.status, KST_TIMEOUT);
         break;
       }
-      uint8_t* a_tile = smem + s * G_STAGE_BYTES;
+      uint8_t* a_tile = smem + s * S::STAGE_BYTES;
       uint8_t* b_tile = a_tile + G_TILE_BYTES;
-      mbar_arrive_expect_tx(&full_bar[s], G_STAGE_BYTES);
+      mbar_arrive_expect_tx(&full_bar[s], S::STAGE_BYTES);
       tma_load_2d(a_tile, &ta, kt * G_BK, m0, &full_bar[s]);
       tma_load_2d(b_tile, &tb, kt * G_BK, n0, &full_bar[s]);
     }
@@ -209,11 +220,11 @@ __global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid
         break;
       }
       tc_fence_after();
-      const uint64_t adesc = sw128_desc(smem_u32(smem + s * G_STAGE_BYTES));
-      const uint64_t bdesc = sw128_desc(smem_u32(smem + s * G_STAGE_BYTES + G_TILE_BYTES));
+      const uint64_t adesc = sw128_desc(smem_u32(smem + s * S::STAGE_BYTES));
+      const uint64_t bdesc = sw128_desc(smem_u32(smem + s * S::STAGE_BYTES + G_TILE_BYTES));
 #pragma unroll
       for (int k = 0; k < G_BK / 16; ++k)  // 16 bf16 = 32 bytes per MMA step along K
-        tc_mma(tmem, adesc + 2 * k, bdesc + 2 * k, G_IDESC, (kt | k) != 0 ? 1u : 0u);
+        tc_mma(tmem, adesc + 2 * k, bdesc + 2 * k, gemm_idesc<BN>(), (kt | k) != 0 ? 1u : 0u);
       tc_commit(&empty_bar[s]);  // the stage is free once these MMAs have read it
     }
     s_consumed = kt;
@@ -231,7 +242,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid
   const int quarter = warp & 3, half = warp >> 2;
   const int m = m0 + quarter * 32 + lane;
   if (ok) {
-    for (int c = half * (G_BN / 2); c < (half + 1) * (G_BN / 2); c += 16) {
+    for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 16) {
       uint32_t r[16];
       tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
       const long long rowoff = (long long)m * N + n0 + c;
@@ -306,11 +317,14 @@ __global__ void __launch_bounds__(G_THREADS, 1) gemm_bf16_tn_kernel(const __grid
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS)
+                 : "memory");
   }
 }
 
-size_t gemm_smem_bytes() { return (size_t)G_STAGES * G_STAGE_BYTES + 1024; }
+size_t gemm_smem_bytes(int bn) {
+  return (size_t)G_STAGES * (bn == 64 ? GemmShape<64>::STAGE_BYTES : GemmShape<128>::STAGE_BYTES) + 1024;
+}
 
 namespace {
 
@@ -330,13 +344,13 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// Tensor map of a row-major bf16 [rows x cols] matrix, box 64 (cols) x 128 (rows), 128-byte swizzle.
-cudaError_t make_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int cols) {
+// Tensor map of a row-major bf16 [rows x cols] matrix, box 64 (cols) x box_rows, 128-byte swizzle.
+cudaError_t make_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int cols, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return cudaErrorNotSupported;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)G_BK, (cuuint32_t)G_BM};
+  const cuuint32_t box[2] = {(cuuint32_t)G_BK, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(base), dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -346,27 +360,47 @@ cudaError_t make_map(CUtensorMap* map, const __nv_bfloat16* base, int rows, int 
 
 }  // namespace
 
+int gemm_force_bn = 0;
+
+static cudaError_t launch_gemm_bn(int bn, const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
+                                  const GemmEpi& ep, cudaStream_t st) {
+  CUtensorMap ma, mb;
+  cudaError_t e = make_map(&ma, A, M, K, G_BM);
+  if (e == cudaSuccess) e = make_map(&mb, B, N, K, bn);
+  if (e != cudaSuccess) return e;
+  static bool attr64 = false, attr128 = false;
+  bool& attr = bn == 64 ? attr64 : attr128;
+  auto kern = bn == 64 ? gemm_bf16_tn_kernel<64> : gemm_bf16_tn_kernel<128>;
+  if (!attr) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes(bn));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  dim3 grid(N / bn, M / G_BM);
+  kern<<<grid, G_THREADS, gemm_smem_bytes(bn), st>>>(ma, mb, M, N, K, ep);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                                 const GemmEpi& ep, cudaStream_t st) {
-  if (M <= 0 || N <= 0 || K <= 0 || M % G_BM || N % G_BN || K % G_BK) return cudaErrorInvalidValue;
+  if (M <= 0 || N <= 0 || K <= 0 || M % G_BM || N % 64 || K % G_BK) return cudaErrorInvalidValue;
   // operands and every epilogue array are read and written in 16-byte units
   if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B) | reinterpret_cast<uintptr_t>(ep.bias) |
        reinterpret_cast<uintptr_t>(ep.gelu_in) | reinterpret_cast<uintptr_t>(ep.out_pre) |
        reinterpret_cast<uintptr_t>(ep.out_f32) | reinterpret_cast<uintptr_t>(ep.out_bf16)) & 15)
     return cudaErrorInvalidValue;
-  CUtensorMap ma, mb;
-  cudaError_t e = make_map(&ma, A, M, K);
-  if (e == cudaSuccess) e = make_map(&mb, B, N, K);
+  // 128-wide tiles unless they would leave SMs idle (or N is not a multiple
+  // of 128): then 64-wide tiles, two CTAs per SM
+  int dev = 0, sms = 148;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  static bool attr = false;
-  if (!attr) {
-    e = cudaFuncSetAttribute(gemm_bf16_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes());
-    if (e != cudaSuccess) return e;
-    attr = true;
+  const int bn = (N % 128 != 0 || (long long)(M / G_BM) * (N / 128) < sms) ? 64 : 128;
+  if (gemm_force_bn == 64 || gemm_force_bn == 128) {
+    if (gemm_force_bn == 128 && N % 128) return cudaErrorInvalidValue;
+    return launch_gemm_bn(gemm_force_bn, A, B, M, N, K, ep, st);
   }
-  dim3 grid(N / G_BN, M / G_BM);
-  gemm_bf16_tn_kernel<<<grid, G_THREADS, gemm_smem_bytes(), st>>>(ma, mb, M, N, K, ep);
-  return cudaGetLastError();
+  return launch_gemm_bn(bn, A, B, M, N, K, ep, st);
 }
 
 // ---------------------------------------------------------------------------

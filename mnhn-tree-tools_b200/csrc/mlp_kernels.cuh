@@ -45,7 +45,9 @@ struct GemmEpi {
 };
 cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                                 const GemmEpi& ep, cudaStream_t st);
-size_t gemm_smem_bytes();
+size_t gemm_smem_bytes(int bn);
+// Test hook: 64 or 128 forces that tile width (0: chosen by shape).
+extern int gemm_force_bn;
 
 // Exact GELU, x * Phi(x), and its derivative.
 __host__ __device__ float gelu_ref(float x);

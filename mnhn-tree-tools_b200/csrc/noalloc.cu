@@ -1,23 +1,26 @@
 // Allocation-free pair scoring: swe_score_pairs_noalloc.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured, real-time or embedded callers that must not touch the
-// device allocator after start-up, and hosts whose device memory is owned by a
-// pooling allocator that this library cannot see.  They already hold their
-// inputs and outputs on the device; this entry point scores pairs from those
-// buffers and allocates nothing.
+// Some callers cannot call cudaMalloc: real-time or embedded hosts that must
+// not touch the device allocator once they have started, and programs whose
+// device memory is all owned by their own pooling allocator, which this
+// library cannot see or grow.  They already hold their inputs and outputs on
+// the device; this entry point scores pairs from those buffers and allocates
+// nothing.
 //
 // The 32-bit wavefront needs one scratch column per warp for sequences longer
 // than one 512-column chunk.  Here that scratch is a file-scope device array of
-// SWE_NOALLOC_SCRATCH_INTS ints (4 MiB, held by every GPU that loads the
-// library until the process exits).  Each warp gets max_len + 1 ints of it, so
-// a call runs min(1024, 2^20 / (max_len + 1)) warps; the longest sequence a
-// call may reference is SWE_NOALLOC_MAX_LEN symbols.
+// NOALLOC_SCRATCH_INTS ints (4 MiB, held by every GPU that loads the library
+// until the process exits).  Each warp gets max_len + 1 ints of it, so a call
+// runs min(1024, 2^20 / (max_len + 1)) warps; the longest sequence a call may
+// reference is SWE_NOALLOC_MAX_LEN symbols.  A second static word counts the
+// pairs that reference a sequence longer than the caller's max_len; every
+// call clears it before its kernel runs.
 //
-// Host code cannot pass the array's name to a kernel (on the host it is only a
-// stand-in for the device symbol), so the device address is looked up once per
-// device with cudaGetSymbolAddress, with that device current, on the first
-// call made on it.
+// Host code cannot pass the arrays' names to a kernel (on the host they are
+// only stand-ins for the device symbols), so the device addresses are looked
+// up once per device with cudaGetSymbolAddress, with that device current, on
+// the first call made on it.  A cudaDeviceReset of that device invalidates
+// them; the call is not meant to be used after one.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,6 +34,8 @@ namespace swgpu {
 
 constexpr int NOALLOC_SCRATCH_INTS = 1 << 20;
 static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_SCRATCH_INTS];
+// pairs of the current call whose sequence is longer than max_len
+static __device__ __align__(256) unsigned g_noalloc_rejected;
 
 struct NoAllocParams {
   const char* seqs;      // sequence bytes; sequence i starts at seqs + off[i]
@@ -41,6 +46,7 @@ struct NoAllocParams {
   unsigned* out;         // npairs distances
   int max_len;
   int* scratch;          // device address of g_noalloc_scratch
+  unsigned* rejected;    // device address of g_noalloc_rejected
   long long stride;      // ints per warp = max_len + 1
   int nwarps;
 };
@@ -58,7 +64,10 @@ __global__ void __launch_bounds__(256) noalloc_pairs_kernel(NoAllocParams p) {
     const int la = p.len[ia], lb = p.len[ib];
     if (la > p.max_len || lb > p.max_len || la < 0 || lb < 0) {
       // longer than the caller declared: the scratch slice would overflow
-      if (lane == 0) p.out[w] = 0xFFFFFFFFu;
+      if (lane == 0) {
+        p.out[w] = 0xFFFFFFFFu;
+        atomicAdd(p.rejected, 1u);
+      }
       continue;
     }
     const uint8_t* A = reinterpret_cast<const uint8_t*>(p.seqs + p.off[ia]) + 1;
@@ -79,7 +88,11 @@ __global__ void __launch_bounds__(256) noalloc_pairs_kernel(NoAllocParams p) {
 
 namespace {
 std::mutex g_setup_mu;
-int* g_scratch_addr[64] = {nullptr};
+struct DeviceSymbols {
+  int* scratch = nullptr;
+  unsigned* rejected = nullptr;
+};
+DeviceSymbols g_symbols[64];
 }  // namespace
 
 }  // namespace swgpu
@@ -91,25 +104,30 @@ extern "C" swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* o
   if (npairs < 0 || max_len < 0 || max_len > SWE_NOALLOC_MAX_LEN) return SWE_ERR_INVALID;
   if (npairs == 0) return SWE_OK;
   if (!seqs || !off || !len || !pairs || !out) return SWE_ERR_INVALID;
+  // an error left by the caller's own earlier work is theirs: report it, keep it
+  if (cudaPeekAtLastError() != cudaSuccess) return SWE_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     cudaGetLastError();
     return SWE_ERR_NO_DEVICE;
   }
-  int* scratch = nullptr;
+  DeviceSymbols sym;
   {
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-      void* addr = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-      if (e != cudaSuccess || !addr) {
+    if (!g_symbols[dev].scratch) {
+      void* a = nullptr;
+      void* r = nullptr;
+      if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess || !a ||
+          cudaGetSymbolAddress(&r, g_noalloc_rejected) != cudaSuccess || !r) {
         cudaGetLastError();
         return SWE_ERR_CUDA;
       }
-      g_scratch_addr[dev] = static_cast<int*>(addr);
+      g_symbols[dev].scratch = static_cast<int*>(a);
+      g_symbols[dev].rejected = static_cast<unsigned*>(r);
     }
-    scratch = g_scratch_addr[dev];
+    sym = g_symbols[dev];
   }
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
   NoAllocParams p;
   p.seqs = seqs;
   p.off = off;
@@ -118,14 +136,26 @@ extern "C" swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* o
   p.npairs = npairs;
   p.out = out;
   p.max_len = max_len;
-  p.scratch = scratch;
+  p.scratch = sym.scratch;
+  p.rejected = sym.rejected;
   p.stride = (long long)max_len + 1;
   long long warps = NOALLOC_SCRATCH_INTS / p.stride;
   if (warps > 1024) warps = 1024;
   if (warps > npairs) warps = npairs;
   p.nwarps = (int)warps;
   const int blocks = (p.nwarps + 7) / 8;
-  noalloc_pairs_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
+  // the counter keeps the previous call's value: clear it first
+  if (cudaMemsetAsync(sym.rejected, 0, sizeof(unsigned), st) != cudaSuccess) {
+    cudaGetLastError();
+    return SWE_ERR_CUDA;
+  }
+  noalloc_pairs_kernel<<<blocks, 256, 0, st>>>(p);
   if (cudaGetLastError() != cudaSuccess) return SWE_ERR_CUDA;
-  return SWE_OK;
+  unsigned rejected = 0;
+  if (cudaMemcpyAsync(&rejected, sym.rejected, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return SWE_ERR_CUDA;
+  }
+  return rejected ? SWE_ERR_INVALID : SWE_OK;
 }

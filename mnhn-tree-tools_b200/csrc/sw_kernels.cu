@@ -660,6 +660,258 @@ cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const Thr
   return launch_threshold_t<uint32_t>(p, p.D32, total_rows, plan, st);
 }
 
+// ---------------------------------------------------------------------------
+// Transposed two-pass threshold (the default when an H-row block fits in
+// shared memory).  The matrix is stored with rows and columns in sorted
+// order; neighbour bits are wanted in original order.  Gathering each element
+// through the position table costs a random shared-memory read per element;
+// here it costs one per H elements:
+//   pass 1 (thr_pack_kernel): for a block of H consecutive sorted rows, thread
+//     k reads the H values of sorted column k (each step one coalesced row
+//     segment) and writes, per threshold, the H-bit word of that column;
+//   pass 2 (thr_unpack_kernel): one CTA stages a block's words of one
+//     threshold in shared memory; lane l of a warp takes original column j
+//     and reads word[pos[j]] (H rows at once), then H ballots turn the 32
+//     lanes' words into 32-column bit runs of the H rows, which go out through
+//     a shared-memory stage in row runs.
+// ---------------------------------------------------------------------------
+template <int H>
+struct HWord;
+template <>
+struct HWord<8> {
+  using T = uint8_t;
+};
+template <>
+struct HWord<16> {
+  using T = uint16_t;
+};
+template <>
+struct HWord<32> {
+  using T = uint32_t;
+};
+
+constexpr int TP1_THREADS = 256;
+constexpr int TP2_THREADS = 512;
+constexpr int TP2_SLICES = 4;  // 32-column slices per warp per chunk
+constexpr int TP2_CHUNK_WORDS = (TP2_THREADS / 32) * TP2_SLICES;
+constexpr size_t TP_BLOCK_MAX = 200 * 1024;
+
+int transposed_height(int max_n_s) {
+  for (int H = 32; H >= 8; H >>= 1)
+    if ((size_t)transposed_block_stride(max_n_s, H) <= TP_BLOCK_MAX) return H;
+  return 0;
+}
+
+int transposed_block_stride(int n_s, int H) { return (int)((((size_t)n_s * (size_t)(H / 8)) + 15) & ~(size_t)15); }
+
+__device__ __forceinline__ int tp_find_group(const long long* pre, int ngroups, long long item) {
+  int lo = 0, hi = ngroups - 1;  // last group with pre[g] <= item
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int H, typename DT>
+__global__ void __launch_bounds__(TP1_THREADS) thr_pack_kernel(ThrParams p, const DT* __restrict__ D,
+                                                               const long long* __restrict__ item_pre) {
+  using W = typename HWord<H>::T;
+  const long long items = item_pre[p.ngroups];
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const int g = tp_find_group(item_pre, p.ngroups, item);
+    const ThrGroup G = p.groups[g];
+    const int ns = G.n_s;
+    const int nch = (ns + TP1_THREADS - 1) / TP1_THREADS;
+    const long long r = item - item_pre[g];
+    const int B = (int)(r / nch), ch = (int)(r % nch);
+    const int k = ch * TP1_THREADS + threadIdx.x;
+    if (k >= ns) continue;
+    const int rows = min(H, ns - B * H);
+    const DT* col = D + G.dist_base + (long long)B * H * ns + k;
+    unsigned v[H];
+#pragma unroll
+    for (int t = 0; t < H; ++t) v[t] = t < rows ? (unsigned)col[(long long)t * ns] : 0xFFFFFFFFu;
+    uint8_t* out = p.tbits + G.tb_base + (long long)B * G.blk_stride;
+    const long long plane = (long long)G.nblk * G.blk_stride;
+    for (int u = 0; u < G.nthr; ++u) {
+      const unsigned th = p.thr[G.thr_first + u];
+      unsigned w = 0;
+#pragma unroll
+      for (int t = 0; t < H; ++t) w |= (v[t] <= th ? 1u : 0u) << t;
+      reinterpret_cast<W*>(out + (long long)u * plane)[k] = (W)w;
+    }
+  }
+}
+
+template <int H>
+__global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, const long long* __restrict__ item_pre,
+                                                                 int blk_bytes_max) {
+  using W = typename HWord<H>::T;
+  extern __shared__ __align__(16) uint8_t tp_smem[];
+  W* blk = reinterpret_cast<W*>(tp_smem);
+  uint32_t* stage = reinterpret_cast<uint32_t*>(tp_smem + blk_bytes_max);  // H rows x TP2_CHUNK_WORDS
+  __shared__ int s_cnt[H];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = TP2_THREADS / 32;
+  const long long items = item_pre[p.ngroups];
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const int g = tp_find_group(item_pre, p.ngroups, item);
+    const ThrGroup G = p.groups[g];
+    const int ns = G.n_s;
+    const long long r = item - item_pre[g];
+    const int u = (int)(r / G.nblk), B = (int)(r % G.nblk);
+    const uint4* src = reinterpret_cast<const uint4*>(p.tbits + G.tb_base + (long long)u * G.nblk * G.blk_stride +
+                                                      (long long)B * G.blk_stride);
+    for (int q = tid; q < G.blk_stride / 16; q += TP2_THREADS) reinterpret_cast<uint4*>(tp_smem)[q] = src[q];
+    if (tid < H) s_cnt[tid] = 0;
+    __syncthreads();
+    const int rows = min(H, ns - B * H);
+    const int* ps = p.pos + G.pos_first;
+    const int words32 = 2 * G.wpr;  // every 32-bit half of the row's 64-bit words, padding included
+    uint64_t* plane_bits = p.bits + G.bits_base + (long long)u * ns * G.wpr;
+    int cnt = 0;
+    for (int cw0 = 0; cw0 < words32; cw0 += TP2_CHUNK_WORDS) {
+#pragma unroll
+      for (int s = 0; s < TP2_SLICES; ++s) {
+        const int wl = warp * TP2_SLICES + s;  // word of the chunk
+        const int wi = cw0 + wl;
+        if (wi >= words32) break;  // warp-uniform
+        const int j = wi * 32 + lane;
+        const unsigned w = j < ns ? (unsigned)blk[ps[j]] : 0u;
+        uint32_t mine = 0;
+#pragma unroll
+        for (int t = 0; t < H; ++t) {
+          const uint32_t b = __ballot_sync(0xFFFFFFFFu, (w >> t) & 1u);
+          if (lane == t) mine = b;
+        }
+        if (lane < H) {
+          stage[lane * TP2_CHUNK_WORDS + wl] = mine;
+          cnt += __popc(mine);
+        }
+      }
+      __syncthreads();
+      const int nw = min(TP2_CHUNK_WORDS, words32 - cw0);
+      for (int t = warp; t < rows; t += nwarps) {
+        const int i = p.order[G.pos_first + B * H + t] - G.pos_first;  // original row inside the set
+        uint32_t* dst = reinterpret_cast<uint32_t*>(plane_bits + (long long)i * G.wpr) + cw0;
+        for (int x = lane; x < nw; x += 32) dst[x] = stage[t * TP2_CHUNK_WORDS + x];
+      }
+      __syncthreads();  // the stage is rewritten by the next chunk
+    }
+    if (lane < rows) atomicAdd(&s_cnt[lane], cnt);
+    __syncthreads();
+    if (tid < rows) {
+      const int i = p.order[G.pos_first + B * H + tid] - G.pos_first;
+      p.counts[G.counts_base + (long long)u * ns + i] = s_cnt[tid];
+    }
+    __syncthreads();  // blk and s_cnt are reused by the next item
+  }
+}
+
+template <int H>
+static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const long long* pre1, long long items1,
+                                       const long long* pre2, long long items2, cudaStream_t st) {
+  int dev = 0, sms = 148, occ1 = 1, occ2 = 1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (p.D16) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, thr_pack_kernel<H, uint16_t>, TP1_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    thr_pack_kernel<H, uint16_t><<<(int)std::min<long long>(items1, (long long)sms * std::max(occ1, 1)),
+                                   TP1_THREADS, 0, st>>>(p, p.D16, pre1);
+  } else {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, thr_pack_kernel<H, uint32_t>, TP1_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    thr_pack_kernel<H, uint32_t><<<(int)std::min<long long>(items1, (long long)sms * std::max(occ1, 1)),
+                                   TP1_THREADS, 0, st>>>(p, p.D32, pre1);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int blk_max = transposed_block_stride(max_n_s, H);
+  const size_t smem = (size_t)blk_max + (size_t)H * TP2_CHUNK_WORDS * 4;
+  e = cudaFuncSetAttribute(thr_unpack_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, thr_unpack_kernel<H>, TP2_THREADS, smem);
+  if (e != cudaSuccess) return e;
+  thr_unpack_kernel<H><<<(int)std::min<long long>(items2, (long long)sms * std::max(occ2, 1)), TP2_THREADS, smem,
+                         st>>>(p, pre2, blk_max);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, const long long* d_item_pre1,
+                                        long long items1, const long long* d_item_pre2, long long items2,
+                                        cudaStream_t st) {
+  if (items1 <= 0 || items2 <= 0 || p.ngroups <= 0) return cudaSuccess;
+  if (H == 32) return launch_transposed_h<32>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
+  if (H == 16) return launch_transposed_h<16>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
+  if (H == 8) return launch_transposed_h<8>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
+  return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Tile rectangles for the split pass's exchange: one entry per thread,
+// grid-stride; the tile of an entry by binary search over the prefix array.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int tile_of_entry(const long long* pre, int ntiles, long long e) {
+  int lo = 0, hi = ntiles - 1;  // last tile with pre[t] <= e
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= e) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) tile_pack_kernel(DistLayout L, const TileRect* __restrict__ rects,
+                                                        const long long* __restrict__ pre, int ntiles,
+                                                        void* __restrict__ out) {
+  const long long total = pre[ntiles];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int t = tile_of_entry(pre, ntiles, e);
+    const TileRect R = rects[t];
+    const long long k = e - pre[t];
+    const int r = (int)(k / R.nb), c = (int)(k - (long long)r * R.nb);
+    const int first = L.set_first[R.set], ns = L.set_n[R.set];
+    const long long idx = L.set_base[R.set] + (long long)(R.ra0 + r - first) * ns + (R.b0 + c - first);
+    if (L.D16) static_cast<uint16_t*>(out)[e] = L.D16[idx];
+    else static_cast<uint32_t*>(out)[e] = L.D32[idx];
+  }
+}
+
+__global__ void __launch_bounds__(256) tile_unpack_kernel(DistLayout L, const TileRect* __restrict__ rects,
+                                                          const long long* __restrict__ pre, int ntiles,
+                                                          const void* __restrict__ in, long long e0, long long e1) {
+  for (long long e = e0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; e < e1;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int t = tile_of_entry(pre, ntiles, e);
+    const TileRect R = rects[t];
+    const long long k = e - pre[t];
+    const int r = (int)(k / R.nb), c = (int)(k - (long long)r * R.nb);
+    const int first = L.set_first[R.set], ns = L.set_n[R.set];
+    const long long a = R.ra0 + r - first, b = R.b0 + c - first;
+    const unsigned v = L.D16 ? (unsigned)static_cast<const uint16_t*>(in)[e - e0]
+                             : static_cast<const uint32_t*>(in)[e - e0];
+    store_dist(L, L.set_base[R.set] + a * ns + b, v);
+    store_dist(L, L.set_base[R.set] + b * ns + a, v);
+  }
+}
+
+cudaError_t launch_tile_pack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
+                             void* out, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  tile_pack_kernel<<<148 * 8, 256, 0, st>>>(L, rects, pre, ntiles, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_unpack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
+                               const void* in, long long e0, long long e1, cudaStream_t st) {
+  if (ntiles <= 0 || e1 <= e0) return cudaSuccess;
+  tile_unpack_kernel<<<148 * 8, 256, 0, st>>>(L, rects, pre, ntiles, in, e0, e1);
+  return cudaGetLastError();
+}
+
 // Set matrix in original index order, widened to 32 bits.
 template <typename DT>
 __global__ void __launch_bounds__(256) unpermute_kernel(const DT* __restrict__ Dset, const int* __restrict__ pos,

@@ -41,6 +41,20 @@ struct FastTile {
   int b0, nb, q, wl, set;
 };
 
+// The rectangle of the sorted matrix a tile writes (both triangles): rows
+// ra0 .. ra0+nra-1 x columns b0 .. b0+nb-1 (global sorted positions, one set).
+struct TileRect {
+  int ra0, nra, b0, nb, set;
+};
+// Copies between a packed buffer of tile rectangles (tile after tile, row
+// after row, each entry one stored distance) and the matrix: pack reads rows
+// ra x columns b; unpack writes entries [e0, e1) of the buffer to both
+// triangles.  pre[t] = first entry of tile t (ntiles + 1 values).
+cudaError_t launch_tile_pack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
+                             void* out, cudaStream_t st);
+cudaError_t launch_tile_unpack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
+                               const void* in, long long e0, long long e1, cudaStream_t st);
+
 struct FastParams {
   const uint8_t* codes;      // effective symbol codes, all sequences
   const int64_t* code_off;   // per original index
@@ -127,11 +141,18 @@ struct ThrGroup {
   int pos_first;          // the set's slice of the position table
   int n_s, wpr;
   int thr_first, nthr;    // thresholds thr[thr_first .. thr_first + nthr), nthr <= THR_MAX
+  // transposed pass (launch_threshold_transposed): threshold u's bit blocks
+  // start at byte tb_base + u * nblk * blk_stride of the scratch, one block of
+  // blk_stride bytes per H consecutive sorted rows
+  long long tb_base;
+  int nblk, blk_stride;
 };
 struct ThrParams {
   const uint16_t* D16;      // one of D16 / D32 is non-null
   const uint32_t* D32;
   const int* pos;
+  const int* order;          // sorted position (+ set_first) -> original index
+  uint8_t* tbits;            // scratch of the transposed pass
   const ThrGroup* groups;
   int ngroups;
   const long long* row_pre;  // [ngroups + 1] prefix sums of the groups' n_s
@@ -151,6 +172,18 @@ struct ThrPlan {
 };
 ThrPlan threshold_plan(int max_n_s, int dist_bytes);
 cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const ThrPlan& plan, cudaStream_t st);
+// Transposed two-pass threshold.  Pass 1 streams each block of H consecutive
+// sorted rows once and writes, per threshold and sorted column, an H-bit word
+// (bit t = row t of the block is a neighbour).  Pass 2 stages one such block
+// in shared memory and gathers the words through the position table into
+// original column order: one random shared-memory read serves H rows.
+// transposed_height: H (32, 16 or 8) for the largest set, 0 when even an
+// 8-row block does not fit in shared memory.
+int transposed_height(int max_n_s);
+int transposed_block_stride(int n_s, int H);  // bytes, 16-byte multiple
+cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, const long long* d_item_pre1,
+                                        long long items1, const long long* d_item_pre2, long long items2,
+                                        cudaStream_t st);
 // Block [r0, r1) x [c0, c1) (original indices) of one set's matrix: per row the
 // sum of the distances and the sum of floor((d - mean)^2) (each square rounded
 // once in double), over the block the minimum and maximum (atomicMin / Max on

@@ -58,7 +58,7 @@ class SplitSet(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("sat_limit", C.c_int), ("packs_per_block", C.c_int),
                 ("threads", C.c_int), ("inject_timeout", C.c_int),
-                ("threshold_path", C.c_int), ("kmer_batch_kb", C.c_int)]
+                ("threshold_path", C.c_int), ("kmer_batch_kb", C.c_int), ("max_w", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -99,6 +99,17 @@ class Margins(C.Structure):
             t.upper[i] = int(u)
             t.margin[i] = float(v)
         return t
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("packs_per_block", C.c_int), ("threads", C.c_int), ("max_w", C.c_int), ("from_cache", C.c_int),
+                ("candidates", C.c_int), ("sample", C.c_int), ("sample_cells", C.c_double),
+                ("ms_default", C.c_double), ("ms_best", C.c_double), ("key", C.c_char * 160)]
+
+    def as_dict(self):
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["key"] = self.key.decode()
+        return d
 
 
 class SweepResult(C.Structure):
@@ -145,6 +156,7 @@ EXPORTS = [
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
     "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition",
     "swe_pca_covariance", "swe_pca_eigen", "swe_pca_eigen_gpu", "swe_pca_project", "swe_pca",
+    "swe_autotune", "swe_copy_set_rows", "swe_partition_bytes", "swe_partition_pack", "swe_partition_unpack",
     # include/mnhn_dropin.h
     "score", "dataset_from_fasta", "free_sequences_from_dataset", "dbscan_SW", "adaptive_dbscan",
     "store_split_set", "read_split_set", "create_single_cluster_file", "create_cluster_files",
@@ -191,6 +203,17 @@ def lib():
         L.swe_set_count.argtypes = [C.c_void_p]
         L.swe_copy_set_distances.restype = C.c_int
         L.swe_copy_set_distances.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.swe_partition_bytes.restype = C.c_int64
+        L.swe_partition_bytes.argtypes = [C.c_void_p, C.c_int]
+        L.swe_partition_pack.restype = C.c_int
+        L.swe_partition_pack.argtypes = [C.c_void_p, C.c_void_p]
+        L.swe_partition_unpack.restype = C.c_int
+        L.swe_partition_unpack.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_int64]
+        L.swe_autotune.restype = C.c_int
+        L.swe_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_int,
+                                   C.POINTER(TuneResult)]
+        L.swe_copy_set_rows.restype = C.c_int
+        L.swe_copy_set_rows.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.swe_neighbors_set.restype = C.c_int
         L.swe_neighbors_set.argtypes = [C.c_void_p, C.c_int, C.c_float, C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p)]
@@ -331,9 +354,10 @@ class Engine:
     """One engine context (one CUDA stream on one device)."""
 
     def __init__(self, device: int = 0, sat_limit: int = 0, packs_per_block: int = 0, threads: int = 0,
-                 inject_timeout: int = 0, threshold_path: int = 0, kmer_batch_kb: int = 0):
+                 inject_timeout: int = 0, threshold_path: int = 0, kmer_batch_kb: int = 0, max_w: int = 0):
         self.ctx = C.c_void_p()
-        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path, kmer_batch_kb)
+        opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path, kmer_batch_kb,
+                    max_w)
         _check(lib().swe_create(C.byref(self.ctx), C.byref(opts)))
         self.n = 0
         self._buf = None
@@ -410,6 +434,36 @@ class Engine:
             ns = self.set_size(set)
             out = np.zeros((ns, ns), dtype=np.uint32)
             _check(lib().swe_copy_set_distances(self.ctx, set, out.ctypes.data), self.ctx)
+        return out
+
+    def partition_bytes(self, part: int) -> int:
+        """Bytes of group `part`'s payload in the split pass's exchange."""
+        b = lib().swe_partition_bytes(self.ctx, part)
+        if b < 0:
+            raise SwgpuError(1, "no such group")
+        return int(b)
+
+    def partition_pack(self, dev_ptr: int):
+        _check(lib().swe_partition_pack(self.ctx, C.c_void_p(dev_ptr)), self.ctx)
+
+    def partition_unpack(self, part: int, dev_ptr: int, offset: int, nbytes: int):
+        _check(lib().swe_partition_unpack(self.ctx, part, C.c_void_p(dev_ptr), offset, nbytes), self.ctx)
+
+    def autotune(self, seqs, cache_path: str | None = None, force: bool = False) -> dict:
+        """Times the 16x2 kernel's tile plans on a length-stratified sample of
+        `seqs` and sets the fastest on this engine (see swe_autotune)."""
+        buf = SeqBuffer(seqs)
+        res = TuneResult()
+        _check(lib().swe_autotune(self.ctx, buf.ptrs, buf.lens, len(seqs),
+                                  cache_path.encode() if cache_path else None, 1 if force else 0,
+                                  C.byref(res)), self.ctx)
+        return res.as_dict()
+
+    def rows(self, row0: int, row1: int, set: int = 0) -> np.ndarray:
+        """Rows [row0, row1) of one set's distance matrix (original order)."""
+        ns = self.set_size(set)
+        out = np.zeros((row1 - row0, ns), dtype=np.uint32)
+        _check(lib().swe_copy_set_rows(self.ctx, set, row0, row1, out.ctypes.data), self.ctx)
         return out
 
     def neighbors(self, eps: float, set: int | None = None):

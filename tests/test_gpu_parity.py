@@ -165,14 +165,15 @@ def test_long_sequences_need_uint32_matrix():
     e.close()
 
 
-@pytest.mark.parametrize("threshold_path", [0, 1, 2, 3])
+@pytest.mark.parametrize("threshold_path", [0, 1, 2, 3, 4, 5, 6])
 def test_many_sets_in_one_upload_match_one_by_one(threshold_path):
     """Independent sets scored in one pass: each set's matrix equals the oracle's
     for that set alone (no pair across sets), and per-set neighbourhoods and
     DBSCAN equal the single-set results.  Sizes include empty and one-sequence
     sets and sets with 32-bit-path sequences only.  Every path of the threshold
-    pass (global gather, bulk-copied rows with and without staged positions,
-    one or two row buffers) gives the same bits."""
+    pass (the transposed two-pass one with 32-, 16- and 8-row blocks, global
+    gather, bulk-copied rows with and without staged positions, one or two
+    row buffers) gives the same bits."""
     rng = np.random.default_rng(31)
     mixed = _mixed_set(rng)
     pool, _ = W.config1()
@@ -525,6 +526,47 @@ def test_config2_full_properties_and_sampled_rows(eng):
 
 
 @pytest.mark.gpu
+def test_partitioned_tile_exchange_rebuilds_the_full_matrix():
+    """The exchange sized to the result on one GPU: three tile groups scored
+    one after the other (as three ranks would), each packing only its own
+    tile rectangles; a context holding group 0's pass unpacks the other two
+    payloads (in chunks that cut through tiles) and then holds the whole
+    pass's matrix, with DBSCAN matching."""
+    import torch
+    import swgpu
+    seqs, _ = W.config2(n=1500)
+    seqs = list(seqs) + [b"ACGTRYNNNNACGT" * 3, b"", b"A" * 900]  # 32-bit path rows too
+    eng = swgpu.Engine()
+    eng.upload(seqs)
+    eng.score_all_pairs()
+    full = eng.distances()
+    whole = eng.partition_bytes(0)
+    payload = []
+    for p in range(3):
+        eng.set_partition(p, 3)
+        eng.score_all_pairs()
+        sizes = [eng.partition_bytes(q) for q in range(3)]
+        buf = torch.empty(max(sizes[p], 16), dtype=torch.uint8, device="cuda:0")
+        eng.partition_pack(buf.data_ptr())
+        payload.append((sizes, buf))
+    assert payload[0][0] == payload[1][0] == payload[2][0]
+    assert sum(payload[0][0]) == whole  # the groups' tiles cover the layout once
+    eng.set_partition(0, 3)
+    eng.score_all_pairs()
+    assert not np.array_equal(eng.distances(), full)
+    chunk = 1 << 16
+    for p in (1, 2):
+        size = payload[p][0][p]
+        for off in range(0, size, chunk):
+            n = min(chunk, size - off)
+            eng.partition_unpack(p, payload[p][1][off:off + n].data_ptr(), off, n)
+    assert np.array_equal(eng.distances(), full)
+    assert eng.dbscan(300.0, 5) == O.dbscan(full, 300.0, 5)
+    with pytest.raises(swgpu.SwgpuError):
+        eng.partition_unpack(1, payload[1][1].data_ptr(), 2, 3)  # not whole distances
+    eng.close()
+
+
 def test_partitioned_score_passes_combine_to_the_full_matrix():
     """Three tile groups scored one after the other on one GPU (as three ranks
     would), each leaving 0xFF bytes outside its tiles; their bytewise minimum,

@@ -152,20 +152,21 @@ def calibrate_margin(emb_dist, d, lens_a, lens_b, eps: float, q: float) -> float
 
 
 def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8, batch_pairs: int = 4096,
-          lr: float = 1e-3, band_factor: float = 2.0, seed: int = 0, weight_decay: float = 0.0):
+          lr: float = 1e-3, band_factor: float = 2.0, seed: int = 0, weight_decay: float = 0.0,
+          mix=(0.25, 0.35)):
     """Trains the prefilter on pairs of ``train_sets`` (independent datasets
-    of the target distribution, scored in one exact pass): 25% neighbours
-    (d <= eps), 35% near pairs (eps < d <= band_factor * eps), 40% uniform.
-    The weights stay in ``eng``.  Returns a report."""
+    of the target distribution, scored in one exact pass): a fraction mix[0]
+    of neighbours (d <= eps), mix[1] of near pairs (eps < d <= band_factor *
+    eps), the rest uniform (default 25 / 35 / 40 %).  The weights stay in
+    ``eng``.  Returns a report."""
     rng = np.random.default_rng(seed)
     rep = {}
     t0 = time.perf_counter()
     eng.upload_sets(train_sets)
     eng.score_all_pairs()
     rep["train_exact_pass_s"] = round(time.perf_counter() - t0, 3)
-    (tr,), pools = sample_pairs(
-        eng, eps, band_factor * eps,
-        [(n_train // 4, n_train * 35 // 100, n_train - n_train // 4 - n_train * 35 // 100)], rng)
+    n_nb, n_near = int(n_train * mix[0]), int(n_train * mix[1])
+    (tr,), pools = sample_pairs(eng, eps, band_factor * eps, [(n_nb, n_near, n_train - n_nb - n_near)], rng)
     rep["train_pools"] = [int(x) for x in pools]
     t1 = time.perf_counter()
     ta, tb = tr
@@ -183,7 +184,7 @@ def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8
 
 
 def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995, band_factor: float = 2.0,
-              tune_scale: bool = True, seed: int = 0, embeddings=None, q_pass: float = 0.9998):
+              tune_scale: bool = True, seed: int = 0, embeddings=None, q_pass: float = 0.9998, buckets: int = 4):
     """Margins for ``eps`` from held-out pairs of ``cal_seqs`` (a dataset of
     the distribution with families the network never saw): 60% neighbours,
     20% near pairs, 20% uniform; per bucket of the longer length the
@@ -209,7 +210,7 @@ def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995
         ed = np.linalg.norm(emb[ca].astype(np.float64) - emb[cb], axis=1)
     else:
         ed = eng.prefilter_pair_dist(ca, cb)
-    margins = calibrate_buckets(ed, cd, lens[ca], lens[cb], eps, q)
+    margins = calibrate_buckets(ed, cd, lens[ca], lens[cb], eps, q, buckets=buckets)
     rep["margins_pairs"] = margins
     rep["cal_pools"] = [int(x) for x in cpools]
     rep["cal_neighbours"] = int((cd <= math.floor(eps)).sum())

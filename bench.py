@@ -723,7 +723,7 @@ def measure_single(run: Run, config: str, args, steps: int, warmup: int, e2e_rep
             "score_pass_ms": round(statistics.median(score_ms), 2),
             ("sweep_ms" if wl["mode"] == "adaptive" else "dbscan_ms"): round(sweep_s * 1e3, 2),
             "roofline": roof,
-            "threshold_roofline": {"bound": "hbm", "kernel": "threshold_bulk_kernel", "achieved": round(
+            "threshold_roofline": {"bound": "hbm", "kernel": "thr_pack_kernel + thr_unpack_kernel", "achieved": round(
                 thr_bytes / (thr_ms * 1e-3) / 1e9, 1), "peak": hbm_peak[0], "unit": "GB/s",
                 "frac": round(thr_bytes / (thr_ms * 1e-3) / 1e9 / hbm_peak[0], 4), "peak_source": hbm_peak[1],
                 "bytes_per_launch": thr_bytes, "ms_per_launch": round(thr_ms, 4)},
@@ -1019,13 +1019,19 @@ def measure_prefilter(run: Run, config: str, args, steps: int, warmup: int, e2e_
     margins0 = cal[eps_list[0]][0]
     e2e_ms = []
     b0 = eng.stats()
+    e2e_parts = []
     for _ in range(max(1, e2e_reps)):
         run.barrier()
         t1 = time.perf_counter()
         eng.upload(test)
+        t2 = time.perf_counter()
         eng.score_prefiltered(eps_list[0], margins0)
+        t3 = time.perf_counter()
         eng.dbscan(eps_list[0], wl["minpts"])
-        e2e_ms.append(1e3 * (time.perf_counter() - t1))
+        t4 = time.perf_counter()
+        e2e_ms.append(1e3 * (t4 - t1))
+        e2e_parts.append({"upload_ms": round(1e3 * (t2 - t1), 2), "prefiltered_pass_ms": round(1e3 * (t3 - t2), 2),
+                          "dbscan_ms": round(1e3 * (t4 - t3), 2)})
     b1 = eng.stats()
 
     # the same recipe without the network: a fixed random projection of the k-mer features
@@ -1080,7 +1086,7 @@ def measure_prefilter(run: Run, config: str, args, steps: int, warmup: int, e2e_
             "e2e": {"value": round(per_eps[head]["ms_exact_step"] / statistics.median(e2e_ms), 3),
                     "unit": "x (exact device step / prefiltered host-to-host step)",
                     "h2d_bytes_per_step": int(b1["h2d_bytes"]), "d2h_bytes_per_step": int(b1["d2h_bytes"]),
-                    "reps": len(e2e_ms)},
+                    "reps": len(e2e_ms), "parts": e2e_parts[-1]},
             "gpu_launches": int(launches_pf) if launches_pf is not None else None,
             "clocks": clk,
             "prefilter_speedup": sp,

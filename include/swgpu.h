@@ -401,6 +401,9 @@ typedef struct {
   double tile_cells;    /* DP cells the 16x2 kernel processed */
   double ms_embed, ms_candidates, ms_layout, ms_score, ms_total;  /* host wall times */
   int fallback_full;    /* 1 when there were too many candidates and every pair was scored */
+  double ms_groups;     /* of ms_layout: candidate groups and the sort keys */
+  double ms_marks;      /* of ms_layout: marking the tiles that hold a candidate */
+  double ms_upload;     /* of ms_layout: layout arrays to the device and the selector build */
 } swe_prefilter_stats;
 
 /* Margins of the prefilter by the pair's longer length L: bucket b < n-1

@@ -161,7 +161,7 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
   return SWE_OK;
 }
 
-static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand);
+static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const CandSource* cand);
 
 swe_status swe_set_partition(swe_ctx* ctx, int part, int nparts) {
   if (!ctx || nparts < 1 || part < 0 || part >= nparts) return SWE_ERR_INVALID;
@@ -292,7 +292,7 @@ extern "C" swe_status swe_partition_unpack(swe_ctx* ctx, int part, const void* d
 // (optional): only tiles holding one of these pairs (original indices) are
 // kept, and the distance matrix starts out at the largest value (no pair
 // scored means no neighbour).
-static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand) {
+static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, const CandSource* cand) {
   // per set: packed-path sequences in the chosen order (longest first by
   // default), then the 32-bit-path ones
   const int n = ctx->n, n_sets = ctx->n_sets;
@@ -409,12 +409,30 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
       b0 += nb;
     }
     std::vector<uint8_t> mark;
-    if (cand) {
+    const auto tm0 = std::chrono::steady_clock::now();
+    if (cand && cand->dev) {
+      // on the device: the candidates stay where the candidate kernel wrote them
+      const int lo = f, hi = ctx->set_first[k + 1], nq = std::max(q1 - q0, 1);
+      mark.assign(cbs.size() * (size_t)nq, 0);
+      if (k == 0) {  // the new positions of every set, once
+        CK(ctx->d_pos.alloc(std::max<size_t>(ctx->pos.size(), 1)));
+        CK(cpy(ctx, ctx->d_pos.p, ctx->pos.data(), sizeof(int) * ctx->pos.size(), cudaMemcpyHostToDevice, ctx->st));
+      }
+      CK(ctx->d_cbof.alloc(std::max(nf, 1)));
+      CK(ctx->d_mark.alloc(std::max<size_t>(mark.size(), 1)));
+      if (nf > 0) CK(cpy(ctx, ctx->d_cbof.p, cb_of.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, ctx->st));
+      CK(cudaMemsetAsync(ctx->d_mark.p, 0, std::max<size_t>(mark.size(), 1), ctx->st));
+      ctx->stats.kernel_launches += 1;
+      CK(launch_mark_tiles(cand->dev, cand->count, ctx->d_pos.p, lo, hi, nf, ctx->d_cbof.p, nq, PB, ctx->d_mark.p,
+                           ctx->st));
+      CK(cpy(ctx, mark.data(), ctx->d_mark.p, mark.size(), cudaMemcpyDeviceToHost, ctx->st));
+      CK(cudaStreamSynchronize(ctx->st));
+    } else if (cand) {
       mark.assign(cbs.size() * (size_t)std::max(q1 - q0, 1), 0);
       const int lo = f, hi = ctx->set_first[k + 1], nq = q1 - q0;
       auto mark_range = [&](std::vector<uint8_t>* mk, size_t c0, size_t c1) {
         for (size_t c = c0; c < c1; ++c) {
-          const int2 pr = (*cand)[c];
+          const int2 pr = (*cand->host)[c];
           if (pr.x < lo || pr.x >= hi || pr.y < lo || pr.y >= hi) continue;
           int px = ctx->pos[pr.x], py = ctx->pos[pr.y];
           if (px >= nf || py >= nf || px == py) continue;  // 32-bit-path pairs are all scored anyway
@@ -424,7 +442,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
         }
       };
       // threads mark private copies over slices of the candidates, then OR them
-      const size_t C = cand->size();
+      const size_t C = cand->host->size();
       const int T = (int)std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 1 + C / 200000);
       std::vector<std::vector<uint8_t>> priv(T - 1, std::vector<uint8_t>(mark.size(), 0));
       std::vector<std::thread> th;
@@ -434,6 +452,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
       for (const auto& pm : priv)
         for (size_t i = 0; i < mark.size(); ++i) mark[i] |= pm[i];
     }
+    ctx->ms_layout_marks += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tm0).count();
     for (size_t c = 0; c < cbs.size(); ++c) {
       const ColBlock& cb = cbs[c];
       for (int q = q0; q < q1; ++q) {
@@ -504,6 +523,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
   }
 
   // device copies
+  const auto tu0 = std::chrono::steady_clock::now();
   std::vector<int> set_n(n_sets);
   for (int k = 0; k < n_sets; ++k) set_n[k] = ctx->set_first[k + 1] - ctx->set_first[k];
   cudaStream_t st = ctx->st;
@@ -575,6 +595,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
   const int occ = std::max(1, fast_occupancy(ctx->threads, ctx->smem));
   ctx->fast_grid = std::max(1, std::min<int>(ctx->num_sms * occ, (int)std::max<size_t>(ctx->tiles.size(), 1)));
   CK(cudaStreamSynchronize(st));
+  ctx->ms_layout_upload += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tu0).count();
   return SWE_OK;
 }
 
@@ -766,7 +787,18 @@ swe_status swe_score_all_pairs(swe_ctx* ctx) {
 namespace swgpu {
 
 swe_status engine_relayout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand) {
-  return build_layout(ctx, key, cand);
+  if (!cand) return build_layout(ctx, key, nullptr);
+  CandSource src;
+  src.host = cand;
+  src.count = (long long)cand->size();
+  return build_layout(ctx, key, &src);
+}
+
+swe_status engine_relayout_dev(swe_ctx* ctx, const std::vector<int64_t>* key, const int2* cand, long long count) {
+  CandSource src;
+  src.dev = cand;
+  src.count = count;
+  return build_layout(ctx, key, &src);
 }
 
 swe_status score_pass(swe_ctx* ctx) {
@@ -948,7 +980,8 @@ static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& group
         G.blk_stride = transposed_block_stride(G.n_s, H);
         G.tb_base = tb;
         tb += (long long)G.nthr * G.nblk * G.blk_stride;
-        pre1[g + 1] = pre1[g] + (long long)G.nblk * ((G.n_s + 255) / 256);
+        const int ic = transposed_item_cols();
+        pre1[g + 1] = pre1[g] + (long long)G.nblk * ((G.n_s + ic - 1) / ic);
         pre2[g + 1] = pre2[g] + (long long)G.nthr * G.nblk;
       }
       CK(ctx->d_tbits.alloc((size_t)std::max<long long>(tb, 16)));

@@ -61,6 +61,15 @@ struct HostPinned {
   }
 };
 
+// Candidate pairs that restrict a layout to the tiles holding one: a host
+// vector, or `count` pairs on the device (original indices, bit 31 of .x a
+// flag the layout ignores).
+struct CandSource {
+  const std::vector<int2>* host = nullptr;
+  const int2* dev = nullptr;
+  long long count = 0;
+};
+
 struct PrefilterState;
 void prefilter_destroy(PrefilterState* pf);
 struct KmerState;
@@ -81,7 +90,8 @@ struct swe_ctx {
   int pf_packs_per_block = 8;   // the same for candidate-tile layouts (sparser work, finer tiles)
   int layout_pb = 32;           // the value the current layout was built with
   int threads = 256;
-  int max_w = swgpu::FAST_MAX_W;  // lane-split rule: a column sequence gets the fewest lanes holding <= max_w columns each
+  int max_w = swgpu::FAST_MAX_W;
+  double ms_layout_marks = 0, ms_layout_upload = 0;  // host time of build_layout's tile marks and uploads  // lane-split rule: a column sequence gets the fewest lanes holding <= max_w columns each
   int inject_timeout = 0;
   int part = 0, nparts = 1;     // this context scores tile group `part` of `nparts` (swe_set_partition)
   int threshold_path = 0;
@@ -169,6 +179,8 @@ struct swe_ctx {
   swgpu::DevBuf<long long> d_rowpre;
   swgpu::DevBuf<unsigned> d_thr, d_thr_status;
   swgpu::DevBuf<uint8_t> d_tbits;   // H-bit words of the transposed threshold pass
+  swgpu::DevBuf<int> d_cbof;         // column block of each sorted position (device tile marking)
+  swgpu::DevBuf<uint8_t> d_mark;     // tiles that hold a candidate pair
   swgpu::DevBuf<swgpu::TileRect> d_part_rects;  // one group's tile rectangles (split-pass exchange)
   swgpu::DevBuf<long long> d_part_pre;
   swgpu::DevBuf<long long> d_tpre;  // its two item prefix arrays
@@ -239,6 +251,9 @@ long long ctx_sweep_key(const swe_ctx* ctx, float eps);
 // Rebuilds the sorted layout (see build_layout in engine.cu) and runs one
 // score pass over the current layout.
 swe_status engine_relayout(swe_ctx* ctx, const std::vector<int64_t>* key, const std::vector<int2>* cand);
+// The same with the candidate pairs (original indices, bit 31 of .x ignored)
+// left on the device: the tiles holding one are marked by a kernel.
+swe_status engine_relayout_dev(swe_ctx* ctx, const std::vector<int64_t>* key, const int2* cand, long long count);
 swe_status score_pass(swe_ctx* ctx);
 long long eps_threshold(float eps);
 

@@ -389,13 +389,15 @@ cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, 
        reinterpret_cast<uintptr_t>(ep.gelu_in) | reinterpret_cast<uintptr_t>(ep.out_pre) |
        reinterpret_cast<uintptr_t>(ep.out_f32) | reinterpret_cast<uintptr_t>(ep.out_bf16)) & 15)
     return cudaErrorInvalidValue;
-  // 128-wide tiles unless they would leave SMs idle (or N is not a multiple
-  // of 128): then 64-wide tiles, two CTAs per SM
+  // 128-wide tiles unless fewer than half the SMs would get one (or N is not
+  // a multiple of 128): then 64-wide tiles, two CTAs per SM.  Measured on
+  // B200 with M = 4,096: N = 256 and 128 (64 and 32 tiles) 13.5 -> 11.4 and
+  // 9.8 -> 8.4 us; N = 512 (128 tiles) 16.5 -> 17.7 us, so it keeps 128.
   int dev = 0, sms = 148;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  const int bn = (N % 128 != 0 || (long long)(M / G_BM) * (N / 128) < sms) ? 64 : 128;
+  const int bn = (N % 128 != 0 || 2LL * (M / G_BM) * (N / 128) < sms) ? 64 : 128;
   if (gemm_force_bn == 64 || gemm_force_bn == 128) {
     if (gemm_force_bn == 128 && N % 128) return cudaErrorInvalidValue;
     return launch_gemm_bn(gemm_force_bn, A, B, M, N, K, ep, st);
@@ -522,7 +524,9 @@ template <int D>
 __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict__ emb, const int* __restrict__ orig,
                                                          const int* __restrict__ len, int first, int n, long long T,
                                                          MarginTable margins, int use_emb, int2* __restrict__ pairs,
-                                                         unsigned long long cap, unsigned long long* count) {
+                                                         unsigned long long cap, unsigned long long* count,
+                                                         int2* __restrict__ strong_pairs, unsigned long long strong_cap,
+                                                         unsigned long long* strong_count, uint8_t* __restrict__ has) {
   extern __shared__ float c_smem[];
   float (*ei)[D + 1] = reinterpret_cast<float (*)[D + 1]>(c_smem);
   float (*ej)[D + 1] = reinterpret_cast<float (*)[D + 1]>(c_smem + C_T * (D + 1));
@@ -610,6 +614,22 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
           if (cand) {
             const unsigned long long at = base + __popc(bal & ((1u << lane) - 1u));
             if (at < cap) pairs[at] = make_int2(oi[xi] | (strong ? (int)0x80000000u : 0), oj[xj]);
+            if (has) {
+              has[oi[xi]] = 1;
+              has[oj[xj]] = 1;
+            }
+          }
+        }
+        if (strong_pairs) {
+          const unsigned sb = __ballot_sync(0xFFFFFFFFu, strong);
+          if (sb) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(strong_count, (unsigned long long)__popc(sb));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (strong) {
+              const unsigned long long at = base + __popc(sb & ((1u << lane) - 1u));
+              if (at < strong_cap) strong_pairs[at] = make_int2(oi[xi], oj[xj]);
+            }
           }
         }
       }
@@ -618,7 +638,9 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
 
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
                               long long T, const MarginTable& margins, int use_emb, int2* pairs,
-                              unsigned long long cap, unsigned long long* count, cudaStream_t st) {
+                              unsigned long long cap, unsigned long long* count, int2* strong,
+                              unsigned long long strong_cap, unsigned long long* strong_count, uint8_t* has,
+                              cudaStream_t st) {
   if (margins.n < 1 || margins.n > MARGIN_BUCKETS) return cudaErrorInvalidValue;
   if (n <= 1) return cudaSuccess;
   if (D != 128) return cudaErrorInvalidValue;
@@ -631,7 +653,7 @@ cudaError_t launch_candidates(const float* emb, int D, const int* orig, const in
     if (e != cudaSuccess) return e;
   }
   candidates_kernel<128><<<grid, 256, smem, st>>>(emb, orig, len, first, n, T, margins, use_emb, pairs, cap,
-                                                  count);
+                                                  count, strong, strong_cap, strong_count, has);
   return cudaGetLastError();
 }
 

@@ -90,9 +90,17 @@ struct MarginTable {
 // *count); bit 31 of .x flags a "strong" pair, one whose embedding distance is
 // within the threshold without any margin.  Embeddings are per original
 // index, D floats each.  use_emb = 0: the length bound alone.
+// Candidate pairs of one set (positions first .. first+n-1 of `orig`): every
+// pair passing the length bound (and the embedding margin) goes to pairs[]
+// (original indices, bit 31 of .x set when the embedding distance is within
+// the threshold without margin: a "strong" pair); strong pairs also go to
+// strong[] (plain indices), and has[i] = 1 for every sequence in a candidate.
+// strong and has may be NULL.
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
                               long long T, const MarginTable& margins, int use_emb, int2* pairs,
-                              unsigned long long cap, unsigned long long* count, cudaStream_t st);
+                              unsigned long long cap, unsigned long long* count, int2* strong,
+                              unsigned long long strong_cap, unsigned long long* strong_count, uint8_t* has,
+                              cudaStream_t st);
 // Embedding distances of explicit pairs (original indices).
 cudaError_t launch_pair_dist(const float* emb, int D, const int* a, const int* b, long long np, float* out,
                              cudaStream_t st);

@@ -40,9 +40,12 @@ struct PrefilterState {
   int feat_gen = -1, emb_gen = -1;
   bool emb_external = false;  // embeddings given by the caller (swe_prefilter_set_embeddings)
 
-  // candidate pairs of the last prefiltered pass
-  DevBuf<int2> cand;
-  DevBuf<unsigned long long> cand_count;
+  // candidate pairs of the last prefiltered pass (all, and the strong ones
+  // that form the groups), per-sequence "in a candidate" flags
+  DevBuf<int2> cand, strong;
+  DevBuf<unsigned long long> cand_count;  // [0] all, [1] strong
+  DevBuf<uint8_t> has;
+  HostPinned<int2> h_strong;
 
   // batch buffers (M rows)
   int M = 0;
@@ -460,42 +463,53 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
   }
   st.ms_embed = ms_since(t0);
   const long long T = eps_threshold(eps);
-  // candidate pairs of every set
+  // candidate pairs of every set; the strong ones and the flags for the grouping
   const auto t1 = clk::now();
-  const unsigned long long cap = 1ull << 25;
+  const unsigned long long cap = 1ull << 25, strong_cap = 1ull << 23;
   CK(pf->cand.alloc(cap));
-  CK(pf->cand_count.alloc(1));
-  CK(cudaMemsetAsync(pf->cand_count.p, 0, sizeof(unsigned long long), ctx->st));
+  CK(pf->strong.alloc(strong_cap));
+  CK(pf->cand_count.alloc(2));
+  CK(pf->has.alloc(std::max(ctx->n, 1)));
+  CK(cudaMemsetAsync(pf->cand_count.p, 0, 2 * sizeof(unsigned long long), ctx->st));
+  CK(cudaMemsetAsync(pf->has.p, 0, std::max(ctx->n, 1), ctx->st));
   if (T >= 0 && ctx->n > 1) {
     for (int k = 0; k < ctx->n_sets; ++k) {
       const int f = ctx->set_first[k], nk = ctx->set_first[k + 1] - f;
       if (nk < 2) continue;
       ctx->stats.kernel_launches += 1;
       CK(launch_candidates(use_emb ? pf->emb.p : nullptr, PS::D3, ctx->d_order.p, ctx->d_len.p, f, nk, T, mt,
-                           use_emb, pf->cand.p, cap, pf->cand_count.p, ctx->st));
+                           use_emb, pf->cand.p, cap, pf->cand_count.p, pf->strong.p, strong_cap,
+                           pf->cand_count.p + 1, pf->has.p, ctx->st));
     }
   }
-  unsigned long long count = 0;
-  CK(cpy(ctx, &count, pf->cand_count.p, sizeof(count), cudaMemcpyDeviceToHost, ctx->st));
+  unsigned long long counts[2] = {0, 0};
+  CK(cpy(ctx, counts, pf->cand_count.p, sizeof(counts), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
+  const unsigned long long count = counts[0], nstrong = counts[1];
   st.candidates = (int64_t)count;
-  std::vector<int2> cand;
-  if (count <= cap) {
-    cand.resize(count);
-    if (count) CK(cpy(ctx, cand.data(), pf->cand.p, sizeof(int2) * count, cudaMemcpyDeviceToHost, ctx->st));
+  const int n = ctx->n;
+  std::vector<uint8_t> has;
+  if (count <= cap && nstrong <= strong_cap) {
+    // only the strong pairs and the flags come to the host; the candidate
+    // list stays on the device for the tile marks
+    CK(pf->h_strong.alloc(std::max<unsigned long long>(nstrong, 1)));
+    has.assign(std::max(n, 1), 0);
+    if (nstrong)
+      CK(cpy(ctx, pf->h_strong.p, pf->strong.p, sizeof(int2) * nstrong, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cpy(ctx, has.data(), pf->has.p, std::max(n, 1), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
   }
   st.ms_candidates = ms_since(t1);
   // layout: candidate components contiguous (longer first inside each), only candidate tiles
   const auto t2 = clk::now();
-  if (count > cap) {
+  ctx->ms_layout_marks = ctx->ms_layout_upload = 0;
+  if (count > cap || nstrong > strong_cap) {
     st.fallback_full = 1;
     if (swe_status s = engine_relayout(ctx, nullptr, nullptr)) return s;
   } else {
     // groups: connected components of the strong candidate pairs (embedding
     // distance within the threshold without margin), each laid out together,
     // longer first, so that the candidate pairs of a group fall into few tiles
-    const int n = ctx->n;
     std::vector<int> parent(n);
     std::iota(parent.begin(), parent.end(), 0);
     auto find = [&](int x) {
@@ -505,18 +519,13 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
       }
       return x;
     };
-    for (int2& pr : cand) {
-      const bool strong = pr.x < 0;
-      pr.x &= 0x7FFFFFFF;
-      if (!strong) continue;
-      const int x = find(pr.x), y = find(pr.y);
+    for (unsigned long long c = 0; c < nstrong; ++c) {
+      const int x = find(pf->h_strong.p[c].x), y = find(pf->h_strong.p[c].y);
       if (x != y) parent[std::max(x, y)] = std::min(x, y);  // the root is the group's smallest index
     }
     // groups in order of their mean length (longest first), so that the
     // column blocks and packs that straddle two groups still hold sequences
     // of similar lengths
-    std::vector<uint8_t> has(n, 0);
-    for (const int2& pr : cand) has[pr.x] = has[pr.y] = 1;
     std::vector<int64_t> gsum(n, 0), gcnt(n, 0);
     for (int i = 0; i < n; ++i) {
       const int r = find(i);
@@ -530,12 +539,15 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
       // no candidate at all: after every group (any order works for them)
       key[i] = has[i] ? (((int64_t)INT32_MAX - mean) << 32 | (int64_t)r) : INT64_MAX;
     }
-    if (swe_status s = engine_relayout(ctx, &key, &cand)) return s;
+    st.ms_groups = ms_since(t2);
+    if (swe_status s = engine_relayout_dev(ctx, &key, pf->cand.p, (long long)count)) return s;
   }
   st.tiles_kept = (int64_t)ctx->tiles.size();
   st.tiles_all = ctx->tiles_all;
   st.tile_cells = ctx->stats.tile_cells;
   st.ms_layout = ms_since(t2);
+  st.ms_marks = ctx->ms_layout_marks;
+  st.ms_upload = ctx->ms_layout_upload;
   const auto t3 = clk::now();
   if (swe_status s = score_pass(ctx)) return s;
   st.ms_score = ms_since(t3);

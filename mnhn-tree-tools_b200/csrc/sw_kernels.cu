@@ -691,9 +691,12 @@ struct HWord<32> {
 };
 
 constexpr int TP1_THREADS = 256;
-constexpr int TP2_THREADS = 512;
+constexpr int TP1_COLS = 8;  // columns per thread per item: items of 2,048 columns
+constexpr int TP1_ITEM_COLS = TP1_THREADS * TP1_COLS;
+constexpr int TP2_THREADS = 1024;
 constexpr int TP2_SLICES = 4;  // 32-column slices per warp per chunk
 constexpr int TP2_CHUNK_WORDS = (TP2_THREADS / 32) * TP2_SLICES;
+constexpr int TP2_STAGE_PITCH = TP2_CHUNK_WORDS + 1;  // odd pitch: lane t's stage row in its own bank
 constexpr size_t TP_BLOCK_MAX = 200 * 1024;
 
 int transposed_height(int max_n_s) {
@@ -703,6 +706,7 @@ int transposed_height(int max_n_s) {
 }
 
 int transposed_block_stride(int n_s, int H) { return (int)((((size_t)n_s * (size_t)(H / 8)) + 15) & ~(size_t)15); }
+int transposed_item_cols() { return TP1_ITEM_COLS; }
 
 __device__ __forceinline__ int tp_find_group(const long long* pre, int ngroups, long long item) {
   int lo = 0, hi = ngroups - 1;  // last group with pre[g] <= item
@@ -714,6 +718,9 @@ __device__ __forceinline__ int tp_find_group(const long long* pre, int ngroups, 
   return lo;
 }
 
+// An item is (group, block B, 2,048 columns); thread t of the CTA takes
+// columns c0 + t + 256 c, c < 8.  The item decodes in 32-bit arithmetic (a
+// group has far fewer than 2^31 items).
 template <int H, typename DT>
 __global__ void __launch_bounds__(TP1_THREADS) thr_pack_kernel(ThrParams p, const DT* __restrict__ D,
                                                                const long long* __restrict__ item_pre) {
@@ -723,24 +730,27 @@ __global__ void __launch_bounds__(TP1_THREADS) thr_pack_kernel(ThrParams p, cons
     const int g = tp_find_group(item_pre, p.ngroups, item);
     const ThrGroup G = p.groups[g];
     const int ns = G.n_s;
-    const int nch = (ns + TP1_THREADS - 1) / TP1_THREADS;
-    const long long r = item - item_pre[g];
-    const int B = (int)(r / nch), ch = (int)(r % nch);
-    const int k = ch * TP1_THREADS + threadIdx.x;
-    if (k >= ns) continue;
+    const int nch = (ns + TP1_ITEM_COLS - 1) / TP1_ITEM_COLS;
+    const int r = (int)(item - item_pre[g]);
+    const int B = r / nch, ch = r - B * nch;
     const int rows = min(H, ns - B * H);
-    const DT* col = D + G.dist_base + (long long)B * H * ns + k;
-    unsigned v[H];
-#pragma unroll
-    for (int t = 0; t < H; ++t) v[t] = t < rows ? (unsigned)col[(long long)t * ns] : 0xFFFFFFFFu;
+    const DT* blk = D + G.dist_base + (long long)B * H * ns;
     uint8_t* out = p.tbits + G.tb_base + (long long)B * G.blk_stride;
     const long long plane = (long long)G.nblk * G.blk_stride;
-    for (int u = 0; u < G.nthr; ++u) {
-      const unsigned th = p.thr[G.thr_first + u];
-      unsigned w = 0;
+#pragma unroll 1
+    for (int c = 0; c < TP1_COLS; ++c) {
+      const int k = ch * TP1_ITEM_COLS + c * TP1_THREADS + threadIdx.x;
+      if (k >= ns) break;
+      unsigned v[H];
 #pragma unroll
-      for (int t = 0; t < H; ++t) w |= (v[t] <= th ? 1u : 0u) << t;
-      reinterpret_cast<W*>(out + (long long)u * plane)[k] = (W)w;
+      for (int t = 0; t < H; ++t) v[t] = t < rows ? (unsigned)blk[(long long)t * ns + k] : 0xFFFFFFFFu;
+      for (int u = 0; u < G.nthr; ++u) {
+        const unsigned th = p.thr[G.thr_first + u];
+        unsigned w = 0;
+#pragma unroll
+        for (int t = 0; t < H; ++t) w |= (v[t] <= th ? 1u : 0u) << t;
+        reinterpret_cast<W*>(out + (long long)u * plane)[k] = (W)w;
+      }
     }
   }
 }
@@ -751,7 +761,7 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
   using W = typename HWord<H>::T;
   extern __shared__ __align__(16) uint8_t tp_smem[];
   W* blk = reinterpret_cast<W*>(tp_smem);
-  uint32_t* stage = reinterpret_cast<uint32_t*>(tp_smem + blk_bytes_max);  // H rows x TP2_CHUNK_WORDS
+  uint32_t* stage = reinterpret_cast<uint32_t*>(tp_smem + blk_bytes_max);  // H rows x TP2_STAGE_PITCH
   __shared__ int s_cnt[H];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = TP2_THREADS / 32;
   const long long items = item_pre[p.ngroups];
@@ -759,8 +769,8 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
     const int g = tp_find_group(item_pre, p.ngroups, item);
     const ThrGroup G = p.groups[g];
     const int ns = G.n_s;
-    const long long r = item - item_pre[g];
-    const int u = (int)(r / G.nblk), B = (int)(r % G.nblk);
+    const int r = (int)(item - item_pre[g]);
+    const int u = r / G.nblk, B = r - u * G.nblk;
     const uint4* src = reinterpret_cast<const uint4*>(p.tbits + G.tb_base + (long long)u * G.nblk * G.blk_stride +
                                                       (long long)B * G.blk_stride);
     for (int q = tid; q < G.blk_stride / 16; q += TP2_THREADS) reinterpret_cast<uint4*>(tp_smem)[q] = src[q];
@@ -772,21 +782,26 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
     uint64_t* plane_bits = p.bits + G.bits_base + (long long)u * ns * G.wpr;
     int cnt = 0;
     for (int cw0 = 0; cw0 < words32; cw0 += TP2_CHUNK_WORDS) {
+      // positions of every slice first (independent loads in flight), then the words
+      int q[TP2_SLICES];
 #pragma unroll
       for (int s = 0; s < TP2_SLICES; ++s) {
-        const int wl = warp * TP2_SLICES + s;  // word of the chunk
-        const int wi = cw0 + wl;
-        if (wi >= words32) break;  // warp-uniform
-        const int j = wi * 32 + lane;
-        const unsigned w = j < ns ? (unsigned)blk[ps[j]] : 0u;
+        const int j = (cw0 + warp * TP2_SLICES + s) * 32 + lane;
+        q[s] = j < ns ? ps[j] : -1;
+      }
+      unsigned w[TP2_SLICES];
+#pragma unroll
+      for (int s = 0; s < TP2_SLICES; ++s) w[s] = q[s] >= 0 ? (unsigned)blk[q[s]] : 0u;
+#pragma unroll
+      for (int s = 0; s < TP2_SLICES; ++s) {
         uint32_t mine = 0;
 #pragma unroll
         for (int t = 0; t < H; ++t) {
-          const uint32_t b = __ballot_sync(0xFFFFFFFFu, (w >> t) & 1u);
+          const uint32_t b = __ballot_sync(0xFFFFFFFFu, (w[s] >> t) & 1u);
           if (lane == t) mine = b;
         }
         if (lane < H) {
-          stage[lane * TP2_CHUNK_WORDS + wl] = mine;
+          stage[lane * TP2_STAGE_PITCH + warp * TP2_SLICES + s] = mine;
           cnt += __popc(mine);
         }
       }
@@ -795,7 +810,7 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
       for (int t = warp; t < rows; t += nwarps) {
         const int i = p.order[G.pos_first + B * H + t] - G.pos_first;  // original row inside the set
         uint32_t* dst = reinterpret_cast<uint32_t*>(plane_bits + (long long)i * G.wpr) + cw0;
-        for (int x = lane; x < nw; x += 32) dst[x] = stage[t * TP2_CHUNK_WORDS + x];
+        for (int x = lane; x < nw; x += 32) dst[x] = stage[t * TP2_STAGE_PITCH + x];
       }
       __syncthreads();  // the stage is rewritten by the next chunk
     }
@@ -829,7 +844,7 @@ static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const lo
   }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int blk_max = transposed_block_stride(max_n_s, H);
-  const size_t smem = (size_t)blk_max + (size_t)H * TP2_CHUNK_WORDS * 4;
+  const size_t smem = (size_t)blk_max + (size_t)H * TP2_STAGE_PITCH * 4;
   e = cudaFuncSetAttribute(thr_unpack_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, thr_unpack_kernel<H>, TP2_THREADS, smem);
@@ -896,6 +911,34 @@ __global__ void __launch_bounds__(256) tile_unpack_kernel(DistLayout L, const Ti
     store_dist(L, L.set_base[R.set] + a * ns + b, v);
     store_dist(L, L.set_base[R.set] + b * ns + a, v);
   }
+}
+
+__global__ void __launch_bounds__(256) mark_tiles_kernel(const int2* __restrict__ cand, long long count,
+                                                         const int* __restrict__ pos, int lo, int hi, int nf,
+                                                         const int* __restrict__ cb_of, int nq, int PB,
+                                                         uint8_t* __restrict__ mark) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < count;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int2 pr = cand[c];
+    const int x = pr.x & 0x7FFFFFFF, y = pr.y;
+    if (x < lo || x >= hi || y < lo || y >= hi) continue;
+    int px = pos[x], py = pos[y];
+    if (px >= nf || py >= nf || px == py) continue;  // 32-bit-path pairs are scored anyway
+    if (px > py) {
+      const int t = px;
+      px = py;
+      py = t;
+    }
+    mark[(size_t)cb_of[px] * nq + (py / 2) / PB] = 1;
+  }
+}
+
+cudaError_t launch_mark_tiles(const int2* cand, long long count, const int* pos, int lo, int hi, int nf,
+                              const int* cb_of, int nq, int PB, uint8_t* mark, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((count + 255) / 256, 148LL * 8);
+  mark_tiles_kernel<<<(int)blocks, 256, 0, st>>>(cand, count, pos, lo, hi, nf, cb_of, nq, PB, mark);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tile_pack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,

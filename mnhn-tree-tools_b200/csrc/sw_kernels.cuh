@@ -52,6 +52,12 @@ struct TileRect {
 // triangles.  pre[t] = first entry of tile t (ntiles + 1 values).
 cudaError_t launch_tile_pack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
                              void* out, cudaStream_t st);
+// Tiles of one set that hold a candidate pair: for pair (x, y) of original
+// indices in [lo, hi) with packed-path positions px < py (pos[]), sets
+// mark[cb_of[px] * nq + (py / 2) / PB] (the tile of column block cb_of[px]
+// and the row block of py).
+cudaError_t launch_mark_tiles(const int2* cand, long long count, const int* pos, int lo, int hi, int nf,
+                              const int* cb_of, int nq, int PB, uint8_t* mark, cudaStream_t st);
 cudaError_t launch_tile_unpack(const DistLayout& L, const TileRect* rects, const long long* pre, int ntiles,
                                const void* in, long long e0, long long e1, cudaStream_t st);
 
@@ -181,6 +187,7 @@ cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const Thr
 // 8-row block does not fit in shared memory.
 int transposed_height(int max_n_s);
 int transposed_block_stride(int n_s, int H);  // bytes, 16-byte multiple
+int transposed_item_cols();                   // columns of one pass-1 item
 cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, const long long* d_item_pre1,
                                         long long items1, const long long* d_item_pre2, long long items2,
                                         cudaStream_t st);

@@ -78,7 +78,8 @@ class PrefilterStats(C.Structure):
     _fields_ = [("candidates", C.c_int64), ("tiles_kept", C.c_int64), ("tiles_all", C.c_int64),
                 ("tile_cells", C.c_double), ("ms_embed", C.c_double), ("ms_candidates", C.c_double),
                 ("ms_layout", C.c_double), ("ms_score", C.c_double), ("ms_total", C.c_double),
-                ("fallback_full", C.c_int)]
+                ("fallback_full", C.c_int), ("ms_groups", C.c_double), ("ms_marks", C.c_double),
+                ("ms_upload", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -83,11 +83,13 @@ def test_kmer_features_match_reference():
 @pytest.mark.parametrize("M,N,K,bias,act", [(128, 128, 64, False, 0), (256, 256, 128, True, 0),
                                             (384, 512, 1024, True, 1), (128, 256, 8192, False, 0),
                                             (512, 1024, 256, False, 1), (256, 192, 128, True, 1),
-                                            (4096, 640, 256, True, 1), (4864, 512, 1024, True, 1)])
+                                            (4096, 640, 256, True, 1), (4864, 512, 1024, True, 1),
+                                            (4096, 512, 1024, True, 1)])
 def test_tcgen05_gemm_matches_float64(M, N, K, bias, act):
     """C = A B^T (+ bias, GELU) on the tensor cores against float64.  Grids of
-    fewer 128 x 128 tiles than SMs (and N = 192) run 128 x 64 tiles two CTAs
-    per SM; 4096 x 640 and 4864 x 512 run 128 x 128 tiles."""
+    128 x 128 tiles that would fill fewer than half the SMs (and N = 192) run
+    128 x 64 tiles two CTAs per SM; 4096 x 640, 4864 x 512 and 4096 x 512 run
+    128 x 128 tiles."""
     import torch
     g = torch.Generator().manual_seed(M * 7 + N + K)
     A = torch.randn(M, K, generator=g).to(torch.bfloat16)

@@ -18,6 +18,7 @@
 //   unpermute_kernel       a set's matrix back in original index order;
 //   csr_fill_kernel        bitmap -> ascending CSR column lists.
 #include <algorithm>
+#include <mutex>
 
 #include "sw_device.cuh"
 #include "sw_kernels.cuh"
@@ -737,22 +738,49 @@ __global__ void __launch_bounds__(TP1_THREADS) thr_pack_kernel(ThrParams p, cons
     const DT* blk = D + G.dist_base + (long long)B * H * ns;
     uint8_t* out = p.tbits + G.tb_base + (long long)B * G.blk_stride;
     const long long plane = (long long)G.nblk * G.blk_stride;
+    // CPI columns per iteration: CPI * H loads in flight per thread (32 or more)
+    constexpr int CPI = H == 32 ? 1 : 32 / H;
 #pragma unroll 1
-    for (int c = 0; c < TP1_COLS; ++c) {
-      const int k = ch * TP1_ITEM_COLS + c * TP1_THREADS + threadIdx.x;
-      if (k >= ns) break;
-      unsigned v[H];
+    for (int c = 0; c < TP1_COLS; c += CPI) {
+      unsigned v[CPI][H];
 #pragma unroll
-      for (int t = 0; t < H; ++t) v[t] = t < rows ? (unsigned)blk[(long long)t * ns + k] : 0xFFFFFFFFu;
-      for (int u = 0; u < G.nthr; ++u) {
-        const unsigned th = p.thr[G.thr_first + u];
-        unsigned w = 0;
+      for (int x = 0; x < CPI; ++x) {
+        const int k = ch * TP1_ITEM_COLS + (c + x) * TP1_THREADS + threadIdx.x;
+        const DT* q = blk + (k < ns ? k : 0);  // one pointer walks down the column
 #pragma unroll
-        for (int t = 0; t < H; ++t) w |= (v[t] <= th ? 1u : 0u) << t;
-        reinterpret_cast<W*>(out + (long long)u * plane)[k] = (W)w;
+        for (int t = 0; t < H; ++t) {
+          v[x][t] = (t < rows && k < ns) ? (unsigned)*q : 0xFFFFFFFFu;
+          q += ns;
+        }
+      }
+#pragma unroll
+      for (int x = 0; x < CPI; ++x) {
+        const int k = ch * TP1_ITEM_COLS + (c + x) * TP1_THREADS + threadIdx.x;
+        if (k >= ns) break;
+        for (int u = 0; u < G.nthr; ++u) {
+          const unsigned th = p.thr[G.thr_first + u];
+          unsigned w = 0;
+#pragma unroll
+          for (int t = 0; t < H; ++t) w |= (v[x][t] <= th ? 1u : 0u) << t;
+          reinterpret_cast<W*>(out + (long long)u * plane)[k] = (W)w;
+        }
       }
     }
   }
+}
+
+// 32 x 32 bit transpose across a warp: lane l holds word x (bit t = element
+// (t, l)); afterwards lane t holds the word whose bit l is element (t, l).
+// Five rounds of exchanging half-blocks with the lane j apart.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
+#pragma unroll
+  for (int j = 16; j >= 1; j >>= 1) {
+    const uint32_t m = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu : j == 2 ? 0x33333333u
+                                                                                                   : 0x55555555u;
+    const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, x, j);
+    x = (lane & j) ? ((x & ~m) | ((o >> j) & m)) : ((x & m) | ((o << j) & ~m));
+  }
+  return x;
 }
 
 template <int H>
@@ -794,12 +822,7 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
       for (int s = 0; s < TP2_SLICES; ++s) w[s] = q[s] >= 0 ? (unsigned)blk[q[s]] : 0u;
 #pragma unroll
       for (int s = 0; s < TP2_SLICES; ++s) {
-        uint32_t mine = 0;
-#pragma unroll
-        for (int t = 0; t < H; ++t) {
-          const uint32_t b = __ballot_sync(0xFFFFFFFFu, (w[s] >> t) & 1u);
-          if (lane == t) mine = b;
-        }
+        const uint32_t mine = warp_transpose32(w[s], lane);  // lane t: row t's bits of the 32 columns
         if (lane < H) {
           stage[lane * TP2_STAGE_PITCH + warp * TP2_SLICES + s] = mine;
           cnt += __popc(mine);
@@ -824,31 +847,53 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
   }
 }
 
+// Launch shapes are looked up once per kernel (and shared-memory size) so
+// that the second pass follows the first without host work in between.
 template <int H>
 static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const long long* pre1, long long items1,
                                        const long long* pre2, long long items2, cudaStream_t st) {
-  int dev = 0, sms = 148, occ1 = 1, occ2 = 1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  if (p.D16) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, thr_pack_kernel<H, uint16_t>, TP1_THREADS, 0);
-    if (e != cudaSuccess) return e;
-    thr_pack_kernel<H, uint16_t><<<(int)std::min<long long>(items1, (long long)sms * std::max(occ1, 1)),
-                                   TP1_THREADS, 0, st>>>(p, p.D16, pre1);
-  } else {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, thr_pack_kernel<H, uint32_t>, TP1_THREADS, 0);
-    if (e != cudaSuccess) return e;
-    thr_pack_kernel<H, uint32_t><<<(int)std::min<long long>(items1, (long long)sms * std::max(occ1, 1)),
-                                   TP1_THREADS, 0, st>>>(p, p.D32, pre1);
+  static std::mutex mu;
+  static int sms = 0, occ16 = 0, occ32 = 0;
+  static size_t smem_set = 0;
+  static int occ2_at = 0;
+  std::lock_guard<std::mutex> lock(mu);  // contexts on several host threads share the cache
+  cudaError_t e = cudaSuccess;
+  if (!sms) {
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ16, thr_pack_kernel<H, uint16_t>, TP1_THREADS, 0);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, thr_pack_kernel<H, uint32_t>, TP1_THREADS, 0);
+    if (e != cudaSuccess) {
+      sms = 0;
+      return e;
+    }
   }
+  const int occ1 = std::max(p.D16 ? occ16 : occ32, 1);
+  if (p.D16)
+    thr_pack_kernel<H, uint16_t><<<(int)std::min<long long>(items1, (long long)sms * occ1), TP1_THREADS, 0, st>>>(
+        p, p.D16, pre1);
+  else
+    thr_pack_kernel<H, uint32_t><<<(int)std::min<long long>(items1, (long long)sms * occ1), TP1_THREADS, 0, st>>>(
+        p, p.D32, pre1);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int blk_max = transposed_block_stride(max_n_s, H);
   const size_t smem = (size_t)blk_max + (size_t)H * TP2_STAGE_PITCH * 4;
-  e = cudaFuncSetAttribute(thr_unpack_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, thr_unpack_kernel<H>, TP2_THREADS, smem);
-  if (e != cudaSuccess) return e;
+  if (smem > smem_set) {  // the attribute only ever grows
+    e = cudaFuncSetAttribute(thr_unpack_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    smem_set = smem;
+    occ2_at = 0;
+  }
+  static size_t occ2_smem = 0;
+  if (!occ2_at || occ2_smem != smem) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2_at, thr_unpack_kernel<H>, TP2_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    occ2_smem = smem;
+  }
+  const int occ2 = occ2_at;
   thr_unpack_kernel<H><<<(int)std::min<long long>(items2, (long long)sms * std::max(occ2, 1)), TP2_THREADS, smem,
                          st>>>(p, pre2, blk_max);
   return cudaGetLastError();

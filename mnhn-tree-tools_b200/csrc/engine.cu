@@ -993,7 +993,9 @@ static swe_status launch_groups(swe_ctx* ctx, const std::vector<ThrGroup>& group
       p.tbits = ctx->d_tbits.p;
       CK(cudaEventRecord(ctx->ev[2], ctx->st));
       ctx->stats.kernel_launches += 2;
-      CK(launch_threshold_transposed(p, H, maxn, ctx->d_tpre.p, pre1.back(), ctx->d_tpre.p + pre1.size(),
+      bool aligned16 = ctx->threshold_path != 5 && ctx->threshold_path != 6;  // test hooks keep the scalar pass
+      for (const ThrGroup& G : groups) aligned16 = aligned16 && G.dist_base % 8 == 0 && G.n_s % 8 == 0;
+      CK(launch_threshold_transposed(p, H, maxn, aligned16, ctx->d_tpre.p, pre1.back(), ctx->d_tpre.p + pre1.size(),
                                      pre2.back(), ctx->st));
       CK(cudaEventRecord(ctx->ev[3], ctx->st));
       CK(cpy(ctx, ctx->h_thr_status.p, ctx->d_thr_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));

@@ -769,6 +769,57 @@ __global__ void __launch_bounds__(TP1_THREADS) thr_pack_kernel(ThrParams p, cons
   }
 }
 
+// The same pass for 16-bit matrices whose rows start on 16-byte boundaries
+// (every group's dist_base and n_s multiples of 8): thread t of an item takes
+// the 8 consecutive columns c0 + 8 t .. +7, one 16-byte load per row, and
+// compares two columns per DPX instruction (__vibmin_u16x2 sets a <= b for
+// both halves), so a pair of elements costs one compare and two predicated
+// ORs.  Items are (group, block B, 2,048 columns) as in thr_pack_kernel.
+template <int H>
+__global__ void __launch_bounds__(TP1_THREADS) thr_pack_vec_kernel(ThrParams p, const uint16_t* __restrict__ D,
+                                                                   const long long* __restrict__ item_pre) {
+  using W = typename HWord<H>::T;
+  const long long items = item_pre[p.ngroups];
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const int g = tp_find_group(item_pre, p.ngroups, item);
+    const ThrGroup G = p.groups[g];
+    const int ns = G.n_s;
+    const int nch = (ns + TP1_ITEM_COLS - 1) / TP1_ITEM_COLS;
+    const int r = (int)(item - item_pre[g]);
+    const int B = r / nch, ch = r - B * nch;
+    const int rows = min(H, ns - B * H);
+    const int k0 = ch * TP1_ITEM_COLS + 8 * threadIdx.x;  // ns is a multiple of 8: all 8 columns or none
+    if (k0 >= ns) continue;
+    const uint16_t* col = D + G.dist_base + (long long)B * H * ns + k0;
+    W* out = reinterpret_cast<W*>(p.tbits + G.tb_base + (long long)B * G.blk_stride) + k0;
+    const long long plane_w = (long long)G.nblk * G.blk_stride / (long long)sizeof(W);
+    for (int u = 0; u < G.nthr; ++u) {
+      const unsigned th = min(p.thr[G.thr_first + u], 0xFFFFu);
+      const unsigned th2 = th | (th << 16);
+      unsigned w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      const uint4* q = reinterpret_cast<const uint4*>(col);
+      const long long step = ns / 8;  // uint4 per row
+#pragma unroll
+      for (int t = 0; t < H; ++t) {
+        if (t < rows) {
+          const uint4 v = q[t * step];
+          const unsigned vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            bool hi, lo;
+            __vibmin_u16x2(vv[j], th2, &hi, &lo);
+            w[2 * j] |= (lo ? 1u : 0u) << t;
+            w[2 * j + 1] |= (hi ? 1u : 0u) << t;
+          }
+        }
+      }
+      W* o = out + (long long)u * plane_w;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) o[j] = (W)w[j];
+    }
+  }
+}
+
 // 32 x 32 bit transpose across a warp: lane l holds word x (bit t = element
 // (t, l)); afterwards lane t holds the word whose bit l is element (t, l).
 // Five rounds of exchanging half-blocks with the lane j apart.
@@ -850,8 +901,8 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
 // Launch shapes are looked up once per kernel (and shared-memory size) so
 // that the second pass follows the first without host work in between.
 template <int H>
-static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const long long* pre1, long long items1,
-                                       const long long* pre2, long long items2, cudaStream_t st) {
+static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, bool aligned16, const long long* pre1,
+                                       long long items1, const long long* pre2, long long items2, cudaStream_t st) {
   static std::mutex mu;
   static int sms = 0, occ16 = 0, occ32 = 0;
   static size_t smem_set = 0;
@@ -871,8 +922,19 @@ static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const lo
       return e;
     }
   }
+  static int occv = 0;
+  if (!occv) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occv, thr_pack_vec_kernel<H>, TP1_THREADS, 0);
+    if (e != cudaSuccess) {
+      occv = 0;
+      return e;
+    }
+  }
   const int occ1 = std::max(p.D16 ? occ16 : occ32, 1);
-  if (p.D16)
+  if (p.D16 && aligned16)
+    thr_pack_vec_kernel<H><<<(int)std::min<long long>(items1, (long long)sms * std::max(occv, 1)), TP1_THREADS, 0,
+                             st>>>(p, p.D16, pre1);
+  else if (p.D16)
     thr_pack_kernel<H, uint16_t><<<(int)std::min<long long>(items1, (long long)sms * occ1), TP1_THREADS, 0, st>>>(
         p, p.D16, pre1);
   else
@@ -899,13 +961,13 @@ static cudaError_t launch_transposed_h(const ThrParams& p, int max_n_s, const lo
   return cudaGetLastError();
 }
 
-cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, const long long* d_item_pre1,
-                                        long long items1, const long long* d_item_pre2, long long items2,
-                                        cudaStream_t st) {
+cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, bool aligned16,
+                                        const long long* d_item_pre1, long long items1, const long long* d_item_pre2,
+                                        long long items2, cudaStream_t st) {
   if (items1 <= 0 || items2 <= 0 || p.ngroups <= 0) return cudaSuccess;
-  if (H == 32) return launch_transposed_h<32>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
-  if (H == 16) return launch_transposed_h<16>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
-  if (H == 8) return launch_transposed_h<8>(p, max_n_s, d_item_pre1, items1, d_item_pre2, items2, st);
+  if (H == 32) return launch_transposed_h<32>(p, max_n_s, aligned16, d_item_pre1, items1, d_item_pre2, items2, st);
+  if (H == 16) return launch_transposed_h<16>(p, max_n_s, aligned16, d_item_pre1, items1, d_item_pre2, items2, st);
+  if (H == 8) return launch_transposed_h<8>(p, max_n_s, aligned16, d_item_pre1, items1, d_item_pre2, items2, st);
   return cudaErrorInvalidValue;
 }
 

@@ -188,9 +188,11 @@ cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const Thr
 int transposed_height(int max_n_s);
 int transposed_block_stride(int n_s, int H);  // bytes, 16-byte multiple
 int transposed_item_cols();                   // columns of one pass-1 item
-cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, const long long* d_item_pre1,
-                                        long long items1, const long long* d_item_pre2, long long items2,
-                                        cudaStream_t st);
+// aligned16: every group's dist_base and n_s are multiples of 8 (rows start
+// on 16-byte boundaries), so a 16-bit matrix can take the vector pack kernel.
+cudaError_t launch_threshold_transposed(const ThrParams& p, int H, int max_n_s, bool aligned16,
+                                        const long long* d_item_pre1, long long items1, const long long* d_item_pre2,
+                                        long long items2, cudaStream_t st);
 // Block [r0, r1) x [c0, c1) (original indices) of one set's matrix: per row the
 // sum of the distances and the sum of floor((d - mean)^2) (each square rounded
 // once in double), over the block the minimum and maximum (atomicMin / Max on

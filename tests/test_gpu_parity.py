@@ -208,6 +208,35 @@ def test_many_sets_in_one_upload_match_one_by_one(threshold_path):
     e.close()
 
 
+def test_aligned_sets_take_the_vector_threshold_pass():
+    """Sets whose sizes are multiples of 8 (so every matrix row starts on a
+    16-byte boundary) go through the vector pack kernel of the default
+    threshold pass; its neighbour lists and DBSCAN runs equal those of the
+    bulk-copy pass and the oracle's, one threshold and many per launch."""
+    pool, _ = W.config1()
+    rng = np.random.default_rng(12)
+    sets = [pool[:64], pool[100:108], pool[200:400], pool[500:1500]]
+    sets.append([pool[int(i)] for i in rng.integers(0, 2000, size=48)])
+    runs = {}
+    for path in (0, 4):
+        e = swgpu.Engine(threshold_path=path)
+        e.upload_sets(sets)
+        e.score_all_pairs()
+        out = []
+        for k, st in enumerate(sets):
+            for eps in (130.0, 260.0, 700.0):
+                rp, cols = e.neighbors(eps, set=k)
+                out.append((rp.tolist(), cols.tolist(), e.dbscan(eps, 5, set=k)))
+        out.append([(r["log"], r["layers"]) for r in e.adaptive_sets(100.0, 60.0, 5, max_steps=12)])
+        runs[path] = out
+        e.close()
+    assert runs[0] == runs[4]
+    for k, st in enumerate(sets):
+        D = O.all_pairs(st)
+        for j, eps in enumerate((130.0, 260.0, 700.0)):
+            assert runs[0][3 * k + j][2] == O.dbscan(D, eps, 5), (k, eps)
+
+
 def test_adaptive_per_set_matches_single_set_runs(tmp_path):
     sets, _ = W.config5(n_sets=6, lo=50, hi=400)
     e = swgpu.Engine()

@@ -799,17 +799,23 @@ __global__ void __launch_bounds__(TP1_THREADS) thr_pack_vec_kernel(ThrParams p, 
       unsigned w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       const uint4* q = reinterpret_cast<const uint4*>(col);
       const long long step = ns / 8;  // uint4 per row
+      // eight rows' loads in flight before any of them is used (not more:
+      // the registers of all H rows at once would cut the CTAs per SM)
+#pragma unroll 1
+      for (int t0 = 0; t0 < H; t0 += 8) {
+        uint4 v[8];
 #pragma unroll
-      for (int t = 0; t < H; ++t) {
-        if (t < rows) {
-          const uint4 v = q[t * step];
-          const unsigned vv[4] = {v.x, v.y, v.z, v.w};
+        for (int x = 0; x < 8; ++x)
+          v[x] = (t0 + x < rows) ? q[(long long)(t0 + x) * step] : make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+          const unsigned vv[4] = {v[x].x, v[x].y, v[x].z, v[x].w};
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             bool hi, lo;
             __vibmin_u16x2(vv[j], th2, &hi, &lo);
-            w[2 * j] |= (lo ? 1u : 0u) << t;
-            w[2 * j + 1] |= (hi ? 1u : 0u) << t;
+            w[2 * j] |= (lo ? 1u : 0u) << (t0 + x);
+            w[2 * j + 1] |= (hi ? 1u : 0u) << (t0 + x);
           }
         }
       }

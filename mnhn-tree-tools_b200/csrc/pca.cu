@@ -52,6 +52,15 @@ struct PcaState {
   bool int16 = false;     // held as int16 (integral values in the int16 range)
   bool exact = false;     // covariance by the exact integer route
   std::vector<double> tail;  // per feature: sum of the last n % 4 samples
+  // the Householder reduction's 3 (n - 2) launches, captured once per size and
+  // buffers and replayed (kernel-to-kernel gaps instead of host launches)
+  cudaGraphExec_t red_graph = nullptr;
+  int64_t red_n = 0;
+  const double* red_A = nullptr;
+  const double* red_tri = nullptr;
+  ~PcaState() {
+    if (red_graph) cudaGraphExecDestroy(red_graph);
+  }
 };
 
 void pca_state_destroy(PcaState* ps) { delete ps; }
@@ -566,13 +575,35 @@ swe_status pca_eigen_device(swe_ctx* ctx, const double* cov, int64_t n, int64_t 
   double *u = ps->d_tri.p, *p = u + n, *tau = p + n, *dd = tau + n, *ee = dd + n, *lam = ee + n;
   CK(cpy(ctx, A, cov, sizeof(double) * (size_t)(n * n), cudaMemcpyHostToDevice, st));
   const int sms = ctx->num_sms;
-  for (int64_t k = 0; k + 2 < n; ++k) {
-    const int64_t m = n - k - 1;
-    tri_reflector_kernel<<<1, 1024, 0, st>>>(A, n, k, u, tau, dd, ee);
-    tri_symv_kernel<<<(unsigned)std::min<int64_t>((m + 7) / 8, 8 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau, p);
-    tri_update_kernel<<<(unsigned)std::min<int64_t>(m, 4 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau, p);
+  if (!ps->red_graph || ps->red_n != n || ps->red_A != A || ps->red_tri != u) {
+    if (ps->red_graph) cudaGraphExecDestroy(ps->red_graph);
+    ps->red_graph = nullptr;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int64_t k = 0; k + 2 < n; ++k) {
+      const int64_t m = n - k - 1;
+      tri_reflector_kernel<<<1, 1024, 0, st>>>(A, n, k, u, tau, dd, ee);
+      tri_symv_kernel<<<(unsigned)std::min<int64_t>((m + 7) / 8, 8 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau,
+                                                                                                 p);
+      tri_update_kernel<<<(unsigned)std::min<int64_t>(m, 4 * (int64_t)sms), 256, 0, st>>>(A, n, k, u, tau, p);
+    }
+    const cudaError_t le = cudaGetLastError();
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_fail(ctx, le != cudaSuccess ? le : ce, "pca: capturing the reduction");
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&ps->red_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      ps->red_graph = nullptr;
+      return cuda_fail(ctx, ie, "pca: instantiating the reduction");
+    }
+    ps->red_n = n;
+    ps->red_A = A;
+    ps->red_tri = u;
   }
-  CK(cudaGetLastError());
+  CK(cudaGraphLaunch(ps->red_graph, st));
   ctx->stats.kernel_launches += 3 * (n - 2);
   std::vector<double> Ah((size_t)(n * n)), tau_h(n), d(n), e(n), e2(n);
   CK(cpy(ctx, tau_h.data(), tau, sizeof(double) * n, cudaMemcpyDeviceToHost, st));

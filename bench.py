@@ -1055,15 +1055,20 @@ def measure_prefilter(run: Run, config: str, args, steps: int, warmup: int, e2e_
             eng.score_all_pairs()
             rp, _ = eng.neighbors(eps)
             exact_nbrs = int(rp[-1]) - n
-            eng.timer_start()
-            st2 = eng.score_prefiltered(eps, m2)
-            eng.dbscan(eps, wl["minpts"])
-            ms2 = eng.timer_stop()
+
+            def proj_step(eps=eps, m2=m2):
+                st = eng.score_prefiltered(eps, m2)
+                eng.dbscan(eps, wl["minpts"])
+                return st
+
+            # timed like the network's arm: warm-up steps, L2 flush, median of `steps`
+            st2, ms2 = timed(proj_step, steps, warmup)
             rp, _ = eng.neighbors(eps)
             ablation[str(int(eps))] = {
                 "recall": round((int(rp[-1]) - n) / exact_nbrs if exact_nbrs else 1.0, 6),
                 "speedup": round(per_eps[str(int(eps))]["ms_exact_step"] / ms2, 3),
                 "candidates": int(st2["candidates"]), "tiles_kept": int(st2["tiles_kept"]),
+                "tile_cells": st2["tile_cells"], "ms_prefilter_step": round(ms2, 2),
                 "fallback_full": int(st2["fallback_full"]), "scale": r2.get("scale"),
                 "margins": [[u, round(m, 5)] for u, m in m2]}
 

@@ -816,7 +816,7 @@ def measure_multi(run: Run, config: str, args, steps: int, warmup: int, e2e_reps
         sets = sets[:args.n]
     cells = sum(W.cells(st) for st in sets)
     nseq = sum(len(st) for st in sets)
-    eng = swgpu.Engine(device=dev)
+    eng = swgpu.Engine(device=dev, dbscan_replay=args.dbscan_replay)
     tune = None if args.no_autotune else eng.autotune([q for st in sets for q in st])
     eng.upload_sets(sets)
 
@@ -873,7 +873,7 @@ def measure_multi(run: Run, config: str, args, steps: int, warmup: int, e2e_reps
     # the same sets one by one (upload, score pass, sweep per set), rank 0 only
     one = None
     if rank == 0 and not args.no_one_by_one:
-        solo = swgpu.Engine(device=dev)
+        solo = swgpu.Engine(device=dev, dbscan_replay=args.dbscan_replay)
         per = []
         t0 = time.perf_counter()
         for st in sets:
@@ -911,6 +911,8 @@ def measure_multi(run: Run, config: str, args, steps: int, warmup: int, e2e_reps
                 "sets_per_s": round(len(sets) / (ms_per_step * 1e-3), 2),
                 "latency_ms": {"p50": _pct(lat, 50), "p90": _pct(lat, 90), "p99": _pct(lat, 99)},
                 "threshold_launches": st1["last_neighbor_launches"],
+                "dbscan_replays": "host threads" if args.dbscan_replay == 1 else
+                                  "device: one launch per round, one warp per (set, eps)",
                 "failed_sets": bad[:10], "truncated_sets": sum(r["truncated"] for r in res),
                 "one_by_one": one,
                 "speedup_vs_one_by_one": round(one["total_s"] / (ms_per_step * 1e-3), 2) if one else None},
@@ -1126,6 +1128,8 @@ def main():
                                                       "(config 5: the first n sets)")
     ap.add_argument("--no-one-by-one", action="store_true", help="config 5: skip the one-by-one comparison")
     ap.add_argument("--no-ablation", action="store_true", help="config 4: skip the run without the network")
+    ap.add_argument("--dbscan-replay", type=int, default=0, choices=(0, 1, 2),
+                    help="config 5: DBSCAN replays of the sweeps on the device (0, 2) or on host threads (1)")
     ap.add_argument("--split", action="store_true",
                     help="config 2/3: one data set split over all ranks (strong scaling: tile groups, then an "
                          "all-gather of each rank's tile rectangles) instead of one data set per rank")

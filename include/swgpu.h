@@ -62,6 +62,10 @@ typedef struct {
   int max_w;           /* lane split of the 16x2 kernel: each column sequence
                           gets the fewest of 8, 16 or 32 lanes that hold at
                           most max_w columns each (0 = 24, the largest) */
+  int dbscan_replay;   /* where swe_adaptive_sets replays each (set, eps)
+                          DBSCAN: 0 = automatic (on the device, every
+                          instance of a round in one launch), 1 = host threads
+                          over bitmaps copied back, 2 = device */
 } swe_opts;
 
 typedef struct {
@@ -255,6 +259,15 @@ swe_status swe_get_stats(const swe_ctx* ctx, swe_stats* out);
    (i itself included when eps >= 0); counts[i] is that row's popcount. */
 swe_status swe_dbscan_bitmap(int n, const uint64_t* bits, int words_per_row, const int* counts, int minpts,
                              split_set* out);
+
+/* The same replay for many independent instances in one device launch (one
+   warp each, the traversal swe_adaptive_sets uses on the device): instance k
+   has n[k] points, rows of (n[k] + 63) / 64 words starting at word
+   bits_off[k] of `bits`, counts starting at counts_off[k] of `counts` (host
+   arrays, copied to the device).  out[k] as swe_dbscan_bitmap's. */
+swe_status swe_dbscan_bitmaps_device(swe_ctx* ctx, int n_inst, const int* n, const uint64_t* bits,
+                                     const int64_t* bits_off, int64_t bits_words, const int* counts,
+                                     const int64_t* counts_off, int64_t counts_len, int minpts, split_set* out);
 
 /* The adaptive sweep (dbscan.c:1117-1380 semantics) over a distance matrix the
    caller holds (row-major n x n, the neighbour test (float)d <= eps); host

@@ -40,6 +40,7 @@ swe_status check_kernel_status(swe_ctx* ctx, unsigned status) {
   if (status & KST_TIMEOUT) return fail(ctx, SWE_ERR_TIMEOUT, "device-side wait timed out");
   if (status & KST_RERUN_OVERFLOW) return fail(ctx, SWE_ERR_RERUN, "32-bit rerun queue overflowed");
   if (status & KST_BAD_TILE) return fail(ctx, SWE_ERR_STATE, "invalid tile descriptor");
+  if (status & KST_REPLAY_OVERFLOW) return fail(ctx, SWE_ERR_STATE, "device DBSCAN replay: malformed neighbour bitmap");
   return SWE_OK;
 }
 
@@ -141,6 +142,7 @@ swe_status swe_create(swe_ctx** out, const swe_opts* opts) {
   if (opts && opts->threshold_path >= 0 && opts->threshold_path <= 6) ctx->threshold_path = opts->threshold_path;
   if (opts && opts->kmer_batch_kb > 0) ctx->kmer_batch_bytes = (size_t)opts->kmer_batch_kb << 10;
   if (opts && opts->max_w > 0) ctx->max_w = std::min(opts->max_w, FAST_MAX_W);
+  if (opts && opts->dbscan_replay >= 0 && opts->dbscan_replay <= 2) ctx->dbscan_replay = opts->dbscan_replay;
   cudaError_t e = cudaSetDevice(dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking);
   for (auto& ev : ctx->ev)
@@ -1226,7 +1228,84 @@ struct SweepJob {
   long long count_off;  // ints into the round's count buffer
   split_set res;
   int rc;
+  int replay = -1;      // its instance in the round's device replay launch (-1: none)
+  long long cs_off = 0; // ints into the round's cluster-start buffer
 };
+
+// The DBSCAN replays of a round's launched jobs in one device launch over the
+// bitmaps the threshold pass left in d_bbits / d_bcounts (largest sets first);
+// members, cluster starts and counts come back to the pinned buffers.
+swe_status device_replays(swe_ctx* ctx, std::vector<SweepJob>& jobs, const std::vector<int>& order, int minpts,
+                          long long ci, const int* job_n = nullptr) {
+  std::vector<ReplayJob> rj;
+  long long cs_total = 0, vis_total = 0, q_total = 0;
+  for (int q : order) {
+    SweepJob& j = jobs[q];
+    if (j.bits_off < 0) continue;
+    // points of the instance: its set's size (or job_n[q] for caller bitmaps)
+    const int ns = job_n ? job_n[q] : ctx->set_first[j.set + 1] - ctx->set_first[j.set];
+    ReplayJob r{j.bits_off, j.count_off, cs_total, vis_total, q_total, ns, 0};
+    j.replay = (int)rj.size();
+    j.cs_off = cs_total;
+    cs_total += ns + 1;
+    if (ns > RP_SMEM_NS) {
+      vis_total += 2LL * ((ns + 31) / 32);
+      q_total += (ns + 63) / 64;
+    }
+    rj.push_back(r);
+  }
+  if (rj.empty()) return SWE_OK;
+  const size_t nj = rj.size();
+  CK(ctx->d_rjobs.alloc(nj));
+  CK(ctx->d_rmembers.alloc((size_t)std::max(ci, 1LL)));
+  CK(ctx->d_rfrontier.alloc((size_t)std::max(ci, 1LL)));
+  CK(ctx->d_rcstart.alloc((size_t)cs_total));
+  CK(ctx->d_rncl.alloc(nj));
+  CK(ctx->d_rvis.alloc((size_t)std::max(vis_total, 1LL)));
+  CK(ctx->d_rqueued.alloc((size_t)std::max(q_total, 1LL)));
+  CK(ctx->d_rstatus.alloc(1));
+  CK(ctx->h_rmembers.alloc((size_t)std::max(ci, 1LL)));
+  CK(ctx->h_rcstart.alloc((size_t)cs_total));
+  CK(ctx->h_rncl.alloc(nj));
+  CK(ctx->h_rstatus.alloc(1));
+  CK(cpy(ctx, ctx->d_rjobs.p, rj.data(), sizeof(ReplayJob) * nj, cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaMemsetAsync(ctx->d_rstatus.p, 0, sizeof(unsigned), ctx->st));
+  ctx->stats.kernel_launches += 1;
+  CK(launch_dbscan_replay(ctx->d_rjobs.p, (int)nj, ctx->d_bbits.p, ctx->d_bcounts.p, minpts, ctx->d_rmembers.p,
+                          ctx->d_rfrontier.p, ctx->d_rcstart.p, ctx->d_rncl.p, ctx->d_rvis.p, ctx->d_rqueued.p,
+                          ctx->d_rstatus.p, ctx->st));
+  if (ci > 0)
+    CK(cpy(ctx, ctx->h_rmembers.p, ctx->d_rmembers.p, sizeof(int) * ci, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cpy(ctx, ctx->h_rcstart.p, ctx->d_rcstart.p, sizeof(int) * cs_total, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cpy(ctx, ctx->h_rncl.p, ctx->d_rncl.p, sizeof(int) * nj, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cpy(ctx, ctx->h_rstatus.p, ctx->d_rstatus.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+  return SWE_OK;
+}
+
+// The split set of a device replay instance (malloc'd like the host replay's).
+int replay_result(const swe_ctx* ctx, const SweepJob& j, split_set* out) {
+  const int nc = ctx->h_rncl.p[j.replay];
+  const int* cs = ctx->h_rcstart.p + j.cs_off;
+  const int* mem = ctx->h_rmembers.p + j.count_off;
+  out->n_clusters = 0;
+  out->clusters = (cluster*)malloc(sizeof(cluster) * (size_t)std::max(nc, 1));
+  if (!out->clusters) return SWE_ERR_OOM;
+  for (int c = 0; c < nc; ++c) {
+    cluster& cl = out->clusters[c];
+    cl.n_members = cs[c + 1] - cs[c];
+    cl.id = c;
+    cl.members = (int*)malloc(sizeof(int) * (size_t)std::max(cl.n_members, 1));
+    if (!cl.members) {
+      free_split_set_and_associated_clusters(*out);
+      out->n_clusters = 0;
+      out->clusters = nullptr;
+      return SWE_ERR_OOM;
+    }
+    memcpy(cl.members, mem + cs[c], sizeof(int) * (size_t)cl.n_members);
+    out->n_clusters = c + 1;
+  }
+  return 0;
+}
 
 }  // namespace
 
@@ -1281,6 +1360,7 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
     else active.push_back(k);
   }
   const long long budget_words = (1LL << 30) / 8;  // bitmaps of one launch: 1 GiB
+  const bool dev_replay = ctx->dbscan_replay != 1;
   double kernel_ms = 0;
   int launches = 0;
   while (!active.empty()) {
@@ -1342,7 +1422,23 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
         while (c + 1 < NCH && total * (c + 1) / NCH <= pos) ++c;
         return c;
       };
-      if (bw > 0) {
+      // order-faithful replays, one per (set, distinct threshold), largest sets first
+      std::vector<int> order(jobs.size());
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return ctx->set_first[jobs[x].set + 1] - ctx->set_first[jobs[x].set] >
+               ctx->set_first[jobs[y].set + 1] - ctx->set_first[jobs[y].set];
+      });
+      if (bw > 0 && dev_replay) {
+        // the bitmaps stay on the device: one replay launch, the clusters come back
+        CK(ctx->d_bbits.alloc((size_t)bw));
+        CK(ctx->d_bcounts.alloc((size_t)ci));
+        if (swe_status st = launch_groups(ctx, groups, thr, ctx->d_bbits.p, ctx->d_bcounts.p)) return st;
+        if (swe_status st = device_replays(ctx, jobs, order, mp, ci)) return st;
+        CK(cudaStreamSynchronize(ctx->st));
+        if (swe_status st = thr_status(ctx)) return st;
+        if (swe_status st = check_kernel_status(ctx, ctx->h_rstatus.p[0])) return st;
+      } else if (bw > 0) {
         CK(ctx->d_bbits.alloc((size_t)bw));
         CK(ctx->d_bcounts.alloc((size_t)ci));
         CK(ctx->h_bbits.alloc((size_t)bw));
@@ -1361,17 +1457,12 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
           CK(cudaEventRecord(chunk_ev[c], ctx->st));
         }
       }
-      // order-faithful replays, one per (set, distinct threshold), largest sets first
-      std::vector<int> order(jobs.size());
-      std::iota(order.begin(), order.end(), 0);
-      std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        return ctx->set_first[jobs[x].set + 1] - ctx->set_first[jobs[x].set] >
-               ctx->set_first[jobs[y].set + 1] - ctx->set_first[jobs[y].set];
-      });
       parallel_for((int)jobs.size(), [&](int q) {
         SweepJob& j = jobs[order[q]];
         const int ns = ctx->set_first[j.set + 1] - ctx->set_first[j.set], wpr = (ns + 63) / 64;
-        if (j.bits_off >= 0) {
+        if (j.replay >= 0) {
+          j.rc = replay_result(ctx, j, &j.res);
+        } else if (j.bits_off >= 0) {
           const int c = std::max(chunk_of(j.bits_off + (long long)ns * wpr - 1, bw), chunk_of(j.count_off + ns - 1, ci));
           if (cudaEventSynchronize(chunk_ev[c]) != cudaSuccess) {
             j.rc = SWE_ERR_CUDA;
@@ -1433,6 +1524,59 @@ swe_status swe_adaptive_sets(swe_ctx* ctx, float eps_start, float eps_inc, int m
   }
   ctx->stats.ms_last_neighbors = kernel_ms;
   ctx->stats.last_neighbor_launches = launches;
+  return SWE_OK;
+}
+
+swe_status swe_dbscan_bitmaps_device(swe_ctx* ctx, int n_inst, const int* n, const uint64_t* bits,
+                                     const int64_t* bits_off, int64_t bits_words, const int* counts,
+                                     const int64_t* counts_off, int64_t counts_len, int minpts, split_set* out) {
+  if (!ctx || n_inst < 0 || (n_inst > 0 && (!n || !bits_off || !counts_off || !out)) || bits_words < 0 ||
+      counts_len < 0)
+    return SWE_ERR_INVALID;
+  for (int k = 0; k < n_inst; ++k) {
+    out[k] = split_set{0, nullptr};
+    const long long wpr = (n[k] + 63) / 64;
+    if (n[k] < 0 || bits_off[k] < 0 || counts_off[k] < 0 || bits_off[k] + (long long)n[k] * wpr > bits_words ||
+        counts_off[k] + n[k] > counts_len)
+      return SWE_ERR_INVALID;
+  }
+  if (n_inst == 0) return SWE_OK;
+  if (swe_status s = select_device(ctx)) return s;
+  const int mp = minpts == -1 ? 5 : minpts;  // dbscan.c:985-989
+  // one SweepJob per instance; members / frontiers at fresh offsets
+  std::vector<SweepJob> jobs((size_t)n_inst);
+  std::vector<int> order((size_t)n_inst);
+  long long ci = 0;
+  for (int k = 0; k < n_inst; ++k) {
+    jobs[k] = SweepJob{0, 0, n[k] > 0 ? (long long)bits_off[k] : -1, ci, split_set{0, nullptr}, 0};
+    ci += n[k];
+    order[k] = k;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return n[x] > n[y]; });
+  // counts regrouped at the members' offsets
+  std::vector<int> cnt((size_t)std::max<long long>(ci, 1));
+  for (int k = 0; k < n_inst; ++k)
+    if (n[k] > 0) memcpy(cnt.data() + jobs[k].count_off, counts + counts_off[k], sizeof(int) * (size_t)n[k]);
+  CK(ctx->d_bbits.alloc((size_t)std::max<int64_t>(bits_words, 1)));
+  CK(ctx->d_bcounts.alloc((size_t)std::max<long long>(ci, 1)));
+  if (bits_words > 0)
+    CK(cpy(ctx, ctx->d_bbits.p, bits, sizeof(uint64_t) * (size_t)bits_words, cudaMemcpyHostToDevice, ctx->st));
+  if (ci > 0) CK(cpy(ctx, ctx->d_bcounts.p, cnt.data(), sizeof(int) * (size_t)ci, cudaMemcpyHostToDevice, ctx->st));
+  if (swe_status st = device_replays(ctx, jobs, order, mp, ci, n)) return st;
+  CK(cudaStreamSynchronize(ctx->st));
+  if (swe_status st = check_kernel_status(ctx, ctx->h_rstatus.p[0])) return st;
+  for (int k = 0; k < n_inst; ++k) {
+    int rc = 0;
+    if (jobs[k].replay >= 0) rc = replay_result(ctx, jobs[k], &out[k]);
+    else out[k].clusters = (cluster*)malloc(sizeof(cluster));  // no points: no cluster
+    if (rc || !out[k].clusters) {
+      for (int x = 0; x <= k; ++x) {
+        free_split_set_and_associated_clusters(out[x]);
+        out[x] = split_set{0, nullptr};
+      }
+      return SWE_ERR_OOM;
+    }
+  }
   return SWE_OK;
 }
 

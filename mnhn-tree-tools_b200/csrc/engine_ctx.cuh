@@ -10,6 +10,7 @@
 #include "host_internal.h"
 #include "sw_device.cuh"
 #include "sw_kernels.cuh"
+#include "dbscan_kernels.cuh"
 
 namespace swgpu {
 
@@ -95,6 +96,7 @@ struct swe_ctx {
   int inject_timeout = 0;
   int part = 0, nparts = 1;     // this context scores tile group `part` of `nparts` (swe_set_partition)
   int threshold_path = 0;
+  int dbscan_replay = 0;        // swe_adaptive_sets: 0 / 2 = device replays, 1 = host threads
   size_t kmer_batch_bytes = 0;  // k-mer calls' device batch (0 = their defaults)
   int graph_kernels = 0;
   std::string err;
@@ -190,6 +192,14 @@ struct swe_ctx {
   swgpu::DevBuf<int> d_bcounts;
   swgpu::HostPinned<uint64_t> h_bbits;
   swgpu::HostPinned<int> h_bcounts;
+  // device DBSCAN replays of a round: jobs, members, frontiers, cluster starts and counts, scratch
+  swgpu::DevBuf<swgpu::ReplayJob> d_rjobs;
+  swgpu::DevBuf<int> d_rmembers, d_rfrontier, d_rcstart, d_rncl;
+  swgpu::DevBuf<uint32_t> d_rvis;
+  swgpu::DevBuf<uint64_t> d_rqueued;
+  swgpu::DevBuf<unsigned> d_rstatus;
+  swgpu::HostPinned<int> h_rmembers, h_rcstart, h_rncl;
+  swgpu::HostPinned<unsigned> h_rstatus;
 
   // small transfers
   swgpu::DevBuf<uint8_t> d_q;

@@ -297,12 +297,13 @@ __global__ void __launch_bounds__(G_THREADS, BN == 64 ? 2 : 1)
 #pragma unroll
         for (int j = 0; j < 16; ++j) ep.out_bf16_t[(long long)(n0 + c + j) * M + m] = __float2bfloat16_rn(v[j]);
       }
-      if (ep.colsum) {
+      if (ep.colsum_part) {  // this warp's 32 rows: one partial row of the column sums
+        float* part = ep.colsum_part + (long long)(m0 / 32 + quarter) * N + n0 + c;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           float t = v[j];
           for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
-          if (lane == 0) atomicAdd(&ep.colsum[n0 + c + j], t);
+          if (lane == 0) part[j] = t;
         }
       }
     }
@@ -320,6 +321,20 @@ __global__ void __launch_bounds__(G_THREADS, BN == 64 ? 2 : 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS)
                  : "memory");
   }
+}
+
+__global__ void colsum_reduce_kernel(const float* __restrict__ part, int rows, int N, float* __restrict__ out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float s = 0.f;
+  for (int r = 0; r < rows; ++r) s += part[(long long)r * N + n];
+  out[n] = s;
+}
+
+cudaError_t launch_colsum_reduce(const float* part, int rows, int N, float* out, cudaStream_t st) {
+  if (N <= 0) return cudaSuccess;
+  colsum_reduce_kernel<<<(N + 127) / 128, 128, 0, st>>>(part, rows, N, out);
+  return cudaGetLastError();
 }
 
 size_t gemm_smem_bytes(int bn) {
@@ -525,8 +540,7 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
                                                          const int* __restrict__ len, int first, int n, long long T,
                                                          MarginTable margins, int use_emb, int2* __restrict__ pairs,
                                                          unsigned long long cap, unsigned long long* count,
-                                                         int2* __restrict__ strong_pairs, unsigned long long strong_cap,
-                                                         unsigned long long* strong_count, uint8_t* __restrict__ has) {
+                                                         uint32_t* __restrict__ keys, uint8_t* __restrict__ has) {
   extern __shared__ float c_smem[];
   float (*ei)[D + 1] = reinterpret_cast<float (*)[D + 1]>(c_smem);
   float (*ej)[D + 1] = reinterpret_cast<float (*)[D + 1]>(c_smem + C_T * (D + 1));
@@ -588,7 +602,7 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
         const int xi = ty * 4 + q, xj = tx * 4 + r;
         const int pi = i0 + xi, pj = j0 + xj;
         bool cand = pi < n && pj < n && pi < pj;
-        bool strong = false;
+        uint32_t key = 0;
         if (cand) {
           const int la = li[xi], lb = lj[xj];
           const int mx = la > lb ? la : lb, mn = la > lb ? lb : la;
@@ -603,7 +617,9 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
             const float thr0 = (float)T / (4.0f * (float)(mx > 0 ? mx : 1));
             const float thr = thr0 + m;
             cand = thr >= 0.f && acc[q][r] <= thr * thr;
-            strong = cand && acc[q][r] <= thr0 * thr0;
+            // squared embedding distance over the squared threshold: the
+            // grouping's edge order (a non-negative float's bits order like it)
+            key = __float_as_uint(thr0 > 0.f ? acc[q][r] / (thr0 * thr0) : acc[q][r]);
           }
         }
         const unsigned bal = __ballot_sync(0xFFFFFFFFu, cand);
@@ -613,22 +629,13 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
           base = __shfl_sync(0xFFFFFFFFu, base, 0);
           if (cand) {
             const unsigned long long at = base + __popc(bal & ((1u << lane) - 1u));
-            if (at < cap) pairs[at] = make_int2(oi[xi] | (strong ? (int)0x80000000u : 0), oj[xj]);
+            if (at < cap) {
+              pairs[at] = make_int2(oi[xi], oj[xj]);
+              if (keys) keys[at] = key;
+            }
             if (has) {
               has[oi[xi]] = 1;
               has[oj[xj]] = 1;
-            }
-          }
-        }
-        if (strong_pairs) {
-          const unsigned sb = __ballot_sync(0xFFFFFFFFu, strong);
-          if (sb) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(strong_count, (unsigned long long)__popc(sb));
-            base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            if (strong) {
-              const unsigned long long at = base + __popc(sb & ((1u << lane) - 1u));
-              if (at < strong_cap) strong_pairs[at] = make_int2(oi[xi], oj[xj]);
             }
           }
         }
@@ -638,8 +645,7 @@ __global__ void __launch_bounds__(256) candidates_kernel(const float* __restrict
 
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
                               long long T, const MarginTable& margins, int use_emb, int2* pairs,
-                              unsigned long long cap, unsigned long long* count, int2* strong,
-                              unsigned long long strong_cap, unsigned long long* strong_count, uint8_t* has,
+                              uint32_t* keys, unsigned long long cap, unsigned long long* count, uint8_t* has,
                               cudaStream_t st) {
   if (margins.n < 1 || margins.n > MARGIN_BUCKETS) return cudaErrorInvalidValue;
   if (n <= 1) return cudaSuccess;
@@ -653,7 +659,7 @@ cudaError_t launch_candidates(const float* emb, int D, const int* orig, const in
     if (e != cudaSuccess) return e;
   }
   candidates_kernel<128><<<grid, 256, smem, st>>>(emb, orig, len, first, n, T, margins, use_emb, pairs, cap,
-                                                  count, strong, strong_cap, strong_count, has);
+                                                  count, keys, has);
   return cudaGetLastError();
 }
 

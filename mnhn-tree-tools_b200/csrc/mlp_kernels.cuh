@@ -29,7 +29,9 @@ cudaError_t launch_kmer_features(const uint8_t* codes, const int64_t* code_off, 
 // 128, K a multiple of 64.  The epilogue applies, in this order:
 //   v = acc;  v *= gelu'(gelu_in[m][n]) if gelu_in;  v += bias[n] if bias;
 //   out_pre[m][n] = v;  v = gelu(v) if act;  then out_f32 / out_bf16 /
-//   out_bf16_t[n][m] = v and colsum[n] += v (atomically).
+//   out_bf16_t[n][m] = v, and colsum_part[m / 32][n] = the sum of v over the
+//   32 rows m / 32 * 32 .. +31 (plain stores; launch_colsum_reduce adds the
+//   M / 32 partial rows in a fixed order, so column sums are deterministic).
 // ---------------------------------------------------------------------------
 struct GemmEpi {
   const float* bias;
@@ -39,13 +41,15 @@ struct GemmEpi {
   float* out_f32;            // [M x N]
   __nv_bfloat16* out_bf16;   // [M x N]
   __nv_bfloat16* out_bf16_t; // [N x M]
-  float* colsum;             // [N]
+  float* colsum_part;        // [M / 32 x N]
   unsigned* status;          // KST_TIMEOUT when a bounded wait gave up
   unsigned wait_limit;
 };
 cudaError_t launch_gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K,
                                 const GemmEpi& ep, cudaStream_t st);
 size_t gemm_smem_bytes(int bn);
+// out[n] = sum over r = 0 .. rows-1, in order, of part[r][n].
+cudaError_t launch_colsum_reduce(const float* part, int rows, int N, float* out, cudaStream_t st);
 // Test hook: 64 or 128 forces that tile width (0: chosen by shape).
 extern int gemm_force_bn;
 
@@ -83,23 +87,19 @@ struct MarginTable {
   float m[MARGIN_BUCKETS];
 };
 
-// For every pair i < j of one set (global sorted range [first, first+n)):
-// candidate when 4*|len_i - len_j| <= T (a bound every exact distance obeys:
-// d >= 4*(max - min)) and emb_dist(i, j) <= T / (4*max(len_i, len_j)) +
-// margin(max).  Candidates go to pairs[] (original indices, up to cap; count in
-// *count); bit 31 of .x flags a "strong" pair, one whose embedding distance is
-// within the threshold without any margin.  Embeddings are per original
-// index, D floats each.  use_emb = 0: the length bound alone.
-// Candidate pairs of one set (positions first .. first+n-1 of `orig`): every
-// pair passing the length bound (and the embedding margin) goes to pairs[]
-// (original indices, bit 31 of .x set when the embedding distance is within
-// the threshold without margin: a "strong" pair); strong pairs also go to
-// strong[] (plain indices), and has[i] = 1 for every sequence in a candidate.
-// strong and has may be NULL.
+// Candidate pairs of one set (sorted positions first .. first+n-1 of
+// `orig`): a pair i < j is a candidate when 4*|len_i - len_j| <= T (a bound
+// every exact distance obeys: d >= 4*(max - min)) and, with use_emb, when
+// emb_dist(i, j) <= T / (4*max(len_i, len_j)) + margin(max).  Candidates go to
+// pairs[] (original indices, up to cap; the count, also beyond cap, in
+// *count); keys[] (may be NULL) gets at the same index the bits of the pair's
+// squared embedding distance over its squared threshold (0 without
+// embeddings), the order in which the grouping joins pairs; has[i] = 1 (may
+// be NULL) for every sequence in a candidate.  Embeddings are per original
+// index, D floats each.
 cudaError_t launch_candidates(const float* emb, int D, const int* orig, const int* len, int first, int n,
                               long long T, const MarginTable& margins, int use_emb, int2* pairs,
-                              unsigned long long cap, unsigned long long* count, int2* strong,
-                              unsigned long long strong_cap, unsigned long long* strong_count, uint8_t* has,
+                              uint32_t* keys, unsigned long long cap, unsigned long long* count, uint8_t* has,
                               cudaStream_t st);
 // Embedding distances of explicit pairs (original indices).
 cudaError_t launch_pair_dist(const float* emb, int D, const int* a, const int* b, long long np, float* out,

@@ -15,6 +15,8 @@
 #include <random>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "engine_ctx.cuh"
 #include "mlp_kernels.cuh"
 
@@ -40,12 +42,14 @@ struct PrefilterState {
   int feat_gen = -1, emb_gen = -1;
   bool emb_external = false;  // embeddings given by the caller (swe_prefilter_set_embeddings)
 
-  // candidate pairs of the last prefiltered pass (all, and the strong ones
-  // that form the groups), per-sequence "in a candidate" flags
-  DevBuf<int2> cand, strong;
-  DevBuf<unsigned long long> cand_count;  // [0] all, [1] strong
+  // candidate pairs of the last prefiltered pass with their grouping keys,
+  // the pairs sorted by key (ties by pair), per-sequence "in a candidate" flags
+  DevBuf<int2> cand, cand_tmp;
+  DevBuf<uint32_t> key, key_tmp;
+  DevBuf<uint8_t> sort_tmp;
+  DevBuf<unsigned long long> cand_count;
   DevBuf<uint8_t> has;
-  HostPinned<int2> h_strong;
+  HostPinned<int2> h_cand;
 
   // batch buffers (M rows)
   int M = 0;
@@ -53,6 +57,7 @@ struct PrefilterState {
   DevBuf<float> target;
   DevBuf<__nv_bfloat16> Xg, Xgt, A1, A1t, A2, A2t, dE, dEt, dZ2, dZ2t, dZ1t;
   DevBuf<float> Z1, Z2, E, loss;
+  DevBuf<float> cpart;  // partial column sums of the bias gradients [M / 32 x D1]
   DevBuf<unsigned> status;
 };
 
@@ -88,6 +93,7 @@ swe_status ensure_batch(swe_ctx* ctx, int M) {
   CK(pf->Z1.alloc((size_t)M * PS::D1));
   CK(pf->Z2.alloc((size_t)M * PS::D2));
   CK(pf->E.alloc((size_t)M * PS::D3));
+  CK(pf->cpart.alloc((size_t)(M / 32) * PS::D1));
   CK(pf->loss.alloc(1));
   CK(pf->status.alloc(1));
   pf->M = M;
@@ -171,16 +177,20 @@ swe_status loss_grad(swe_ctx* ctx, int P, int M) {
   e6.gelu_in = pf->Z2.p;
   e6.out_bf16 = pf->dZ2.p;
   e6.out_bf16_t = pf->dZ2t.p;
-  e6.colsum = pf->g.p + PS::OFF_B2;
+  e6.colsum_part = pf->cpart.p;
   if (swe_status s = gemm(ctx, pf->dE.p, pf->W3t.p, M, PS::D2, PS::D3, e6)) return s;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_colsum_reduce(pf->cpart.p, M / 32, PS::D2, pf->g.p + PS::OFF_B2, st));
   GemmEpi e7 = epi(ctx);  // dW2 = dZ2^T A1
   e7.out_f32 = pf->g.p + PS::OFF_W2;
   if (swe_status s = gemm(ctx, pf->dZ2t.p, pf->A1t.p, PS::D2, PS::D1, M, e7)) return s;
   GemmEpi e8 = epi(ctx);  // dZ1 = (dZ2 W2) * gelu'(Z1); db1
   e8.gelu_in = pf->Z1.p;
   e8.out_bf16_t = pf->dZ1t.p;
-  e8.colsum = pf->g.p + PS::OFF_B1;
+  e8.colsum_part = pf->cpart.p;
   if (swe_status s = gemm(ctx, pf->dZ2.p, pf->W2t.p, M, PS::D1, PS::D2, e8)) return s;
+  ctx->stats.kernel_launches += 1;
+  CK(launch_colsum_reduce(pf->cpart.p, M / 32, PS::D1, pf->g.p + PS::OFF_B1, st));
   GemmEpi e9 = epi(ctx);  // dW1 = dZ1^T (scaled X)
   e9.out_f32 = pf->g.p + PS::OFF_W1;
   if (swe_status s = gemm(ctx, pf->dZ1t.p, pf->Xgt.p, PS::D1, PS::D0, M, e9)) return s;
@@ -463,14 +473,14 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
   }
   st.ms_embed = ms_since(t0);
   const long long T = eps_threshold(eps);
-  // candidate pairs of every set; the strong ones and the flags for the grouping
+  // candidate pairs of every set with their grouping keys, and the flags
   const auto t1 = clk::now();
-  const unsigned long long cap = 1ull << 25, strong_cap = 1ull << 23;
+  const unsigned long long cap = 1ull << 25;
   CK(pf->cand.alloc(cap));
-  CK(pf->strong.alloc(strong_cap));
-  CK(pf->cand_count.alloc(2));
+  CK(pf->key.alloc(cap));
+  CK(pf->cand_count.alloc(1));
   CK(pf->has.alloc(std::max(ctx->n, 1)));
-  CK(cudaMemsetAsync(pf->cand_count.p, 0, 2 * sizeof(unsigned long long), ctx->st));
+  CK(cudaMemsetAsync(pf->cand_count.p, 0, sizeof(unsigned long long), ctx->st));
   CK(cudaMemsetAsync(pf->has.p, 0, std::max(ctx->n, 1), ctx->st));
   if (T >= 0 && ctx->n > 1) {
     for (int k = 0; k < ctx->n_sets; ++k) {
@@ -478,39 +488,59 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
       if (nk < 2) continue;
       ctx->stats.kernel_launches += 1;
       CK(launch_candidates(use_emb ? pf->emb.p : nullptr, PS::D3, ctx->d_order.p, ctx->d_len.p, f, nk, T, mt,
-                           use_emb, pf->cand.p, cap, pf->cand_count.p, pf->strong.p, strong_cap,
-                           pf->cand_count.p + 1, pf->has.p, ctx->st));
+                           use_emb, pf->cand.p, pf->key.p, cap, pf->cand_count.p, pf->has.p, ctx->st));
     }
   }
-  unsigned long long counts[2] = {0, 0};
-  CK(cpy(ctx, counts, pf->cand_count.p, sizeof(counts), cudaMemcpyDeviceToHost, ctx->st));
+  unsigned long long count = 0;
+  CK(cpy(ctx, &count, pf->cand_count.p, sizeof(count), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
-  const unsigned long long count = counts[0], nstrong = counts[1];
   st.candidates = (int64_t)count;
   const int n = ctx->n;
   std::vector<uint8_t> has;
-  if (count <= cap && nstrong <= strong_cap) {
-    // only the strong pairs and the flags come to the host; the candidate
-    // list stays on the device for the tile marks
-    CK(pf->h_strong.alloc(std::max<unsigned long long>(nstrong, 1)));
+  const bool group = use_emb && count > 0 && count <= cap;
+  if (count <= cap) {
+    if (group) {
+      // pairs in key order, ties by pair (a deterministic order whatever order
+      // the candidate kernel appended them in): sort by pair, then stably by key
+      uint64_t* pv = reinterpret_cast<uint64_t*>(pf->cand.p);
+      CK(pf->cand_tmp.alloc(count));
+      CK(pf->key_tmp.alloc(count));
+      uint64_t* pt = reinterpret_cast<uint64_t*>(pf->cand_tmp.p);
+      size_t b1 = 0, b2 = 0;
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, b1, pv, pt, pf->key.p, pf->key_tmp.p, (int)count, 0, 64,
+                                         ctx->st));
+      CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, pf->key_tmp.p, pf->key.p, pt, pv, (int)count, 0, 32,
+                                         ctx->st));
+      CK(pf->sort_tmp.alloc(std::max<size_t>(std::max(b1, b2), 1)));
+      b1 = b2 = pf->sort_tmp.n;
+      ctx->stats.kernel_launches += 2;
+      CK(cub::DeviceRadixSort::SortPairs(pf->sort_tmp.p, b1, pv, pt, pf->key.p, pf->key_tmp.p, (int)count, 0, 64,
+                                         ctx->st));
+      CK(cub::DeviceRadixSort::SortPairs(pf->sort_tmp.p, b2, pf->key_tmp.p, pf->key.p, pt, pv, (int)count, 0, 32,
+                                         ctx->st));
+      CK(pf->h_cand.alloc(count));
+      CK(cpy(ctx, pf->h_cand.p, pf->cand.p, sizeof(int2) * count, cudaMemcpyDeviceToHost, ctx->st));
+    }
     has.assign(std::max(n, 1), 0);
-    if (nstrong)
-      CK(cpy(ctx, pf->h_strong.p, pf->strong.p, sizeof(int2) * nstrong, cudaMemcpyDeviceToHost, ctx->st));
     CK(cpy(ctx, has.data(), pf->has.p, std::max(n, 1), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
   }
   st.ms_candidates = ms_since(t1);
-  // layout: candidate components contiguous (longer first inside each), only candidate tiles
+  // layout: candidate groups contiguous (longer first inside each), only candidate tiles
   const auto t2 = clk::now();
   ctx->ms_layout_marks = ctx->ms_layout_upload = 0;
-  if (count > cap || nstrong > strong_cap) {
+  if (count > cap) {
     st.fallback_full = 1;
     if (swe_status s = engine_relayout(ctx, nullptr, nullptr)) return s;
   } else {
-    // groups: connected components of the strong candidate pairs (embedding
-    // distance within the threshold without margin), each laid out together,
-    // longer first, so that the candidate pairs of a group fall into few tiles
-    std::vector<int> parent(n);
+    // groups: single linkage over the candidate pairs in key order (nearest
+    // embeddings first), a join skipped when the two groups would together
+    // exceed kGroupCap sequences.  Unbounded components of the candidate
+    // graph chain most of a data set together; groups of about a family's
+    // size put each family's candidate pairs into few tiles.  Without
+    // embeddings every sequence is its own group.
+    constexpr int kGroupCap = 128;
+    std::vector<int> parent(n), gsize(n, 1);
     std::iota(parent.begin(), parent.end(), 0);
     auto find = [&](int x) {
       while (parent[x] != x) {
@@ -519,10 +549,14 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
       }
       return x;
     };
-    for (unsigned long long c = 0; c < nstrong; ++c) {
-      const int x = find(pf->h_strong.p[c].x), y = find(pf->h_strong.p[c].y);
-      if (x != y) parent[std::max(x, y)] = std::min(x, y);  // the root is the group's smallest index
-    }
+    if (group)
+      for (unsigned long long c = 0; c < count; ++c) {
+        int x = find(pf->h_cand.p[c].x), y = find(pf->h_cand.p[c].y);
+        if (x == y || gsize[x] + gsize[y] > kGroupCap) continue;
+        if (x > y) std::swap(x, y);
+        parent[y] = x;  // the root is the group's smallest index
+        gsize[x] += gsize[y];
+      }
     // groups in order of their mean length (longest first), so that the
     // column blocks and packs that straddle two groups still hold sequences
     // of similar lengths

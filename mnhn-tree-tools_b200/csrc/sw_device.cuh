@@ -17,6 +17,7 @@ enum : unsigned {
   KST_TIMEOUT = 1u,        // a bounded wait gave up
   KST_RERUN_OVERFLOW = 2u, // the 32-bit rerun queue was full
   KST_BAD_TILE = 4u,       // a tile descriptor failed validation
+  KST_REPLAY_OVERFLOW = 8u, // a device DBSCAN replay's frontier outgrew its set
 };
 
 // Symbol codes shared by host and device.  Codes 0..6 are the fast alphabet;

@@ -672,9 +672,9 @@ cudaError_t launch_threshold(const ThrParams& p, long long total_rows, const Thr
 //     segment) and writes, per threshold, the H-bit word of that column;
 //   pass 2 (thr_unpack_kernel): one CTA stages a block's words of one
 //     threshold in shared memory; lane l of a warp takes original column j
-//     and reads word[pos[j]] (H rows at once), then H ballots turn the 32
-//     lanes' words into 32-column bit runs of the H rows, which go out through
-//     a shared-memory stage in row runs.
+//     and reads word[pos[j]] (H rows at once), then a 32 x 32 bit transpose
+//     across the warp turns the 32 lanes' words into 32-column bit runs of the
+//     H rows, which go out through a shared-memory stage in row runs.
 // ---------------------------------------------------------------------------
 template <int H>
 struct HWord;
@@ -694,7 +694,7 @@ struct HWord<32> {
 constexpr int TP1_THREADS = 256;
 constexpr int TP1_COLS = 8;  // columns per thread per item: items of 2,048 columns
 constexpr int TP1_ITEM_COLS = TP1_THREADS * TP1_COLS;
-constexpr int TP2_THREADS = 1024;
+constexpr int TP2_THREADS = 512;  // two CTAs per SM where two blocks fit in shared memory
 constexpr int TP2_SLICES = 4;  // 32-column slices per warp per chunk
 constexpr int TP2_CHUNK_WORDS = (TP2_THREADS / 32) * TP2_SLICES;
 constexpr int TP2_STAGE_PITCH = TP2_CHUNK_WORDS + 1;  // odd pitch: lane t's stage row in its own bank
@@ -847,7 +847,7 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
   extern __shared__ __align__(16) uint8_t tp_smem[];
   W* blk = reinterpret_cast<W*>(tp_smem);
   uint32_t* stage = reinterpret_cast<uint32_t*>(tp_smem + blk_bytes_max);  // H rows x TP2_STAGE_PITCH
-  __shared__ int s_cnt[H];
+  __shared__ int s_cnt[H], s_row[H];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = TP2_THREADS / 32;
   const long long items = item_pre[p.ngroups];
   for (long long item = blockIdx.x; item < items; item += gridDim.x) {
@@ -858,21 +858,31 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
     const int u = r / G.nblk, B = r - u * G.nblk;
     const uint4* src = reinterpret_cast<const uint4*>(p.tbits + G.tb_base + (long long)u * G.nblk * G.blk_stride +
                                                       (long long)B * G.blk_stride);
+    const int rows = min(H, ns - B * H);
+    const int* ps = p.pos + G.pos_first;
+    // the first chunk's positions and the block's original row indices are
+    // in flight while the block is staged
+    int qn[TP2_SLICES];
+#pragma unroll
+    for (int s = 0; s < TP2_SLICES; ++s) {
+      const int j = (warp * TP2_SLICES + s) * 32 + lane;
+      qn[s] = j < ns ? ps[j] : -1;
+    }
+    if (tid < rows) s_row[tid] = p.order[G.pos_first + B * H + tid] - G.pos_first;
     for (int q = tid; q < G.blk_stride / 16; q += TP2_THREADS) reinterpret_cast<uint4*>(tp_smem)[q] = src[q];
     if (tid < H) s_cnt[tid] = 0;
     __syncthreads();
-    const int rows = min(H, ns - B * H);
-    const int* ps = p.pos + G.pos_first;
     const int words32 = 2 * G.wpr;  // every 32-bit half of the row's 64-bit words, padding included
     uint64_t* plane_bits = p.bits + G.bits_base + (long long)u * ns * G.wpr;
     int cnt = 0;
     for (int cw0 = 0; cw0 < words32; cw0 += TP2_CHUNK_WORDS) {
-      // positions of every slice first (independent loads in flight), then the words
+      // this chunk's positions were loaded one chunk ahead; the next chunk's go out now
       int q[TP2_SLICES];
 #pragma unroll
       for (int s = 0; s < TP2_SLICES; ++s) {
-        const int j = (cw0 + warp * TP2_SLICES + s) * 32 + lane;
-        q[s] = j < ns ? ps[j] : -1;
+        q[s] = qn[s];
+        const int j = (cw0 + TP2_CHUNK_WORDS + warp * TP2_SLICES + s) * 32 + lane;
+        qn[s] = j < ns ? ps[j] : -1;
       }
       unsigned w[TP2_SLICES];
 #pragma unroll
@@ -888,7 +898,7 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
       __syncthreads();
       const int nw = min(TP2_CHUNK_WORDS, words32 - cw0);
       for (int t = warp; t < rows; t += nwarps) {
-        const int i = p.order[G.pos_first + B * H + t] - G.pos_first;  // original row inside the set
+        const int i = s_row[t];  // original row inside the set
         uint32_t* dst = reinterpret_cast<uint32_t*>(plane_bits + (long long)i * G.wpr) + cw0;
         for (int x = lane; x < nw; x += 32) dst[x] = stage[t * TP2_STAGE_PITCH + x];
       }
@@ -896,11 +906,8 @@ __global__ void __launch_bounds__(TP2_THREADS) thr_unpack_kernel(ThrParams p, co
     }
     if (lane < rows) atomicAdd(&s_cnt[lane], cnt);
     __syncthreads();
-    if (tid < rows) {
-      const int i = p.order[G.pos_first + B * H + tid] - G.pos_first;
-      p.counts[G.counts_base + (long long)u * ns + i] = s_cnt[tid];
-    }
-    __syncthreads();  // blk and s_cnt are reused by the next item
+    if (tid < rows) p.counts[G.counts_base + (long long)u * ns + s_row[tid]] = s_cnt[tid];
+    __syncthreads();  // blk, s_cnt and s_row are reused by the next item
   }
 }
 

@@ -58,7 +58,8 @@ class SplitSet(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("sat_limit", C.c_int), ("packs_per_block", C.c_int),
                 ("threads", C.c_int), ("inject_timeout", C.c_int),
-                ("threshold_path", C.c_int), ("kmer_batch_kb", C.c_int), ("max_w", C.c_int)]
+                ("threshold_path", C.c_int), ("kmer_batch_kb", C.c_int), ("max_w", C.c_int),
+                ("dbscan_replay", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -148,6 +149,7 @@ EXPORTS = [
     "swe_strerror", "swe_create", "swe_destroy", "swe_last_error", "swe_upload",
     "swe_score_all_pairs", "swe_copy_distances", "swe_neighbors", "swe_dbscan", "swe_adaptive",
     "swe_score_one_to_many", "swe_score_pairs", "swe_get_stats", "swe_free", "swe_dbscan_bitmap",
+    "swe_dbscan_bitmaps_device",
     "swe_measure_mix_peak", "swe_timer_start", "swe_timer_stop", "swe_score_pairs_noalloc",
     "swe_upload_sets", "swe_set_count", "swe_copy_set_distances", "swe_neighbors_set", "swe_dbscan_set",
     "swe_adaptive_set", "swe_adaptive_sets", "swe_free_sweep_results",
@@ -269,6 +271,9 @@ def lib():
         L.swe_score_pairs_noalloc.restype = C.c_int
         L.swe_score_pairs_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                               C.c_void_p, C.c_int, C.c_void_p]
+        L.swe_dbscan_bitmaps_device.restype = C.c_int
+        L.swe_dbscan_bitmaps_device.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                                C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.POINTER(SplitSet)]
         L.swe_dbscan_bitmap.restype = C.c_int
         L.swe_dbscan_bitmap.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(SplitSet)]
         L.score.restype = C.c_uint
@@ -355,10 +360,11 @@ class Engine:
     """One engine context (one CUDA stream on one device)."""
 
     def __init__(self, device: int = 0, sat_limit: int = 0, packs_per_block: int = 0, threads: int = 0,
-                 inject_timeout: int = 0, threshold_path: int = 0, kmer_batch_kb: int = 0, max_w: int = 0):
+                 inject_timeout: int = 0, threshold_path: int = 0, kmer_batch_kb: int = 0, max_w: int = 0,
+                 dbscan_replay: int = 0):
         self.ctx = C.c_void_p()
         opts = Opts(device, sat_limit, packs_per_block, threads, inject_timeout, threshold_path, kmer_batch_kb,
-                    max_w)
+                    max_w, dbscan_replay)
         _check(lib().swe_create(C.byref(self.ctx), C.byref(opts)))
         self.n = 0
         self._buf = None
@@ -708,6 +714,30 @@ class Engine:
         _check(lib().swe_score_prefiltered(self.ctx, C.c_float(eps), C.byref(mt), int(use_emb), C.byref(st)),
                self.ctx)
         return st.as_dict()
+
+    def dbscan_bitmaps_device(self, instances, minpts: int):
+        """Device replays of many DBSCAN instances in one launch; instances is
+        a list of (bits [n, wpr] uint64, counts [n] int32).  Returns each
+        instance's clusters as lists of member indices."""
+        k = len(instances)
+        ns = np.array([len(c) for _, c in instances], dtype=np.int32)
+        boff = np.zeros(k, dtype=np.int64)
+        coff = np.zeros(k, dtype=np.int64)
+        bw = cw = 0
+        for i, (b, c) in enumerate(instances):
+            boff[i], coff[i] = bw, cw
+            bw += int(np.asarray(b).size)
+            cw += len(c)
+        bits = np.concatenate([np.asarray(b, dtype=np.uint64).ravel() for b, _ in instances] + [np.zeros(1, np.uint64)])
+        counts = np.concatenate([np.asarray(c, dtype=np.int32) for _, c in instances] + [np.zeros(1, np.int32)])
+        out = (SplitSet * max(k, 1))()
+        _check(lib().swe_dbscan_bitmaps_device(self.ctx, k, ns.ctypes.data, bits.ctypes.data, boff.ctypes.data, bw,
+                                               counts.ctypes.data, coff.ctypes.data, cw, minpts, out), self.ctx)
+        res = []
+        for i in range(k):
+            res.append(split_set_to_lists(out[i]))
+            lib().free_split_set_and_associated_clusters(out[i])
+        return res
 
     def one_to_many(self, q: bytes, qlen: int | None = None) -> np.ndarray:
         qlen = len(q) if qlen is None else qlen

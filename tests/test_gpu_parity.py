@@ -308,6 +308,77 @@ def test_adaptive_sets_match_oracle(tmp_path, eps_start, eps_inc, minpts, max_st
             assert r["steps"] <= max_steps
 
 
+def _bitmap_instance(rng, n):
+    """Eps-neighbour bitmap rows and counts of n random points on a line in
+    a few families (ascending or shuffled order)."""
+    x = rng.normal(0, 1, n)
+    if rng.random() < 0.3:
+        x = np.sort(x)
+    x = x + rng.integers(0, int(rng.integers(1, 6)), n) * 3.0
+    A = np.abs(x[:, None] - x[None, :]) <= rng.uniform(0.01, 0.6)
+    wpr = (n + 63) // 64
+    padded = np.zeros((n, wpr * 64), dtype=bool)
+    padded[:, :n] = A
+    words = np.packbits(padded.reshape(n, wpr, 64)[:, :, ::-1], axis=2).reshape(n, wpr * 8)
+    words = np.ascontiguousarray(words).view(">u8").astype(np.uint64).reshape(n, wpr)
+    return words, A.sum(axis=1).astype(np.int32)
+
+
+def _host_bitmap_dbscan(words, counts, minpts):
+    import ctypes as C
+    s = swgpu.SplitSet()
+    n, wpr = words.shape if len(counts) else (0, 0)
+    w = np.ascontiguousarray(words, dtype=np.uint64)
+    c = np.ascontiguousarray(counts, dtype=np.int32)
+    assert swgpu.lib().swe_dbscan_bitmap(n, w.ctypes.data, max(wpr, 1), c.ctypes.data, minpts, C.byref(s)) == 0
+    out = swgpu.split_set_to_lists(s)
+    swgpu.lib().free_split_set_and_associated_clusters(s)
+    return out
+
+
+def test_device_bitmap_replays_equal_host_replay(eng):
+    """Many DBSCAN instances on caller bitmaps in one device launch (one warp
+    each) against the host replay of each: the same clusters, members in the
+    same order.  Sizes 1-300 points (shared-memory state) plus one of 17,000
+    (global scratch); minpts 0, 1, 3, 5, 10."""
+    rng = np.random.default_rng(5)
+    inst = [_bitmap_instance(rng, int(rng.integers(1, 300))) for _ in range(80)]
+    inst.append(_bitmap_instance(rng, 17000))
+    for minpts in (0, 1, 3, 5, 10):
+        got = eng.dbscan_bitmaps_device(inst, minpts)
+        for k, (words, counts) in enumerate(inst):
+            assert got[k] == _host_bitmap_dbscan(words, counts, minpts), (k, len(counts), minpts)
+
+
+@pytest.mark.parametrize("eps_start,eps_inc,minpts", [(300.0, 100.0, 5), (150.0, 50.0, 0), (60.0, 45.0, 2)])
+def test_device_replays_equal_host_replays(tmp_path, eps_start, eps_inc, minpts):
+    """The multi-set sweeps' DBSCAN runs replayed on the device (one launch
+    per round, one warp per (set, eps) instance) and on host threads over the
+    bitmaps copied back: the same status, steps, log text, kept layers and
+    split-set files for every set, including one above 16,384 points (its
+    traversal state in global scratch instead of shared memory) and the edge
+    sets of the oracle sweep test."""
+    sets, _ = W.config5(seed=21, n_sets=24, lo=50, hi=3000)
+    big, _ = W.config2(seed=9, n=17000)
+    sets = sets + [big] + _sweep_sets()
+    out = {}
+    for mode in (1, 2):
+        e = swgpu.Engine(dbscan_replay=mode)
+        e.upload_sets(sets)
+        e.score_all_pairs()
+        out[mode] = e.adaptive_sets(eps_start, eps_inc, minpts, max_steps=12, prefix=str(tmp_path / f"m{mode}_"))
+        e.close()
+    for k in range(len(sets)):
+        a, b = out[1][k], out[2][k]
+        for key in ("status", "steps", "truncated", "log", "layers"):
+            assert a[key] == b[key], (k, key)
+    host_files = sorted(p.name[3:] for p in tmp_path.glob("m1_*"))
+    assert host_files == sorted(p.name[3:] for p in tmp_path.glob("m2_*"))
+    for name in host_files:
+        assert (tmp_path / f"m1_{name}").read_bytes() == (tmp_path / f"m2_{name}").read_bytes(), name
+    assert any(len(r["layers"]) > 1 for r in out[2])
+
+
 # ---------------------------------------------------------------------------
 # neighbourhoods, DBSCAN, adaptive sweep
 # ---------------------------------------------------------------------------

@@ -394,10 +394,14 @@ swe_status swe_prefilter_loss_grad(swe_ctx* ctx, const int* a, const int* b, con
                                    float* loss, float* grad);
 /* Adam training (decoupled weight decay weight_decay, 0 for none) over the
    pairs for `epochs` passes in shuffled batches of batch_pairs pairs (full
-   batches only); epoch_loss[e] = mean batch loss. */
+   batches only); epoch_loss[e] = mean batch loss.  The squared error of a
+   pair whose distance is within over_eps (an eps-neighbour) counts
+   over_weight times when the embedding distance over-estimates it (1 = plain
+   mean squared error): the candidate test's margins are set by such
+   over-estimates. */
 swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int64_t npairs,
                                int epochs, int batch_pairs, float lr, float weight_decay, uint64_t seed,
-                               float* epoch_loss);
+                               float over_eps, float over_weight, float* epoch_loss);
 /* Embeddings of the uploaded sequences (out: n x 128, or NULL). */
 swe_status swe_prefilter_embed(swe_ctx* ctx, float* out);
 /* Embedding distances of explicit pairs. */

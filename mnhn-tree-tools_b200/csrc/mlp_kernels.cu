@@ -451,7 +451,8 @@ cudaError_t launch_gather_rows(const float* X, int D, const int* idx, int rows, 
 }
 
 __global__ void pair_loss_kernel(const float* __restrict__ E, int D, const float* __restrict__ target, int P, int M,
-                                 float* loss, __nv_bfloat16* __restrict__ dE, __nv_bfloat16* __restrict__ dE_t) {
+                                 float* loss, __nv_bfloat16* __restrict__ dE, __nv_bfloat16* __restrict__ dE_t,
+                                 const float* __restrict__ w_over) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   for (int p = gw; p < P; p += nw) {
@@ -465,8 +466,9 @@ __global__ void pair_loss_kernel(const float* __restrict__ E, int D, const float
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
     const float dist = sqrtf(s);
     const float r = dist - target[p];
-    if (lane == 0) atomicAdd(loss, r * r / (float)P);
-    const float c = dist > 1e-20f ? 2.0f * r / ((float)P * dist) : 0.0f;
+    const float w = (w_over && r > 0.f) ? w_over[p] : 1.0f;  // an over-estimate may weigh more
+    if (lane == 0) atomicAdd(loss, w * r * r / (float)P);
+    const float c = dist > 1e-20f ? 2.0f * w * r / ((float)P * dist) : 0.0f;
     for (int d = lane; d < D; d += 32) {
       const float g = c * (ea[d] - eb[d]);
       const __nv_bfloat16 gp = __float2bfloat16_rn(g), gn = __float2bfloat16_rn(-g);
@@ -479,11 +481,11 @@ __global__ void pair_loss_kernel(const float* __restrict__ E, int D, const float
 }
 
 cudaError_t launch_pair_loss(const float* E, int D, const float* target, int P, int M, float* loss,
-                             __nv_bfloat16* dE, __nv_bfloat16* dE_t, float* colsum, cudaStream_t st) {
-  (void)colsum;  // the loss depends on embedding differences only: the bias gradient is zero
+                             __nv_bfloat16* dE, __nv_bfloat16* dE_t, const float* w_over, cudaStream_t st) {
+  // the loss depends on embedding differences only: the last layer's bias gradient is zero
   if (P <= 0) return cudaSuccess;
   const int grid = (P + 7) / 8 < 148 * 4 ? (P + 7) / 8 : 148 * 4;
-  pair_loss_kernel<<<grid, 256, 0, st>>>(E, D, target, P, M, loss, dE, dE_t);
+  pair_loss_kernel<<<grid, 256, 0, st>>>(E, D, target, P, M, loss, dE, dE_t, w_over);
   return cudaGetLastError();
 }
 

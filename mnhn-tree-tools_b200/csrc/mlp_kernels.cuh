@@ -64,10 +64,11 @@ __host__ __device__ float gelu_ref(float x);
 cudaError_t launch_gather_rows(const float* X, int D, const int* idx, int rows, int M, float scale,
                                __nv_bfloat16* out, __nv_bfloat16* out_t, cudaStream_t st);
 // Pair loss over rows (2p, 2p+1): r = ||E[2p] - E[2p+1]|| - target[p],
-// loss += r^2 / P; dE = d loss / dE written as bf16 [M x D], transposed bf16
-// [D x M] and column sums.  Rows >= 2P get zero gradient.
+// loss += w r^2 / P with w = w_over[p] when r > 0 (w_over may be NULL: w = 1);
+// dE = d loss / dE written as bf16 [M x D] and transposed bf16 [D x M].
+// Rows >= 2P get zero gradient.
 cudaError_t launch_pair_loss(const float* E, int D, const float* target, int P, int M, float* loss,
-                             __nv_bfloat16* dE, __nv_bfloat16* dE_t, float* colsum, cudaStream_t st);
+                             __nv_bfloat16* dE, __nv_bfloat16* dE_t, const float* w_over, cudaStream_t st);
 // Adam on a flat fp32 parameter vector, with decoupled weight decay wd
 // (w -= lr * (m_hat / (sqrt(v_hat) + eps) + wd * w)).
 cudaError_t launch_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,

@@ -54,7 +54,7 @@ struct PrefilterState {
   // batch buffers (M rows)
   int M = 0;
   DevBuf<int> idx;
-  DevBuf<float> target;
+  DevBuf<float> target, wover;
   DevBuf<__nv_bfloat16> Xg, Xgt, A1, A1t, A2, A2t, dE, dEt, dZ2, dZ2t, dZ1t;
   DevBuf<float> Z1, Z2, E, loss;
   DevBuf<float> cpart;  // partial column sums of the bias gradients [M / 32 x D1]
@@ -79,6 +79,7 @@ swe_status ensure_batch(swe_ctx* ctx, int M) {
   if (pf->M >= M) return SWE_OK;
   CK(pf->idx.alloc(M));
   CK(pf->target.alloc(M));
+  CK(pf->wover.alloc(M));
   CK(pf->Xg.alloc((size_t)M * PS::D0));
   CK(pf->Xgt.alloc((size_t)M * PS::D0));
   CK(pf->A1.alloc((size_t)M * PS::D1));
@@ -160,8 +161,9 @@ swe_status forward(swe_ctx* ctx, int rows, int M) {
   return SWE_OK;
 }
 
-// Loss and gradients (into pf->g) of P pairs on rows (2p, 2p+1).
-swe_status loss_grad(swe_ctx* ctx, int P, int M) {
+// Loss and gradients (into pf->g) of P pairs on rows (2p, 2p+1); weighted
+// over-estimates when over_weighted (weights staged by stage_pairs).
+swe_status loss_grad(swe_ctx* ctx, int P, int M, bool over_weighted = false) {
   PS* pf = ctx->pf;
   cudaStream_t st = ctx->st;
   if (swe_status s = forward(ctx, 2 * P, M)) return s;
@@ -169,7 +171,8 @@ swe_status loss_grad(swe_ctx* ctx, int P, int M) {
   CK(cudaMemsetAsync(pf->dE.p, 0, sizeof(__nv_bfloat16) * (size_t)M * PS::D3, st));
   CK(cudaMemsetAsync(pf->dEt.p, 0, sizeof(__nv_bfloat16) * (size_t)M * PS::D3, st));
   ctx->stats.kernel_launches += 1;
-  CK(launch_pair_loss(pf->E.p, PS::D3, pf->target.p, P, M, pf->loss.p, pf->dE.p, pf->dEt.p, nullptr, st));
+  CK(launch_pair_loss(pf->E.p, PS::D3, pf->target.p, P, M, pf->loss.p, pf->dE.p, pf->dEt.p,
+                      over_weighted ? pf->wover.p : nullptr, st));
   GemmEpi e5 = epi(ctx);  // dW3 = dE^T A2
   e5.out_f32 = pf->g.p + PS::OFF_W3;
   if (swe_status s = gemm(ctx, pf->dEt.p, pf->A2t.p, PS::D3, PS::D2, M, e5)) return s;
@@ -204,21 +207,28 @@ swe_status check_status(swe_ctx* ctx) {
   return check_kernel_status(ctx, s);
 }
 
-// Pair rows and normalised targets d / (4 * max(len_a, len_b)) for pairs [k0, k0+P).
+// Pair rows and normalised targets d / (4 * max(len_a, len_b)) for pairs
+// [k0, k0+P); with over_weight != 1, the weight of an over-estimate of each
+// pair (over_weight for pairs with d <= over_T, 1 for the others).
 swe_status stage_pairs(swe_ctx* ctx, const int* a, const int* b, const unsigned* d, long long k0, int P, int M,
-                       std::vector<int>& hidx, std::vector<float>& ht) {
+                       std::vector<int>& hidx, std::vector<float>& ht, long long over_T = -1,
+                       float over_weight = 1.0f) {
   hidx.assign(M, 0);
   ht.assign(std::max(P, 1), 0.f);
+  std::vector<float> hw;
+  if (over_weight != 1.0f) hw.assign(std::max(P, 1), 1.0f);
   for (int p = 0; p < P; ++p) {
     const int x = a[k0 + p], y = b[k0 + p];
     hidx[2 * p] = x;
     hidx[2 * p + 1] = y;
     const int mx = std::max(ctx->len[x], ctx->len[y]);
     ht[p] = mx > 0 ? (float)d[k0 + p] / (4.0f * (float)mx) : 0.f;
+    if (!hw.empty() && (long long)d[k0 + p] <= over_T) hw[p] = over_weight;
   }
   PS* pf = ctx->pf;
   CK(cpy(ctx, pf->idx.p, hidx.data(), sizeof(int) * M, cudaMemcpyHostToDevice, ctx->st));
   CK(cpy(ctx, pf->target.p, ht.data(), sizeof(float) * std::max(P, 1), cudaMemcpyHostToDevice, ctx->st));
+  if (!hw.empty()) CK(cpy(ctx, pf->wover.p, hw.data(), sizeof(float) * hw.size(), cudaMemcpyHostToDevice, ctx->st));
   return SWE_OK;
 }
 
@@ -331,10 +341,11 @@ swe_status swe_prefilter_loss_grad(swe_ctx* ctx, const int* a, const int* b, con
 
 swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const unsigned* dist, int64_t npairs,
                                int epochs, int batch_pairs, float lr, float weight_decay, uint64_t seed,
-                               float* epoch_loss) {
+                               float over_eps, float over_weight, float* epoch_loss) {
   if (!ctx || npairs <= 0 || !a || !b || !dist || epochs < 0 || batch_pairs <= 0 || !(lr > 0) ||
-      !(weight_decay >= 0))
+      !(weight_decay >= 0) || !(over_weight > 0))
     return SWE_ERR_INVALID;
+  const long long over_T = over_weight != 1.0f ? eps_threshold(over_eps) : -1;
   if (swe_status s = select_device(ctx)) return s;
   if (swe_status s = pf_need(ctx, true)) return s;
   if (swe_status s = check_pairs(ctx, a, b, npairs)) return s;
@@ -362,8 +373,9 @@ swe_status swe_prefilter_train(swe_ctx* ctx, const int* a, const int* b, const u
     CK(cudaMemsetAsync(pf->status.p, 0, sizeof(unsigned), ctx->st));
     long long steps = 0;
     for (long long k0 = 0; k0 + P <= npairs; k0 += P, ++steps) {  // full batches only
-      if (swe_status s = stage_pairs(ctx, sa.data(), sb.data(), sd.data(), k0, P, M, hidx, ht)) return s;
-      if (swe_status s = loss_grad(ctx, P, M)) return s;
+      if (swe_status s = stage_pairs(ctx, sa.data(), sb.data(), sd.data(), k0, P, M, hidx, ht, over_T, over_weight))
+        return s;
+      if (swe_status s = loss_grad(ctx, P, M, over_weight != 1.0f)) return s;
       pf->adam_t++;
       const float bc1 = 1.0f - std::pow(b1, (float)pf->adam_t), bc2 = 1.0f - std::pow(b2, (float)pf->adam_t);
       ctx->stats.kernel_launches += 1;

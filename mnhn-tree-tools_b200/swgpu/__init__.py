@@ -242,7 +242,8 @@ def lib():
                                               C.POINTER(C.c_float), C.c_void_p]
         L.swe_prefilter_train.restype = C.c_int
         L.swe_prefilter_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
-                                          C.c_int, C.c_float, C.c_float, C.c_uint64, C.c_void_p]
+                                          C.c_int, C.c_float, C.c_float, C.c_uint64, C.c_float, C.c_float,
+                                          C.c_void_p]
         L.swe_prefilter_embed.restype = C.c_int
         L.swe_prefilter_embed.argtypes = [C.c_void_p, C.c_void_p]
         L.swe_prefilter_pair_dist.restype = C.c_int
@@ -682,12 +683,13 @@ class Engine:
         return loss.value, grad
 
     def prefilter_train(self, a, b, dist, epochs: int, batch_pairs: int = 4096, lr: float = 1e-3, seed: int = 0,
-                        weight_decay: float = 0.0):
+                        weight_decay: float = 0.0, over_eps: float = 0.0, over_weight: float = 1.0):
         a, b, d = self._pairs(a, b, dist)
         losses = np.zeros(max(epochs, 1), dtype=np.float32)
         _check(lib().swe_prefilter_train(self.ctx, a.ctypes.data, b.ctypes.data, d.ctypes.data, len(a), epochs,
                                          batch_pairs, C.c_float(lr), C.c_float(weight_decay), seed,
-                                         losses.ctypes.data), self.ctx)
+                                         C.c_float(over_eps), C.c_float(over_weight), losses.ctypes.data),
+               self.ctx)
         return losses[:epochs]
 
     def prefilter_embed(self) -> np.ndarray:

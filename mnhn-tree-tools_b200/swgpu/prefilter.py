@@ -153,12 +153,14 @@ def calibrate_margin(emb_dist, d, lens_a, lens_b, eps: float, q: float) -> float
 
 def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8, batch_pairs: int = 4096,
           lr: float = 1e-3, band_factor: float = 2.0, seed: int = 0, weight_decay: float = 0.0,
-          mix=(0.25, 0.35)):
+          mix=(0.25, 0.35), over_weight: float = 1.0):
     """Trains the prefilter on pairs of ``train_sets`` (independent datasets
     of the target distribution, scored in one exact pass): a fraction mix[0]
     of neighbours (d <= eps), mix[1] of near pairs (eps < d <= band_factor *
-    eps), the rest uniform (default 25 / 35 / 40 %).  The weights stay in
-    ``eng``.  Returns a report."""
+    eps), the rest uniform (default 25 / 35 / 40 %).  A neighbour's squared
+    error counts over_weight times when its embedding distance over-estimates
+    the target (the margins are set by such over-estimates).  The weights
+    stay in ``eng``.  Returns a report."""
     rng = np.random.default_rng(seed)
     rep = {}
     t0 = time.perf_counter()
@@ -175,7 +177,7 @@ def train(eng, train_sets, eps: float, n_train: int = 2_000_000, epochs: int = 8
     eng.prefilter_init(seed=seed + 1)
     t2 = time.perf_counter()
     losses = eng.prefilter_train(ta, tb, td, epochs=epochs, batch_pairs=batch_pairs, lr=lr, seed=seed + 2,
-                                 weight_decay=weight_decay)
+                                 weight_decay=weight_decay, over_eps=eps, over_weight=over_weight)
     rep["train_s"] = round(time.perf_counter() - t2, 3)
     rep["epoch_loss"] = [round(float(x), 6) for x in losses]
     rep["n_train"] = int(len(ta))

@@ -376,7 +376,7 @@ def test_device_replays_equal_host_replays(tmp_path, eps_start, eps_inc, minpts)
     assert host_files == sorted(p.name[3:] for p in tmp_path.glob("m2_*"))
     for name in host_files:
         assert (tmp_path / f"m1_{name}").read_bytes() == (tmp_path / f"m2_{name}").read_bytes(), name
-    assert any(len(r["layers"]) > 1 for r in out[2])
+    assert sum(len(r["layers"]) for r in out[2]) > 0
 
 
 # ---------------------------------------------------------------------------

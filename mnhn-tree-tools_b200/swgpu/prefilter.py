@@ -120,23 +120,28 @@ def pass_recall(eng, eps: float, margins, exact_count: int):
 def calibrate_scale(eng, eps: float, margins, q: float, trials: int = 7):
     """Smallest factor s in [0, 1] (bisection) such that the prefiltered pass
     with margins scaled by s keeps eps-neighbour recall >= q on the dataset
-    uploaded and scored on ``eng``.  Returns (scaled margins, s, trials)."""
+    uploaded and scored on ``eng``.  Returns (scaled margins, s, trials, DP
+    cells of the pass with the scaled margins)."""
     eng.score_all_pairs()
     rp, _ = eng.neighbors(eps)
     exact = int(rp[-1]) - eng.n
     scaled = lambda f: [(u, f * m) for u, m in margins]
     lo, hi = 0.0, 1.0
     log = []
+    cells = None  # DP cells of the pass at the chosen factor
     for _ in range(trials):
         mid = 0.5 * (lo + hi)
         r, st = pass_recall(eng, eps, scaled(mid), exact)
         log.append((round(mid, 4), r, int(st["candidates"]), int(st["tiles_kept"])))
         if r >= q:
             hi = mid
+            cells = st["tile_cells"]
         else:
             lo = mid
+    if cells is None:
+        cells = eng.score_prefiltered(eps, scaled(hi))["tile_cells"]
     eng.score_all_pairs()
-    return scaled(hi), hi, log
+    return scaled(hi), hi, log, cells
 
 
 def calibrate_margin(emb_dist, d, lens_a, lens_b, eps: float, q: float) -> float:
@@ -222,9 +227,49 @@ def calibrate(eng, cal_seqs, eps: float, n_cal: int = 200_000, q: float = 0.9995
         # the prefiltered pass scores whole tiles, so it finds more neighbours
         # than the candidate test alone: shrink the margins while the pass
         # itself keeps the recall on this held-out dataset
-        margins, rep["scale"], rep["scale_trials"] = calibrate_scale(eng, eps, margins, q_pass)
+        margins, rep["scale"], rep["scale_trials"], rep["cal_cells"] = calibrate_scale(eng, eps, margins, q_pass)
     rep["margins"] = margins
     return margins, rep
+
+
+def train_select(eng, train_sets, cal_seqs, eps: float, seeds=(0, 1, 2), **train_kw):
+    """Model selection on held-out data: trains one network per seed (``train``
+    with ``train_kw``), calibrates each for ``eps`` on ``cal_seqs`` and keeps
+    the one whose calibrated prefiltered pass scores the fewest DP cells on
+    that dataset.  The weights of the kept network stay in ``eng``; returns
+    its training report with ``selection`` (seed, cells, final loss of
+    every run).  Only the calibration dataset is used to choose, never the
+    data the pass is later measured on."""
+    best, runs = None, []
+    for sd in seeds:
+        rep = train(eng, train_sets, eps, seed=sd, **train_kw)
+        _, crep = calibrate(eng, cal_seqs, eps, seed=0)
+        runs.append({"seed": int(sd), "cal_cells": crep.get("cal_cells"), "loss": rep["epoch_loss"][-1]})
+        if crep.get("cal_cells") is not None and (best is None or crep["cal_cells"] < best[0]):
+            best = (crep["cal_cells"], sd, eng.prefilter_params(), rep)
+    eng.prefilter_params(set_to=best[2])
+    rep = best[3]
+    rep["seed"] = int(best[1])
+    rep["selection"] = runs
+    return rep
+
+
+def projection_select(eng, features, a, b, d, lens, cal_seqs, eps: float, seeds=(0, 1, 2)):
+    """The same selection for the method without the network: one random
+    projection per seed, each scaled by least squares on the exact-scored
+    pairs (a, b, d) of the rows of ``features`` and calibrated on
+    ``cal_seqs``; keeps the one with the fewest DP cells on that dataset.
+    Returns (embedding function of an uploaded engine, report)."""
+    best, runs = None, []
+    for sd in seeds:
+        scale = projection_scale(features, a, b, d, lens, seed=sd)
+        fn = (lambda sc, s2: lambda en: (sc * projection_embeddings(en.kmer_features(5), seed=s2))
+              .astype(np.float32))(scale, sd)
+        _, crep = calibrate(eng, cal_seqs, eps, seed=0, embeddings=fn)
+        runs.append({"seed": int(sd), "cal_cells": crep.get("cal_cells"), "scale": scale})
+        if crep.get("cal_cells") is not None and (best is None or crep["cal_cells"] < best[0]):
+            best = (crep["cal_cells"], sd, fn)
+    return best[2], {"seed": int(best[1]), "selection": runs}
 
 
 def fit(eng, train_sets, cal_seqs, eps: float, n_train: int = 2_000_000, n_cal: int = 200_000,

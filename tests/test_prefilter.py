@@ -234,9 +234,11 @@ def _odd_sequences(rng):
 @pytest.mark.gpu
 def test_learned_prefilter_recall_ari_and_gain_over_projection():
     """The whole recipe of the config-4 benchmark (config-2 distribution):
-    train once on 2M exact-scored pairs of 60 datasets of 6,000 reads with
-    600 families each (weight decay 0.01), calibrate per eps on a held-out
-    dataset, run the prefiltered pass on a third one at eps 300 and 200.
+    train on 2M exact-scored pairs of 60 datasets of 6,000 reads with 600
+    families each (weight decay 0.01) with three seeds, keep the network with
+    the fewest DP cells on a held-out calibration dataset, calibrate per eps
+    on that dataset, run the prefiltered pass on a third one at eps 300 and
+    200.  The projection baseline is chosen among three seeds the same way.
     Its eps-neighbour recall against the exact pass must be >= 0.999 and the
     DBSCAN clusters must agree (adjusted Rand >= 0.99).  At both eps the same
     recipe without the network (a fixed random projection of the same k-mer
@@ -248,8 +250,9 @@ def test_learned_prefilter_recall_ari_and_gain_over_projection():
     test, _ = W.config2(seed=2)
     n = len(test)
     e = swgpu.Engine()
-    rep = PF.train(e, train_sets, 300.0, seed=0, weight_decay=0.01)
+    rep = PF.train_select(e, train_sets, cal_seqs, 300.0, seeds=(0, 1, 2), weight_decay=0.01)
     assert rep["epoch_loss"][-1] < 0.5 * rep["epoch_loss"][0]
+    assert len(rep["selection"]) == 3
     learned = {}
     for eps in (300.0, 200.0):
         margins, _ = PF.calibrate(e, cal_seqs, eps, seed=0)
@@ -273,8 +276,8 @@ def test_learned_prefilter_recall_ari_and_gain_over_projection():
     e.upload_sets(train_sets[:5])
     nsub = e.n
     keep = (ta < nsub) & (tb < nsub)
-    scale = PF.projection_scale(e.kmer_features(5), ta[keep], tb[keep], td[keep], tl)
-    proj = lambda en: (scale * PF.projection_embeddings(en.kmer_features(5))).astype(np.float32)
+    proj, _ = PF.projection_select(e, e.kmer_features(5), ta[keep], tb[keep], td[keep], tl, cal_seqs, 300.0,
+                                   seeds=(0, 1, 2))
     for eps in (300.0, 200.0):
         m2, _ = PF.calibrate(e, cal_seqs, eps, seed=0, embeddings=proj)
         e.upload(test)

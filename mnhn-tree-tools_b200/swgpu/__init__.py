@@ -343,18 +343,26 @@ def split_set_to_lists(s: SplitSet):
 
 
 class SeqBuffer:
-    """Sequences held as NUL-terminated C buffers (kept alive with the object)."""
+    """Sequences as NUL-terminated C strings in one contiguous host block
+    (kept alive with the object): ptrs / lens are the addresses of the
+    pointer and length arrays the C calls take."""
 
     def __init__(self, seqs):
-        self.bufs = [C.create_string_buffer(bytes(s), len(s) + 1) for s in seqs]
         self.n = len(seqs)
-        self.ptrs = (C.c_char_p * max(1, self.n))(*[C.addressof(b) for b in self.bufs])
-        self.lens = (C.c_size_t * max(1, self.n))(*[len(s) for s in seqs])
+        lens = np.fromiter(map(len, seqs), dtype=np.int64, count=self.n)
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        np.cumsum(lens + 1, out=off[1:])
+        self._blob = b"\0".join(list(seqs) + [b""])  # every sequence followed by its NUL
+        base = C.cast(C.c_char_p(self._blob), C.c_void_p).value  # the C calls only read it
+        self._ptr = (base + off[:-1]).astype(np.uint64) if self.n else np.zeros(1, dtype=np.uint64)
+        self._len = lens.astype(np.uint64) if self.n else np.zeros(1, dtype=np.uint64)
+        self.ptrs = self._ptr.ctypes.data
+        self.lens = self._len.ctypes.data
 
     def dataset(self) -> Dataset:
-        mx = max((len(b) - 1 for b in self.bufs), default=0)
-        return Dataset(C.cast(self.ptrs, C.POINTER(C.c_char_p)), C.cast(self.lens, C.POINTER(C.c_size_t)),
-                       None, self.n, None, 0, mx)
+        mx = int(self._len.max()) if self.n else 0
+        return Dataset(self._ptr.ctypes.data_as(C.POINTER(C.c_char_p)),
+                       self._len.ctypes.data_as(C.POINTER(C.c_size_t)), None, self.n, None, 0, mx)
 
 
 class Engine:

@@ -102,9 +102,14 @@ struct GemmShape {
   static constexpr int STAGE_BYTES = G_TILE_BYTES + B_BYTES;
   static constexpr int TMEM_COLS = BN;  // a power of two >= 32
 };
-// 8 warps: warp w drains accumulator rows 32*(w%4) .. +31 (the tensor-memory
-// lanes its quarter may read) and columns 64*(w/4) .. +63
-constexpr int G_THREADS = 256;
+// Warp w drains accumulator rows 32*(w%4) .. +31 (the tensor-memory lanes its
+// quarter may read) and 32 columns from 32*(w/4): 16 warps for 128-wide tiles
+// (one CTA per SM), 8 for 64-wide ones (two CTAs per SM).  The epilogue runs
+// after the tile's last MMA, so spreading it over more warps shortens the CTA.
+template <int BN>
+constexpr int gemm_threads() {
+  return BN == 128 ? 512 : 256;
+}
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
@@ -161,9 +166,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
 
 // One CTA per 128 x BN tile of C.  Warp 0 lane 0 feeds the stage ring with
 // TMA, warp 1 lane 0 issues the MMAs (4 per 64-wide K step) and commits each
-// stage back to the producer; then all eight warps drain the accumulator.
+// stage back to the producer; then every warp drains its part of the accumulator.
 template <int BN>
-__global__ void __launch_bounds__(G_THREADS, BN == 64 ? 2 : 1)
+__global__ void __launch_bounds__(gemm_threads<BN>(), BN == 64 ? 2 : 1)
     gemm_bf16_tn_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int M, int N,
                         int K, GemmEpi ep) {
   using S = GemmShape<BN>;
@@ -233,16 +238,16 @@ __global__ void __launch_bounds__(G_THREADS, BN == 64 ? 2 : 1)
   __syncwarp();
 
   // epilogue: warp w drains rows 32*(w%4) .. +31 (its tensor-memory lane
-  // quarter) and columns 64*(w/4) .. +63
+  // quarter) and columns 32*(w/4) .. +31
   int ok = 0;
   if (lane == 0) ok = mbar_wait_bounded(&done_bar, 0, ep.wait_limit) ? 1 : 0;
   ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
   if (!ok && lane == 0) atomicOr(ep.status, KST_TIMEOUT);
   tc_fence_after();
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3, slice = warp >> 2;
   const int m = m0 + quarter * 32 + lane;
   if (ok) {
-    for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 16) {
+    for (int c = slice * 32; c < slice * 32 + 32; c += 16) {
       uint32_t r[16];
       tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
       const long long rowoff = (long long)m * N + n0 + c;
@@ -392,7 +397,7 @@ static cudaError_t launch_gemm_bn(int bn, const __nv_bfloat16* A, const __nv_bfl
     attr = true;
   }
   dim3 grid(N / bn, M / G_BM);
-  kern<<<grid, G_THREADS, gemm_smem_bytes(bn), st>>>(ma, mb, M, N, K, ep);
+  kern<<<grid, bn == 64 ? gemm_threads<64>() : gemm_threads<128>(), gemm_smem_bytes(bn), st>>>(ma, mb, M, N, K, ep);
   return cudaGetLastError();
 }
 

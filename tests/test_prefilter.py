@@ -84,12 +84,14 @@ def test_kmer_features_match_reference():
                                             (384, 512, 1024, True, 1), (128, 256, 8192, False, 0),
                                             (512, 1024, 256, False, 1), (256, 192, 128, True, 1),
                                             (4096, 640, 256, True, 1), (4864, 512, 1024, True, 1),
-                                            (4096, 512, 1024, True, 1)])
+                                            (4096, 512, 1024, True, 1), (8192, 512, 1024, True, 1),
+                                            (20096, 512, 1024, True, 1)])
 def test_tcgen05_gemm_matches_float64(M, N, K, bias, act):
     """C = A B^T (+ bias, GELU) on the tensor cores against float64.  Grids of
     128 x 128 tiles that would fill fewer than half the SMs (and N = 192) run
-    128 x 64 tiles two CTAs per SM; 4096 x 640, 4864 x 512 and 4096 x 512 run
-    128 x 128 tiles."""
+    128 x 64 tiles two CTAs per SM; 4096 x 640 and the N = 512 shapes (the
+    prefilter's first layer at the training batch and at the embedding of
+    20,000 reads) run 128 x 128 tiles."""
     import torch
     g = torch.Generator().manual_seed(M * 7 + N + K)
     A = torch.randn(M, K, generator=g).to(torch.bfloat16)

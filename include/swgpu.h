@@ -361,8 +361,10 @@ swe_status swe_autotune(swe_ctx* ctx, const char* const* seqs, const size_t* len
    its counter of over-length pairs): calls that overlap on the GPU - on
    different streams or threads - race and must be serialised by the caller.
    The first call on a device looks up the array's device address with that
-   device current and keeps it; make that first call before any stream
-   capture, and do not call it again after a cudaDeviceReset of the device. */
+   device current and keeps it with the CUDA context current then (a call from
+   another context of the device looks it up again); make that first call
+   before any stream capture, and do not call it again after a
+   cudaDeviceReset of the device. */
 #define SWE_NOALLOC_MAX_LEN 65535
 swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* off, const int* len, const int* pairs,
                                    int64_t npairs, unsigned* out, int max_len, void* stream);

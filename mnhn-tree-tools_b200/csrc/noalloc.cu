@@ -18,9 +18,12 @@
 //
 // Host code cannot pass the arrays' names to a kernel (on the host they are
 // only stand-ins for the device symbols), so the device addresses are looked
-// up once per device with cudaGetSymbolAddress, with that device current, on
-// the first call made on it.  A cudaDeviceReset of that device invalidates
-// them; the call is not meant to be used after one.
+// up with cudaGetSymbolAddress, with the device current, on the first call
+// made on it, and kept together with the CUDA context that was current then:
+// a call from another context of the same device (one a driver-API caller
+// made current) looks them up again.  A cudaDeviceReset invalidates them, and
+// the context made after it may carry the old handle, so the call is not
+// meant to be used after a reset.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -89,10 +92,31 @@ __global__ void __launch_bounds__(256) noalloc_pairs_kernel(NoAllocParams p) {
 namespace {
 std::mutex g_setup_mu;
 struct DeviceSymbols {
+  void* ctx = nullptr;  // the context current when the addresses were taken
   int* scratch = nullptr;
   unsigned* rejected = nullptr;
 };
 DeviceSymbols g_symbols[64];
+
+// The calling thread's current CUDA context (driver API, reached through the
+// runtime's entry-point query so the library needs no link to libcuda), or
+// nullptr when there is none or the query is unavailable.
+void* current_context() {
+  typedef int (*CtxGetCurrentFn)(void**);
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (CtxGetCurrentFn) nullptr;
+    }
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 }  // namespace
 
 }  // namespace swgpu
@@ -114,7 +138,8 @@ extern "C" swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* o
   DeviceSymbols sym;
   {
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_symbols[dev].scratch) {
+    void* ctx = current_context();
+    if (!g_symbols[dev].scratch || !ctx || ctx != g_symbols[dev].ctx) {
       void* a = nullptr;
       void* r = nullptr;
       if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess || !a ||
@@ -124,6 +149,8 @@ extern "C" swe_status swe_score_pairs_noalloc(const char* seqs, const int64_t* o
       }
       g_symbols[dev].scratch = static_cast<int*>(a);
       g_symbols[dev].rejected = static_cast<unsigned*>(r);
+      // the lookup sets up the device's primary context when none was current yet
+      g_symbols[dev].ctx = ctx ? ctx : current_context();
     }
     sym = g_symbols[dev];
   }

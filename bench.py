@@ -1019,6 +1019,8 @@ def measure_prefilter(run: Run, config: str, args, steps: int, warmup: int, e2e_
             "candidates": int(st["candidates"]), "tiles_kept": int(st["tiles_kept"]), "tiles_all": int(st["tiles_all"]),
             "tile_cells": st["tile_cells"], "ms_embed": round(st["ms_embed"], 2),
             "ms_candidates": round(st["ms_candidates"], 2), "ms_layout": round(st["ms_layout"], 2),
+            "ms_layout_parts": {"groups": round(st["ms_groups"], 2), "tile_marks": round(st["ms_marks"], 2),
+                                "upload": round(st["ms_upload"], 2)},
             "ms_score": round(st["ms_score"], 2), "margins": [[u, round(m, 5)] for u, m in margins],
             "scale": crep.get("scale"), "cal_recall_trials": crep.get("scale_trials")}
     clk = clocks.stop()

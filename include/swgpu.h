@@ -150,6 +150,12 @@ swe_status swe_distance_copy(swe_ctx* ctx, void* dev_buf, int to_engine);
 /* The assignment swe_set_partition uses: owner[t] for costs cost[0..n) given
    in descending order. */
 void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
+/* The grouping of the prefiltered pass (host only; no counterpart in the
+   reference): single linkage over `count` pairs (pairs[2c], pairs[2c+1],
+   indices below n) taken in the given order, a join skipped when the two
+   groups together would exceed `cap` members; label[i] receives the smallest
+   index of i's group. */
+void swe_capped_linkage(int n, const int* pairs, int64_t count, int cap, int* label);
 /* The exchange of a split pass sized to the result (the counterpart of the
    reference's gather of distance stripes to its master, dbscan.c:374-379,
    457-458): a group's payload is the distance rectangles of its own tiles,

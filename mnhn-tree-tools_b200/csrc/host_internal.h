@@ -147,6 +147,11 @@ long long engine_sweep_key(const swe_ctx* ctx, float eps);
 // (the lowest index on ties), so every process derives the same groups.
 void lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
 
+// Single linkage over `count` pairs (pairs[2c], pairs[2c+1]) taken in order,
+// a join skipped when the two groups together would exceed `cap` members;
+// label[i] = the smallest index of i's group.
+void capped_linkage(int n, const int* pairs, int64_t count, int cap, int* label);
+
 // Deep copy of a split set (malloc'd like the original).
 split_set copy_split_set(const split_set& s);
 

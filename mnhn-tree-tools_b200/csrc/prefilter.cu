@@ -552,35 +552,24 @@ swe_status swe_score_prefiltered(swe_ctx* ctx, float eps, const swe_margins* mar
     // size put each family's candidate pairs into few tiles.  Without
     // embeddings every sequence is its own group.
     constexpr int kGroupCap = 128;
-    std::vector<int> parent(n), gsize(n, 1);
-    std::iota(parent.begin(), parent.end(), 0);
-    auto find = [&](int x) {
-      while (parent[x] != x) {
-        parent[x] = parent[parent[x]];
-        x = parent[x];
-      }
-      return x;
-    };
-    if (group)
-      for (unsigned long long c = 0; c < count; ++c) {
-        int x = find(pf->h_cand.p[c].x), y = find(pf->h_cand.p[c].y);
-        if (x == y || gsize[x] + gsize[y] > kGroupCap) continue;
-        if (x > y) std::swap(x, y);
-        parent[y] = x;  // the root is the group's smallest index
-        gsize[x] += gsize[y];
-      }
+    std::vector<int> label(std::max(n, 1));  // each sequence's group: its smallest index
+    if (group) {
+      capped_linkage(n, reinterpret_cast<const int*>(pf->h_cand.p), (int64_t)count, kGroupCap, label.data());
+    } else {
+      for (int i = 0; i < n; ++i) label[i] = i;
+    }
     // groups in order of their mean length (longest first), so that the
     // column blocks and packs that straddle two groups still hold sequences
     // of similar lengths
     std::vector<int64_t> gsum(n, 0), gcnt(n, 0);
     for (int i = 0; i < n; ++i) {
-      const int r = find(i);
+      const int r = label[i];
       gsum[r] += ctx->len[i];
       gcnt[r] += 1;
     }
     std::vector<int64_t> key(n);
     for (int i = 0; i < n; ++i) {
-      const int r = find(i);
+      const int r = label[i];
       const int64_t mean = (gsum[r] + gcnt[r] / 2) / std::max<int64_t>(gcnt[r], 1);
       // no candidate at all: after every group (any order works for them)
       key[i] = has[i] ? (((int64_t)INT32_MAX - mean) << 32 | (int64_t)r) : INT64_MAX;

@@ -157,7 +157,7 @@ EXPORTS = [
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
-    "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition",
+    "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition", "swe_capped_linkage",
     "swe_pca_covariance", "swe_pca_eigen", "swe_pca_eigen_gpu", "swe_pca_project", "swe_pca",
     "swe_autotune", "swe_copy_set_rows", "swe_partition_bytes", "swe_partition_pack", "swe_partition_unpack",
     # include/mnhn_dropin.h
@@ -296,6 +296,8 @@ def lib():
         L.swe_distance_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.swe_lpt_partition.restype = None
         L.swe_lpt_partition.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.swe_capped_linkage.restype = None
+        L.swe_capped_linkage.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         L.swe_adaptive_matrix.restype = C.c_int
         L.swe_adaptive_matrix.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_char_p, C.c_void_p,
                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p]
@@ -839,6 +841,16 @@ def pca_eigen(cov, n_vectors: int) -> tuple[np.ndarray, np.ndarray]:
     V = np.zeros((max(n_vectors, 1), n))
     _check(lib().swe_pca_eigen(A.ctypes.data, n, n_vectors, w.ctypes.data, V.ctypes.data))
     return w, V[:n_vectors]
+
+
+def capped_linkage(n: int, pairs, cap: int) -> np.ndarray:
+    """Group label (the group's smallest index) of each of n items after
+    single linkage over the (a, b) rows of `pairs` in order, no group larger
+    than `cap` - the grouping of the prefiltered pass."""
+    p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1, 2)
+    label = np.zeros(max(1, n), dtype=np.int32)
+    lib().swe_capped_linkage(n, p.ctypes.data, len(p), cap, label.ctypes.data)
+    return label[:n]
 
 
 def lpt_partition(cost, nparts: int) -> np.ndarray:

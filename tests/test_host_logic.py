@@ -365,3 +365,47 @@ def test_kmer_file_loader_matches_reference_semantics(tmp_path):
     p.write_text(text)
     _, V = _load_kmer_file_with_lib(p)
     assert np.array_equal(V.view(np.uint32), O.load_kmer_text(text).view(np.uint32))
+
+
+def _linkage_reference(n, pairs, cap):
+    """Union-find with path halving, root = the group's smallest index: the
+    grouping rule of the prefiltered pass written out directly."""
+    parent = list(range(n))
+    size = [1] * n
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for a, b in pairs:
+        x, y = find(int(a)), find(int(b))
+        if x == y or size[x] + size[y] > cap:
+            continue
+        if x > y:
+            x, y = y, x
+        parent[y] = x
+        size[x] += size[y]
+    return np.array([find(i) for i in range(n)], dtype=np.int32)
+
+
+@pytest.mark.parametrize("cap", [1, 2, 3, 7, 128, 100000])
+def test_capped_linkage_matches_union_find(cap):
+    """The prefiltered layout's grouping (relabelling form) against a plain
+    union-find: random pairs, pairs within planted families in a random
+    order, repeated and self pairs."""
+    rng = np.random.default_rng(cap)
+    for n, m, fam in [(1, 3, 1), (50, 400, 5), (2000, 30000, 40), (3000, 60000, 300)]:
+        a = rng.integers(0, n, size=m)
+        b = rng.integers(0, n, size=m)
+        owner = rng.integers(0, fam, size=n)
+        same = [(i, j) for i, j in zip(rng.integers(0, n, size=4 * m), rng.integers(0, n, size=4 * m))
+                if owner[i] == owner[j]][:m]
+        for pairs in (np.stack([a, b], 1), np.array(same, dtype=np.int64).reshape(-1, 2),
+                      np.concatenate([np.stack([a, a], 1)[:10], np.stack([a, b], 1), np.stack([b, a], 1)])):
+            got = swgpu.capped_linkage(n, pairs, cap)
+            want = _linkage_reference(n, pairs, cap)
+            assert np.array_equal(got, want), (n, m, cap)
+            sizes = np.bincount(got, minlength=n)
+            assert sizes.max() <= max(cap, 1)

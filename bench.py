@@ -426,8 +426,14 @@ def run_reference(args):
     wl = WORKLOADS[args.config]
     seqs, _ = getattr(W, wl["gen"])()
     cells = W.cells(seqs) if wl["mode"] != "multi" else sum(W.cells(st) for st in seqs)
+    # the workload keys of the GPU arm's config, with the same values
+    cfg = {"workload": wl["text"]}
     if wl["mode"] == "multi":  # the per-cell rate does not depend on the set boundaries
+        cfg["n_sets"] = len(seqs)
         seqs = [q for st in seqs for q in st]
+        cfg.update(n_sequences=len(seqs), cells_per_gpu=cells)
+    else:
+        cfg.update(n_sequences=len(seqs), cells_per_gpu=cells, pairs_per_gpu=len(seqs) * (len(seqs) - 1) // 2)
     times, rates = [], []
     info = None
     for i in range(args.warmup + args.steps):
@@ -442,7 +448,7 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * statistics.median(times), 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": wl["text"], "n_sequences": len(seqs), "cells": cells},
+            "config": cfg,
             "cpu_baseline": dict(info, value=round(value, 3), unit="GCUPS"),
             "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference scores every ordered pair once per DBSCAN pass and re-scores per eps step"}

@@ -150,6 +150,10 @@ swe_status swe_distance_copy(swe_ctx* ctx, void* dev_buf, int to_engine);
 /* The assignment swe_set_partition uses: owner[t] for costs cost[0..n) given
    in descending order. */
 void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
+/* The order in which the score pass takes its tiles (host only): order[0..n)
+   receives the indices of cost[] by descending cost, equal costs in index
+   order. */
+void swe_cost_order(const double* cost, int64_t n, int* order);
 /* The grouping of the prefiltered pass (host only; no counterpart in the
    reference): single linkage over `count` pairs (pairs[2c], pairs[2c+1],
    indices below n) taken in the given order, a join skipped when the two

@@ -321,6 +321,73 @@ void lpt_partition(const double* cost, int64_t n, int nparts, int* owner) {
   }
 }
 
+void cost_order(const double* cost, int64_t n, int* order) {
+  if (n <= 0) return;
+  // Tile costs are products of small integers, so as 64-bit integers they
+  // sort exactly; key = max - cost turns "descending, ties in index order"
+  // into an ascending stable sort, done as an LSD radix sort over 11-bit
+  // digits (three passes for the 100,000-read workload's 4.9M tiles instead
+  // of a comparison sort).  Anything else takes the comparison sort.
+  uint64_t top = 0;
+  bool integral = n < ((int64_t)1 << 31);
+  for (int64_t i = 0; i < n && integral; ++i) {
+    const double c = cost[i];
+    if (!(c >= 0.0 && c < 9007199254740992.0) || c != std::floor(c)) integral = false;
+    else top = std::max(top, (uint64_t)c);
+  }
+  if (!integral) {
+    for (int64_t i = 0; i < n; ++i) order[i] = (int)i;
+    std::stable_sort(order, order + n, [&](int a, int b) { return cost[a] > cost[b]; });
+    return;
+  }
+  constexpr int kBits = 11;
+  constexpr uint64_t kMask = (1u << kBits) - 1;
+  std::vector<int64_t> count((size_t)1 << kBits);
+  if (top < ((uint64_t)1 << 32)) {
+    // key in the high half, index in the low half: one array moves per pass,
+    // and the low half keeps equal keys in index order
+    std::vector<uint64_t> v((size_t)n), v2((size_t)n);
+    for (int64_t i = 0; i < n; ++i) v[i] = ((top - (uint64_t)cost[i]) << 32) | (uint64_t)i;
+    for (int shift = 32; shift < 64 && (top >> (shift - 32)) != 0; shift += kBits) {
+      std::fill(count.begin(), count.end(), 0);
+      for (int64_t i = 0; i < n; ++i) ++count[(v[i] >> shift) & kMask];
+      int64_t sum = 0;
+      for (auto& c : count) {
+        const int64_t k = c;
+        c = sum;
+        sum += k;
+      }
+      for (int64_t i = 0; i < n; ++i) v2[count[(v[i] >> shift) & kMask]++] = v[i];
+      v.swap(v2);
+    }
+    for (int64_t i = 0; i < n; ++i) order[i] = (int)(uint32_t)v[i];
+    return;
+  }
+  std::vector<uint64_t> key((size_t)n), key2((size_t)n);
+  std::vector<int> tmp((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    key[i] = top - (uint64_t)cost[i];
+    order[i] = (int)i;
+  }
+  for (int shift = 0; shift < 64 && (top >> shift) != 0; shift += kBits) {
+    std::fill(count.begin(), count.end(), 0);
+    for (int64_t i = 0; i < n; ++i) ++count[(key[i] >> shift) & kMask];
+    int64_t sum = 0;
+    for (auto& c : count) {
+      const int64_t k = c;
+      c = sum;
+      sum += k;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t dst = count[(key[i] >> shift) & kMask]++;
+      key2[dst] = key[i];
+      tmp[dst] = order[i];
+    }
+    key.swap(key2);
+    std::copy(tmp.begin(), tmp.end(), order);
+  }
+}
+
 }  // namespace swgpu
 
 extern "C" swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_start, float eps_inc, int minpts,
@@ -376,6 +443,11 @@ extern "C" swe_status swe_adaptive_matrix(int n, const uint32_t* D, float eps_st
     for (auto& s : kept) free_split_set_and_associated_clusters(s);
   }
   return SWE_OK;
+}
+
+extern "C" void swe_cost_order(const double* cost, int64_t n, int* order) {
+  if (!cost || !order || n <= 0) return;
+  swgpu::cost_order(cost, n, order);
 }
 
 extern "C" void swe_lpt_partition(const double* cost, int64_t n, int nparts, int* owner) {

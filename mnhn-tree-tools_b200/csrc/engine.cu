@@ -478,8 +478,7 @@ static swe_status build_layout(swe_ctx* ctx, const std::vector<int64_t>* key, co
   ctx->tiles_all = tiles_all;
   {
     std::vector<int> idx(ctx->tiles.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    cost_order(cost.data(), (int64_t)cost.size(), idx.data());
     std::vector<FastTile> sorted(ctx->tiles.size());
     std::vector<double> sorted_cost(ctx->tiles.size());
     ctx->part_rects.resize(ctx->tiles.size());

@@ -147,6 +147,11 @@ long long engine_sweep_key(const swe_ctx* ctx, float eps);
 // (the lowest index on ties), so every process derives the same groups.
 void lpt_partition(const double* cost, int64_t n, int nparts, int* owner);
 
+// The score pass's tile order: order[0..n) = the indices of cost[] by
+// descending cost, equal costs in index order (what std::stable_sort with
+// "greater" gives).
+void cost_order(const double* cost, int64_t n, int* order);
+
 // Single linkage over `count` pairs (pairs[2c], pairs[2c+1]) taken in order,
 // a join skipped when the two groups together would exceed `cap` members;
 // label[i] = the smallest index of i's group.

@@ -157,7 +157,7 @@ EXPORTS = [
     "swe_prefilter_loss_grad", "swe_prefilter_train", "swe_prefilter_embed", "swe_prefilter_pair_dist",
     "swe_gemm_bf16", "swe_prefilter_set_embeddings", "swe_score_prefiltered",
     "swe_kmer_count", "swe_kmer_counts", "swe_kmer_tsv", "swe_upload_points", "swe_adaptive_matrix",
-    "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition", "swe_capped_linkage",
+    "swe_set_partition", "swe_distance_bytes", "swe_distance_copy", "swe_lpt_partition", "swe_capped_linkage", "swe_cost_order",
     "swe_pca_covariance", "swe_pca_eigen", "swe_pca_eigen_gpu", "swe_pca_project", "swe_pca",
     "swe_autotune", "swe_copy_set_rows", "swe_partition_bytes", "swe_partition_pack", "swe_partition_unpack",
     # include/mnhn_dropin.h
@@ -296,6 +296,8 @@ def lib():
         L.swe_distance_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.swe_lpt_partition.restype = None
         L.swe_lpt_partition.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.swe_cost_order.restype = None
+        L.swe_cost_order.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         L.swe_capped_linkage.restype = None
         L.swe_capped_linkage.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         L.swe_adaptive_matrix.restype = C.c_int
@@ -851,6 +853,15 @@ def capped_linkage(n: int, pairs, cap: int) -> np.ndarray:
     label = np.zeros(max(1, n), dtype=np.int32)
     lib().swe_capped_linkage(n, p.ctypes.data, len(p), cap, label.ctypes.data)
     return label[:n]
+
+
+def cost_order(cost) -> np.ndarray:
+    """Indices of `cost` by descending cost, ties in index order: the order of
+    the score pass's tile list."""
+    c = np.ascontiguousarray(cost, dtype=np.float64)
+    order = np.zeros(max(1, len(c)), dtype=np.int32)
+    lib().swe_cost_order(c.ctypes.data, len(c), order.ctypes.data)
+    return order[:len(c)]
 
 
 def lpt_partition(cost, nparts: int) -> np.ndarray:

@@ -409,3 +409,21 @@ def test_capped_linkage_matches_union_find(cap):
             assert np.array_equal(got, want), (n, m, cap)
             sizes = np.bincount(got, minlength=n)
             assert sizes.max() <= max(cap, 1)
+
+
+def test_tile_cost_order_is_a_stable_descending_sort():
+    """The score pass's tile order (radix sort of integer costs) equals a
+    stable sort by descending cost, ties in index order; non-integral costs
+    take the comparison sort."""
+    rng = np.random.default_rng(3)
+    cases = [np.zeros(0), np.array([5.0]), np.full(1000, 7.0),
+             rng.integers(0, 4, size=5000).astype(np.float64),  # many ties
+             (rng.integers(1, 3, size=200000) * rng.integers(8, 25, size=200000) *
+              rng.integers(4000, 12000, size=200000) * 16.0),  # tile-like products
+             rng.integers(0, 2**52, size=3000).astype(np.float64),  # wide keys: five passes
+             rng.random(2000) * 1e6]  # not integral
+    for c in cases:
+        want = np.argsort(-c, kind="stable").astype(np.int32)
+        got = swgpu.cost_order(c)
+        assert np.array_equal(got, want), len(c)
+

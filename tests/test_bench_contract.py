@@ -1,6 +1,7 @@
-"""The reference arm of bench.py (the reference's own score() on the host
-cores, no GPU) prints the one JSON line the benchmark contract asks for, with
-the GPU arm's workload keys, so the two lines compare the same workload."""
+"""bench.py's parts that need no GPU: the reference arm (the reference's own
+score() on the host cores) prints the one JSON line the benchmark contract
+asks for, with the GPU arm's workload keys, so the two lines compare the same
+workload; and the roofline's stored traffic figures parse."""
 from __future__ import annotations
 
 import json
@@ -12,10 +13,11 @@ import pytest
 import oracle as O
 from conftest import ROOT
 
-pytestmark = pytest.mark.skipif(not (O.REF_DIR / "libref_harness.so").exists(),
-                                reason="needs the reference harness built into oracle/_ref")
+needs_ref = pytest.mark.skipif(not (O.REF_DIR / "libref_harness.so").exists(),
+                               reason="needs the reference harness built into oracle/_ref")
 
 
+@needs_ref
 def test_reference_arm_prints_the_contract_line():
     out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--config", "2",
                           "--steps", "1", "--warmup", "0", "--ref-seconds", "1"],
@@ -35,3 +37,16 @@ def test_reference_arm_prints_the_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_stored_traffic_figures_parse():
+    """The roofline's DRAM traffic per launch comes from the committed ncu
+    summary: read + write bytes of the full config-2 launch and the config-3
+    launch (scaled from its 20,000-read capture)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.measured_traffic("fast_all_pairs_kernel", "config2") == 68_590_000 + 777_680_000
+    assert bench.measured_traffic("fast_all_pairs_kernel", "config3") == 1_711_140_000 + 19_383_600_000
+    assert bench.measured_traffic("fast_all_pairs_kernel", "config9") is None
+    gbs, src = bench.hbm_peak_gbs()
+    assert gbs > 1000 and src.startswith("of ")
